@@ -1,0 +1,174 @@
+/*
+ * mossb200.h - C ABI of the B200 dense simulation backend for MOSSQuantum.
+ *
+ * The library owns device-resident quantum states (ComplexF64, interleaved re/im, the
+ * same byte layout as Julia's Vector{ComplexF64}) and runs every numerical step on one
+ * NVIDIA B200 (sm_100a). The host-side backend (a Julia package through `ccall`, or the
+ * Python package mossquantum_b200 through ctypes) calls only these functions.
+ *
+ * Conventions (identical to MOSSQuantum, docs/conventions.md:5-17):
+ *   - qubit positions are ZERO-based here (reference position q is bit q-1);
+ *     bit 0 is the least significant bit of the amplitude index;
+ *   - a gate matrix's first position is its least significant local bit;
+ *   - matrices are column-major, complex interleaved (Julia Matrix{ComplexF64});
+ *   - density matrices are 2^n x 2^n column-major: row bits are the low n bits of the
+ *     vectorised index, column bits the high n bits;
+ *   - batch states store B samples back to back, one per column.
+ *
+ * Every function returns MB_OK (0) or a negative MB_E* code; mb_last_error() returns a
+ * thread-local message for the last failure on the calling thread. Validation happens
+ * before any device memory is touched, matching the reference's "validate before
+ * mutating" rule (src/api/backend_protocols.jl:203-215). There is no CPU fallback:
+ * every numerical call runs on the GPU or fails.
+ */
+#ifndef MOSSB200_H
+#define MOSSB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define MB_API __attribute__((visibility("default")))
+#else
+#define MB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------------------ */
+#define MB_OK 0
+#define MB_EINVAL (-1)          /* invalid argument: ArgumentError / DimensionMismatch   */
+#define MB_EUNSUPPORTED (-2)    /* UnsupportedOperation / UnsupportedGradient            */
+#define MB_ENOMEM_BUDGET (-3)   /* the HBM byte budget would be exceeded                 */
+#define MB_ETIMEOUT (-4)        /* a bounded wait ran out (serving loop, persistent work) */
+#define MB_EDEVICE (-5)         /* CUDA runtime error                                    */
+#define MB_ENOTINIT (-6)        /* mb_init has not been called                           */
+#define MB_ENORM (-7)           /* probabilities: state not normalised / negative entry  */
+#define MB_ENOTREADY (-8)       /* serving: result not available yet                     */
+
+/* ---- state kinds --------------------------------------------------------------------- */
+#define MB_PURE 0            /* StateVector           (src/states/state_vector.jl:12)        */
+#define MB_DENSITY 1         /* DensityMatrix         (src/states/density_matrix.jl:12)      */
+#define MB_BATCH_PURE 2      /* BatchStateVector      (src/states/batch_state_vector.jl:18)  */
+#define MB_BATCH_DENSITY 3   /* BatchDensityMatrix    (src/states/batch_density_matrix.jl:17)*/
+
+/* ---- instruction kinds and gate families ---------------------------------------------- */
+#define MB_OP_GATE 0         /* unitary gate (Gate{N}, src/quantum_circuits/gates/)          */
+#define MB_OP_CHANNEL 1      /* Kraus channel (QuantumMap, channels/quantum_map.jl:9-36)     */
+
+#define MB_FAM_MATRIX 0      /* fixed matrix given in mb_op.data                             */
+#define MB_FAM_RX 1          /* RxGate   Rx(θ)          (gates/Gates.jl:37)                  */
+#define MB_FAM_RY 2          /* RyGate   Ry(θ)          (gates/Gates.jl:39)                  */
+#define MB_FAM_RZ 3          /* RzGate   Rz(θ)          (gates/Gates.jl:41)                  */
+#define MB_FAM_PHASE 4       /* PHASEGate diag(1,e^{iθ}) (gates/Gates.jl:11)                 */
+#define MB_FAM_CRX 5         /* CRxGate  CONTROL(Rx(θ)), pos = (control, target)             */
+#define MB_FAM_CRY 6         /* CRyGate                                                      */
+#define MB_FAM_CRZ 7         /* CRzGate                                                      */
+#define MB_FAM_CPHASE 8      /* CPHASEGate CONTROL(PHASE(θ))                                 */
+#define MB_FAM_CCPHASE 9     /* CCPHASEGate CONTROLCONTROL(PHASE(θ)), pos = (c1, c2, target) */
+
+#define MB_OPF_ADJOINT 1     /* AdjointQuantumGate wrapper (gates/quantum_gate.jl:32-45)     */
+
+/* One instruction of a circuit template (QCircuit element, circuits/circuit.jl:98).
+ * pos: zero-based positions in the gate's own order (positions(g)); the library sorts
+ * them and permutes the matrix exactly like ordered_positions/ordered_mat
+ * (gates/abstract_gates.jl:88-112,162-166).
+ * Parametric families take their angle from theta[slot] at apply time (slot >= 0, an
+ * active parameter) or from `value` (slot < 0, a frozen parameter). */
+typedef struct mb_op {
+  int32_t kind;        /* MB_OP_GATE or MB_OP_CHANNEL                                     */
+  int32_t nq;          /* number of positions: gates 0..5, channels 1..2                  */
+  int32_t pos[5];      /* zero-based qubit positions in the instruction's own order       */
+  int32_t family;      /* MB_FAM_*; channels use MB_FAM_MATRIX                            */
+  int32_t slot;        /* active-parameter slot (0-based) or -1                           */
+  int32_t flags;       /* MB_OPF_*                                                        */
+  int32_t nkraus;      /* channels: number of Kraus matrices in data                      */
+  int32_t reserved;
+  double value;        /* frozen parameter value for parametric families                  */
+  const double* data;  /* MATRIX gates: 2^nq x 2^nq; channels: nkraus such matrices       */
+} mb_op;
+
+/* One observable term (QubitsTerm, operators/qubits_term.jl:12-30): coeff * ⊗ ops[j] on
+ * sites[j]. Sites are zero-based, distinct, in any order; ops are 2x2 column-major. */
+typedef struct mb_term {
+  int32_t nsites;      /* 0..5 (0 = coeff * identity)                                      */
+  int32_t sites[5];
+  double coeff[2];     /* complex coefficient (re, im)                                     */
+  const double* ops;   /* nsites 2x2 complex matrices, 8 doubles each                      */
+} mb_term;
+
+typedef struct mb_state_s* mb_state;
+typedef struct mb_circuit_s* mb_circuit;
+typedef struct mb_observable_s* mb_observable;
+
+/* apply flags */
+#define MB_APPLY_FUSED 0       /* tiled / fused kernels (default)                          */
+#define MB_APPLY_PLAIN 1       /* one plain kernel launch per gate (the per-call drop-in)  */
+#define MB_APPLY_PER_SAMPLE 2  /* batch states: theta holds B rows of nslots values         */
+
+/* ---- context: replaces the CPUBackend singleton (src/api/backend_protocols.jl:10-70) --- */
+MB_API int mb_init(int device, size_t hbm_budget_bytes);      /* budget 0 = 90% of free HBM    */
+MB_API int mb_shutdown(void);
+MB_API const char* mb_last_error(void);
+MB_API int mb_memory_info(size_t* used_bytes, size_t* budget_bytes);
+MB_API int mb_synchronize(void);
+MB_API int mb_version(void);
+/* Kernel launches the library has issued since mb_init (for launch accounting). */
+MB_API int mb_launch_count(uint64_t* launches);
+
+/* ---- states: StateVector / DensityMatrix / batches (src/states/*.jl) ------------------ */
+/* Allocate a state of `kind` with n qubits (0..30 pure, 0..15 density) and `batch`
+ * samples (ignored for single kinds). Contents are |0...0> (state_vector.jl:36-40). */
+MB_API int mb_state_create(int kind, int n, int batch, mb_state* out);
+MB_API int mb_state_free(mb_state s);
+MB_API int mb_state_set_zero(mb_state s);
+MB_API int mb_state_upload(mb_state s, const double* host, size_t n_doubles);
+MB_API int mb_state_download(mb_state s, double* host, size_t n_doubles);
+MB_API int mb_state_copy(mb_state dst, mb_state src);               /* same kind, n and batch  */
+MB_API int mb_state_info(mb_state s, int* kind, int* n, int* batch);
+/* DensityMatrix(psi) = psi psi' per sample (execution/channels.jl:19). dst must be the
+ * density kind of src's shape. */
+MB_API int mb_state_to_density(mb_state src, mb_state dst);
+/* Device address of the sample storage (for zero-copy interop; never a host pointer). */
+MB_API int mb_state_device_ptr(mb_state s, void** dev_ptr);
+
+/* ---- circuits (QCircuit + bind_parameters, src/api/parameter_binding.jl:19-63) -------- */
+MB_API int mb_circuit_create(const mb_op* ops, size_t nops, int n, mb_circuit* out);
+MB_API int mb_circuit_free(mb_circuit c);
+MB_API int mb_circuit_nslots(mb_circuit c, int* nslots);
+/* Number of fused passes the fused schedule uses on an n-qubit pure state. */
+MB_API int mb_circuit_passes(mb_circuit c, int* npasses);
+/* apply!(circuit, state) (execution/gates.jl:21-36, batch_gates.jl, channels.jl).
+ * theta: host array of nslots values (or B*nslots with MB_APPLY_PER_SAMPLE).
+ * A circuit with channels requires a density kind (pure states must be promoted first,
+ * mirroring StateVector -> DensityMatrix in execution/channels.jl:19). */
+MB_API int mb_apply(mb_circuit c, mb_state s, const double* theta, size_t ntheta, int flags);
+
+/* ---- observables (QubitsOperator, src/observables/expectation.jl:1-73) ---------------- */
+MB_API int mb_observable_create(const mb_term* terms, size_t nterms, mb_observable* out);
+MB_API int mb_observable_free(mb_observable o);
+/* <H> per sample: out holds 2 doubles (re, im) per sample (1 sample for single kinds). */
+MB_API int mb_expect(mb_observable o, mb_state s, double* out);
+/* out = H * in (execution/operators.jl:3-63); out has in's kind and shape. */
+MB_API int mb_observable_apply(mb_observable o, mb_state in, mb_state out);
+
+/* ---- readout (src/execution/probabilities.jl:42-105) ---------------------------------- */
+/* Marginal probabilities on `qubits` (zero-based; the first is the least significant bit
+ * of the output index), normalised; out holds 2^nq doubles per sample. */
+MB_API int mb_probabilities(mb_state s, const int* qubits, int nq, double* out);
+
+/* ---- adjoint gradients (src/differentiation/objectives.jl:183-296) --------------------
+ * value = sum_b w_b Re<H>_b after applying the circuit to a copy of `init`; grad[slot] =
+ * d value / d theta[slot] (slots, not independent parameters: the host accumulates a
+ * ParameterMap). weights: one per sample (NULL = 1 for single kinds, 1/B for batches).
+ * checkpoint_every: forward checkpoints every k instructions (<= 0 picks automatically). */
+MB_API int mb_adjoint(mb_circuit c, mb_observable o, mb_state init, const double* theta, size_t ntheta,
+               const double* weights, int checkpoint_every, double* value, double* grad);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MOSSB200_H */

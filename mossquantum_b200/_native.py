@@ -1,0 +1,164 @@
+"""ctypes binding of ``libmossb200.so`` (the C ABI declared in include/mossb200.h).
+
+The shared library is built in-tree (``mossquantum_b200/libmossb200.so``). There is no
+CPU fallback: if the library or a CUDA device is missing, every numerical call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libmossb200.so")
+
+# status codes (include/mossb200.h)
+MB_OK = 0
+MB_EINVAL = -1
+MB_EUNSUPPORTED = -2
+MB_ENOMEM_BUDGET = -3
+MB_ETIMEOUT = -4
+MB_EDEVICE = -5
+MB_ENOTINIT = -6
+MB_ENORM = -7
+MB_ENOTREADY = -8
+
+MB_PURE, MB_DENSITY, MB_BATCH_PURE, MB_BATCH_DENSITY = 0, 1, 2, 3
+MB_OP_GATE, MB_OP_CHANNEL = 0, 1
+FAMILIES = {"MATRIX": 0, "RX": 1, "RY": 2, "RZ": 3, "PHASE": 4, "CRX": 5, "CRY": 6, "CRZ": 7,
+            "CPHASE": 8, "CCPHASE": 9}
+MB_OPF_ADJOINT = 1
+MB_APPLY_FUSED, MB_APPLY_PLAIN, MB_APPLY_PER_SAMPLE = 0, 1, 2
+
+
+class BackendError(RuntimeError):
+    """A device-side failure reported by libmossb200."""
+
+
+class UnsupportedOperation(Exception):
+    """Mirror of MOSSQuantum.UnsupportedOperation (src/api/backend_protocols.jl:15-36)."""
+
+
+class BudgetExceeded(MemoryError):
+    """The HBM byte budget would be exceeded."""
+
+
+class MbOp(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int32), ("nq", ctypes.c_int32), ("pos", ctypes.c_int32 * 5),
+                ("family", ctypes.c_int32), ("slot", ctypes.c_int32), ("flags", ctypes.c_int32),
+                ("nkraus", ctypes.c_int32), ("reserved", ctypes.c_int32), ("value", ctypes.c_double),
+                ("data", ctypes.c_void_p)]
+
+
+class MbTerm(ctypes.Structure):
+    _fields_ = [("nsites", ctypes.c_int32), ("sites", ctypes.c_int32 * 5), ("coeff", ctypes.c_double * 2),
+                ("ops", ctypes.c_void_p)]
+
+
+_lib = None
+_lock = threading.Lock()
+_initialised = False
+
+
+def load():
+    """Load the shared library (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise BackendError(f"libmossb200.so is missing ({LIB_PATH}); run __graft_entry__.build() first")
+    L = ctypes.CDLL(LIB_PATH)
+    vp, dp, ip, sz = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int), ctypes.c_size_t
+    sig = {
+        "mb_init": ([ctypes.c_int, sz], ctypes.c_int),
+        "mb_shutdown": ([], ctypes.c_int),
+        "mb_last_error": ([], ctypes.c_char_p),
+        "mb_memory_info": ([ctypes.POINTER(sz), ctypes.POINTER(sz)], ctypes.c_int),
+        "mb_synchronize": ([], ctypes.c_int),
+        "mb_version": ([], ctypes.c_int),
+        "mb_launch_count": ([ctypes.POINTER(ctypes.c_uint64)], ctypes.c_int),
+        "mb_state_create": ([ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp)], ctypes.c_int),
+        "mb_state_free": ([vp], ctypes.c_int),
+        "mb_state_set_zero": ([vp], ctypes.c_int),
+        "mb_state_upload": ([vp, dp, sz], ctypes.c_int),
+        "mb_state_download": ([vp, dp, sz], ctypes.c_int),
+        "mb_state_copy": ([vp, vp], ctypes.c_int),
+        "mb_state_info": ([vp, ip, ip, ip], ctypes.c_int),
+        "mb_state_to_density": ([vp, vp], ctypes.c_int),
+        "mb_state_device_ptr": ([vp, ctypes.POINTER(vp)], ctypes.c_int),
+        "mb_circuit_create": ([ctypes.POINTER(MbOp), sz, ctypes.c_int, ctypes.POINTER(vp)], ctypes.c_int),
+        "mb_circuit_free": ([vp], ctypes.c_int),
+        "mb_circuit_nslots": ([vp, ip], ctypes.c_int),
+        "mb_circuit_passes": ([vp, ip], ctypes.c_int),
+        "mb_apply": ([vp, vp, dp, sz, ctypes.c_int], ctypes.c_int),
+        "mb_observable_create": ([ctypes.POINTER(MbTerm), sz, ctypes.POINTER(vp)], ctypes.c_int),
+        "mb_observable_free": ([vp], ctypes.c_int),
+        "mb_expect": ([vp, vp, dp], ctypes.c_int),
+        "mb_observable_apply": ([vp, vp, vp], ctypes.c_int),
+        "mb_probabilities": ([vp, ip, ctypes.c_int, dp], ctypes.c_int),
+        "mb_adjoint": ([vp, vp, vp, dp, sz, dp, ctypes.c_int, dp, dp], ctypes.c_int),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = L
+    return L
+
+
+def last_error() -> str:
+    return load().mb_last_error().decode(errors="replace")
+
+
+def check(rc: int, what: str = "") -> None:
+    if rc == MB_OK:
+        return
+    msg = last_error()
+    text = f"{what}: {msg}" if what else msg
+    if rc == MB_EINVAL:
+        raise ValueError(text)
+    if rc == MB_EUNSUPPORTED:
+        raise UnsupportedOperation(text)
+    if rc == MB_ENOMEM_BUDGET:
+        raise BudgetExceeded(text)
+    if rc == MB_ENORM:
+        raise ValueError(text)
+    raise BackendError(f"{text} (code {rc})")
+
+
+def lib():
+    """The library, initialised on device 0 on first use (override with init())."""
+    if not _initialised:
+        init()
+    return _lib
+
+
+def init(device: int = 0, budget_bytes: int = 0) -> None:
+    """mb_init: bind the backend to one GPU with an HBM byte budget (0 = 90% of free)."""
+    global _initialised
+    with _lock:
+        L = load()
+        check(L.mb_init(int(device), int(budget_bytes)), "mb_init")
+        _initialised = True
+
+
+def memory_info():
+    used, budget = ctypes.c_size_t(), ctypes.c_size_t()
+    check(lib().mb_memory_info(ctypes.byref(used), ctypes.byref(budget)))
+    return used.value, budget.value
+
+
+def launch_count() -> int:
+    v = ctypes.c_uint64()
+    check(load().mb_launch_count(ctypes.byref(v)))
+    return v.value
+
+
+def synchronize() -> None:
+    check(lib().mb_synchronize())
+
+
+def dptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))

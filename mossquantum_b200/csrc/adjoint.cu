@@ -1,0 +1,203 @@
+// Adjoint reverse sweep (src/differentiation/circuit.jl:77-229, expectation.jl:4-73,
+// objectives.jl:183-296, batch.jl:35-204).
+//
+// Forward: the circuit runs on a private copy of the initial state; the state at the start
+// of every checkpointed segment of k instructions is kept in HBM. Reverse: per instruction
+//   gate     Δ <- U'Δ (U'ΔU on density matrices), y <- U'y, and for every active parameter
+//            g += Re<y|D|Δ>  (pure)  or  Re(<Δ, D'y> + <Δ, yD>)  (density), D = (dU)'U;
+//   channel  Δ <- S'Δ and y <- the channel's input, recomputed from the segment checkpoint
+//            (the reference keeps every channel input; recomputation bounds the memory to
+//            one checkpoint per segment plus the channel inputs of one segment).
+// Circuits with channels run on density matrices throughout (a pure initial state is
+// promoted first, DensityMatrix(psi), execution/channels.jl:19); this gives the same
+// parameter gradient as promoting at the first channel.
+#include <algorithm>
+#include <cmath>
+#include <memory>
+#include <vector>
+
+#include "internal.h"
+
+using namespace mb;
+
+namespace {
+
+// Owns one device buffer for the duration of an adjoint call.
+struct Buf {
+  double2* p = nullptr;
+  Buf() = default;
+  Buf(const Buf&) = delete;
+  ~Buf() { dev_free(p); }
+  int alloc(size_t bytes) { return dev_alloc((void**)&p, bytes); }
+};
+
+}  // namespace
+
+namespace mb {
+
+// Gradient contribution of one active parameter (generator D at gen_off).
+static int gate_gradient(mb_circuit c, const COp& op, const double2* y, const double2* delta, int n, int is_dm,
+                         int nsamples, double* d_grad_slot, const double* d_w) {
+  Pos p{};
+  p.k = op.k;
+  for (int j = 0; j < op.k; ++j) p.p[j] = op.pos[j];
+  const double2* D = c->d_table + op.gen_off;
+  ReduceOut ro{nullptr, d_grad_slot, d_w, 0};
+  if (!is_dm) {
+    // Re <y| D |Δ> (back_propagate, circuit.jl:136-144)
+    return launch_cross_dense(y, delta, int64_t(1) << n, nsamples, p, D, 0, MAT_PLAIN, ws(), 0, ro, g_ctx.stream);
+  }
+  // Re(<Δ, D' y> + <Δ, y D>) (_density_gate_gradient!, circuit.jl:155-172): D' on the row
+  // bits, D^T on the column bits.
+  const int64_t elems = int64_t(1) << (2 * n);
+  int rc = launch_cross_dense(delta, y, elems, nsamples, p, D, 0, MAT_ADJOINT, ws(), 0, ro, g_ctx.stream);
+  if (rc) return rc;
+  for (int j = 0; j < op.k; ++j) p.p[j] = op.pos[j] + n;
+  return launch_cross_dense(delta, y, elems, nsamples, p, D, 0, MAT_TRANSPOSE, ws(), 0, ro, g_ctx.stream);
+}
+
+}  // namespace mb
+
+extern "C" int mb_adjoint(mb_circuit c, mb_observable o, mb_state init, const double* theta, size_t ntheta,
+                          const double* weights, int checkpoint_every, double* value, double* grad) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (int rc = check_init()) return rc;
+  if (!c || !o || !init || !value || (!grad && c->nslots) || (!theta && ntheta)) return MB_EINVAL;
+  if (init->n != c->n) {
+    set_error("circuit compiled for %d qubits, initial state has %d", c->n, init->n);
+    return MB_EINVAL;
+  }
+  if (int rc = validate_observable(o, init)) return rc;
+  if (!o->hermitian) {
+    set_error("adjoint gradients need a Hermitian observable");
+    return MB_EUNSUPPORTED;
+  }
+  const int B = init->batch;
+  if (B < 1) {
+    set_error("scalar batch objectives require at least one sample");
+    return MB_EINVAL;
+  }
+  const bool init_dm = init->kind == MB_DENSITY || init->kind == MB_BATCH_DENSITY;
+  const int is_dm = (init_dm || c->has_channel) ? 1 : 0;
+  const int n = c->n;
+  const int64_t elems = is_dm ? (int64_t(1) << (2 * n)) : (int64_t(1) << n);
+  const size_t sbytes = sizeof(double2) * size_t(elems) * B;
+  cudaStream_t st = g_ctx.stream;
+  int rc;
+  if ((rc = bind_circuit(c, theta, ntheta, 1))) return rc;
+
+  // Sample weights (the reduction of BatchExpectationObjective, api/objectives.jl:229-244).
+  std::vector<double> w(B, init->kind >= MB_BATCH_PURE ? 1.0 / B : 1.0);
+  if (weights) {
+    for (int b = 0; b < B; ++b) {
+      if (!std::isfinite(weights[b])) {
+        set_error("weights must be finite");
+        return MB_EINVAL;
+      }
+      w[b] = weights[b];
+    }
+  }
+  Buf d_w, d_grad, y, delta;
+  if ((rc = d_w.alloc(sizeof(double) * B)) || (rc = d_grad.alloc(sizeof(double) * std::max(1, c->nslots))) ||
+      (rc = y.alloc(sbytes)) || (rc = delta.alloc(sbytes)))
+    return rc;
+  MB_CHECK_CUDA(cudaMemcpyAsync(d_w.p, w.data(), sizeof(double) * B, cudaMemcpyHostToDevice, st));
+  double* d_g = reinterpret_cast<double*>(d_grad.p);
+  MB_CHECK_CUDA(cudaMemsetAsync(d_g, 0, sizeof(double) * std::max(1, c->nslots), st));
+  if (is_dm && !init_dm) {
+    if ((rc = launch_to_density(init->d, y.p, n, B, st))) return rc;
+  } else {
+    MB_CHECK_CUDA(cudaMemcpyAsync(y.p, init->d, sbytes, cudaMemcpyDeviceToDevice, st));
+  }
+
+  // Segments of k instructions; checkpoint where a segment holds a channel or k was given.
+  const int nops = int(c->ops.size());
+  int k = checkpoint_every;
+  if (k <= 0) k = c->has_channel ? std::max(1, int(std::ceil(std::sqrt(double(std::max(nops, 1)))))) : std::max(nops, 1);
+  const int S = std::max(1, (nops + k - 1) / k);
+  std::vector<std::unique_ptr<Buf>> ckpt(S);
+  std::vector<char> seg_channel(S, 0);
+  for (int i = 0; i < nops; ++i)
+    if (c->ops[i].kind == MB_OP_CHANNEL) seg_channel[i / k] = 1;
+
+  // Forward pass.
+  for (int s = 0; s < S; ++s) {
+    if (checkpoint_every > 0 || seg_channel[s]) {
+      ckpt[s].reset(new Buf());
+      if ((rc = ckpt[s]->alloc(sbytes))) return rc;
+      MB_CHECK_CUDA(cudaMemcpyAsync(ckpt[s]->p, y.p, sbytes, cudaMemcpyDeviceToDevice, st));
+    }
+    for (int i = s * k; i < std::min(nops, (s + 1) * k); ++i)
+      if ((rc = plain_op(c, c->ops[i], y.p, n, is_dm, B, 0, false))) return rc;
+  }
+
+  // Observation: value and seed (expectation.jl:4-73).
+  {
+    mb_state_s view;
+    view.kind = is_dm ? (init->kind >= MB_BATCH_PURE ? MB_BATCH_DENSITY : MB_DENSITY)
+                      : (init->kind >= MB_BATCH_PURE ? MB_BATCH_PURE : MB_PURE);
+    view.n = n;
+    view.batch = B;
+    view.dim = int64_t(1) << n;
+    view.elems = elems;
+    view.d = y.p;
+    if ((rc = expect_keys(o, &view))) return rc;
+    std::vector<double2> r(B);
+    MB_CHECK_CUDA(cudaMemcpyAsync(r.data(), g_ctx.results, sizeof(double2) * B, cudaMemcpyDeviceToHost, st));
+    MB_CHECK_CUDA(cudaStreamSynchronize(st));
+    double v = 0;
+    for (int b = 0; b < B; ++b) v += w[b] * r[b].x;
+    *value = v;
+  }
+  if (!is_dm) {
+    // λ = (conj z) Hψ + z H'ψ = 2Hψ for Hermitian H and z = 1.
+    if ((rc = observable_apply(o, y.p, delta.p, n, 0, B))) return rc;
+    if ((rc = launch_scale(delta.p, elems * B, 2.0, st))) return rc;
+  } else {
+    // z H' applied to the identity: the dense matrix H per sample.
+    Buf ident;
+    if ((rc = ident.alloc(sbytes))) return rc;
+    if ((rc = launch_identity_density(ident.p, n, B, st))) return rc;
+    if ((rc = observable_apply(o, ident.p, delta.p, n, 1, B))) return rc;
+    MB_CHECK_CUDA(cudaStreamSynchronize(st));
+  }
+
+  // Reverse pass.
+  for (int s = S - 1; s >= 0; --s) {
+    const int lo = s * k, hi = std::min(nops, (s + 1) * k);
+    std::vector<std::unique_ptr<Buf>> chin(hi - lo);
+    if (seg_channel[s]) {
+      Buf z;
+      if ((rc = z.alloc(sbytes))) return rc;
+      MB_CHECK_CUDA(cudaMemcpyAsync(z.p, ckpt[s]->p, sbytes, cudaMemcpyDeviceToDevice, st));
+      for (int i = lo; i < hi; ++i) {
+        if (c->ops[i].kind == MB_OP_CHANNEL) {
+          chin[i - lo].reset(new Buf());
+          if ((rc = chin[i - lo]->alloc(sbytes))) return rc;
+          MB_CHECK_CUDA(cudaMemcpyAsync(chin[i - lo]->p, z.p, sbytes, cudaMemcpyDeviceToDevice, st));
+        }
+        if ((rc = plain_op(c, c->ops[i], z.p, n, is_dm, B, 0, false))) return rc;
+      }
+      MB_CHECK_CUDA(cudaStreamSynchronize(st));
+    }
+    for (int i = hi - 1; i >= lo; --i) {
+      const COp& op = c->ops[i];
+      if (op.kind == MB_OP_CHANNEL) {
+        if ((rc = plain_op(c, op, delta.p, n, is_dm, B, 0, true))) return rc;
+        MB_CHECK_CUDA(cudaMemcpyAsync(y.p, chin[i - lo]->p, sbytes, cudaMemcpyDeviceToDevice, st));
+        continue;
+      }
+      if ((rc = plain_op(c, op, delta.p, n, is_dm, B, 0, true))) return rc;
+      if ((rc = plain_op(c, op, y.p, n, is_dm, B, 0, true))) return rc;
+      if (op.gen_off >= 0)
+        if ((rc = gate_gradient(c, op, y.p, delta.p, n, is_dm, B, d_g + op.slot, reinterpret_cast<const double*>(d_w.p)))) return rc;
+    }
+    if (ckpt[s]) MB_CHECK_CUDA(cudaMemcpyAsync(y.p, ckpt[s]->p, sbytes, cudaMemcpyDeviceToDevice, st));
+    MB_CHECK_CUDA(cudaStreamSynchronize(st));
+    chin.clear();
+    ckpt[s].reset();
+  }
+  if (c->nslots) MB_CHECK_CUDA(cudaMemcpyAsync(grad, d_g, sizeof(double) * c->nslots, cudaMemcpyDeviceToHost, st));
+  MB_CHECK_CUDA(cudaStreamSynchronize(st));
+  return MB_OK;
+}

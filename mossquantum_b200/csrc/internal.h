@@ -1,0 +1,126 @@
+// Internal host-side structures of libmossb200 (handles behind the opaque ABI types).
+#pragma once
+#include <map>
+#include <mutex>
+#include <vector>
+
+#include "kernels.h"
+
+namespace mb {
+
+enum OpClass { CLS_DENSE = 0, CLS_DIAG = 1, CLS_MONO = 2 };
+
+// One compiled instruction: positions sorted ascending, matrix stored in ordered form in
+// the circuit's matrix table (ordered_positions / ordered_mat, abstract_gates.jl:88-112).
+struct COp {
+  int kind;            // MB_OP_GATE / MB_OP_CHANNEL
+  int k;               // number of positions (channel: qubits; its supermatrix spans 2k bits)
+  int pos[5];          // ordered positions
+  int family, slot, flags;
+  double value;
+  bool parametric;     // matrix evaluated on the device from theta
+  int cls;             // OpClass
+  uint32_t active;     // CLS_DIAG: local indices whose factor may differ from 1
+  int sigma[32];       // CLS_MONO: destination of local index a (-1 = unchanged)
+  int sigma_inv[32];
+  int mat_off;         // ordered matrix (gates) or supermatrix (channels) in the table
+  int gen_off;         // derivative generator (active parametric gates) or -1
+};
+
+struct Schedule;       // fused-pass schedule (fused.cu)
+
+struct mb_circuit_impl_tag {};
+
+}  // namespace mb
+
+struct mb_state_s {
+  int kind = 0, n = 0, batch = 1;
+  int64_t dim = 1, elems = 1;
+  double2* d = nullptr;
+  size_t bytes = 0;
+};
+
+struct mb_circuit_s {
+  int n = 0;
+  std::vector<mb::COp> ops;
+  int nslots = 0;
+  bool has_channel = false;
+  std::vector<double2> fixed_table;   // one sample's table with fixed matrices filled in
+  int64_t table_elems = 1;            // double2 entries per sample row
+  std::vector<mb::BindRec> binds;
+  mb::BindRec* d_binds = nullptr;
+  double2* d_table = nullptr;
+  int table_rows = 1;
+  double* d_theta = nullptr;
+  size_t theta_cap = 0;
+  double* h_theta = nullptr;          // pinned staging for theta uploads
+  size_t h_theta_cap = 0;
+  mb::Schedule* sched = nullptr;      // fused schedule for pure states (built lazily)
+};
+
+namespace mb {
+struct OKey {
+  int k;
+  int pos[5];
+  int mat_off;
+};
+struct PauliGroup;   // pauli.cu
+}  // namespace mb
+
+struct mb_observable_s {
+  std::vector<mb::OKey> keys;         // one dense local matrix per sorted site tuple
+  std::vector<double2> h_mats;
+  double2* d_mats = nullptr;
+  bool hermitian = true;
+  int max_site = -1;
+  // Pauli-string form for the fused expectation kernel.
+  bool pauli_ok = false;
+  void* d_pauli = nullptr;
+  std::vector<char> h_pauli;          // serialized groups (pauli.cu owns the layout)
+  int pauli_ngroups = 0;
+};
+
+namespace mb {
+
+struct Ctx {
+  bool init = false;
+  int device = 0;
+  int sm_count = 148;
+  cudaStream_t stream = nullptr;
+  size_t budget = 0, used = 0;
+  std::map<void*, size_t> sizes;
+  double2* partials = nullptr;
+  unsigned* counters = nullptr;
+  int64_t partials_cap = 0;
+  int ncounters = 0;
+  double2* results = nullptr;
+  unsigned* flags = nullptr;
+};
+
+extern Ctx g_ctx;
+extern std::recursive_mutex g_mu;
+
+int dev_alloc(void** p, size_t bytes);
+void dev_free(void* p);
+int check_init();
+ReduceWs ws();
+
+int state_alloc(int kind, int n, int batch, mb_state* out);
+int bind_circuit(mb_circuit c, const double* theta, size_t ntheta, int rows);
+int plain_op(mb_circuit c, const COp& op, double2* v, int n, int is_dm, int nsamples, int64_t mrow_stride,
+             bool dagger);
+int apply_plain(mb_circuit c, mb_state s, int64_t mrow_stride);
+int validate_apply(mb_circuit c, mb_state s);
+int validate_observable(mb_observable o, mb_state s);
+int expect_keys(mb_observable o, mb_state s);
+int observable_apply(mb_observable o, const double2* in, double2* out, int n, int is_dm, int nsamples);
+
+// fused.cu
+int apply_fused(mb_circuit c, mb_state s, int64_t mrow_stride);
+void release_schedules(mb_circuit c);
+
+// pauli.cu
+int pauli_compile(mb_observable o, const mb_term* terms, size_t nterms);
+int expect_pauli(mb_observable o, mb_state s);
+
+}  // namespace mb

@@ -1,0 +1,92 @@
+"""Seeded synthetic workloads: the circuits and observables the benchmarks and tests use.
+
+The reference publishes no dataset for this path; every input is synthetic and seeded
+(base seed 20261203). Shapes follow the reference's hardware-efficient benchmark circuits
+(docs/performance/cpu-scheduling-2026-11-17/benchmark-source/cpu_thread_scan.jl:4-18) and
+its spin-chain builders (src/utilities/models/spin_hamiltonians.jl:7-63).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from .channels import AmplitudeDamping, Depolarizing
+from .circuit import QCircuit
+from .gates import CNOTGate, CZGate, QuantumGate, RxGate, RyGate, RzGate, U3
+from .operators import QubitsOperator, QubitsTerm
+
+BASE_SEED = 20261203
+
+
+def rng_for(*stream):
+    return np.random.default_rng([BASE_SEED, *stream])
+
+
+def hea_angles(n, depth, rng):
+    return rng.uniform(0.0, 2 * np.pi, size=(depth, n, 3))
+
+
+def hea_circuit(n, depth, angles=None, active=True, noise=None):
+    """Layer: RX, RY, RZ on every qubit (in that order per qubit), then CNOT(i, i+1).
+
+    noise=(p, gamma): after every gate, Depolarizing(p) then AmplitudeDamping(gamma) on
+    each qubit the gate touches.
+    """
+    if angles is None:
+        angles = np.zeros((depth, n, 3))
+    c = QCircuit()
+
+    def add(g):
+        c.push(g)
+        if noise is not None:
+            p, gamma = noise
+            for q in g.positions:
+                if p:
+                    c.push(Depolarizing(q, p))
+                if gamma:
+                    c.push(AmplitudeDamping(q, gamma))
+
+    for layer in range(depth):
+        for q in range(1, n + 1):
+            add(RxGate(q, angles[layer, q - 1, 0], isparas=active))
+            add(RyGate(q, angles[layer, q - 1, 1], isparas=active))
+            add(RzGate(q, angles[layer, q - 1, 2], isparas=active))
+        for q in range(1, n):
+            add(CNOTGate(q, q + 1))
+    return c
+
+
+def u3_params(n, depth, rng):
+    u = rng.uniform(0.0, 1.0, size=(depth, n))
+    theta = np.arccos(1 - 2 * u)
+    phi = rng.uniform(0.0, 2 * np.pi, size=(depth, n))
+    lam = rng.uniform(0.0, 2 * np.pi, size=(depth, n))
+    return np.stack([theta, phi, lam], axis=-1)
+
+
+def u3_brickwork(n, depth, params):
+    """Layer l (0-based): U3 on every qubit, then CZ on (1,2),(3,4),... for even l and
+    (2,3),(4,5),... for odd l."""
+    c = QCircuit()
+    for layer in range(depth):
+        for q in range(1, n + 1):
+            c.push(QuantumGate(q, U3(*params[layer, q - 1])))
+        start = 1 if layer % 2 == 0 else 2
+        for q in range(start, n, 2):
+            c.push(CZGate(q, q + 1))
+    return c
+
+
+def tfim(n, h=1.0, J=1.0):
+    """H = -J sum Z_i Z_{i+1} - h sum X_i (open chain)."""
+    terms = [QubitsTerm([i, i + 1], ["Z", "Z"], -J) for i in range(1, n)]
+    terms += [QubitsTerm([i], ["X"], -h) for i in range(1, n + 1)]
+    return QubitsOperator(terms)
+
+
+def xxz(n, J=1.0, Jzz=0.5):
+    """H = sum (J X_i X_{i+1} + J Y_i Y_{i+1} + Jzz Z_i Z_{i+1})."""
+    terms = []
+    for i in range(1, n):
+        terms += [QubitsTerm([i, i + 1], ["X", "X"], J), QubitsTerm([i, i + 1], ["Y", "Y"], J),
+                  QubitsTerm([i, i + 1], ["Z", "Z"], Jzz)]
+    return QubitsOperator(terms)

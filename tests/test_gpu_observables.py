@@ -1,0 +1,100 @@
+"""Expectations, observable action and readout on the GPU vs the oracle.
+
+Mirrors test/regression/kernels.jl:45-94 (4/5-site and non-Hermitian expectations, H*rho)
+and src/execution/probabilities.jl semantics (marginals, normalisation, sampling).
+Tolerances: 1e-11 on expectations, 1e-12 on probabilities and amplitudes.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def random_state(n, rng):
+    v = rng.normal(size=1 << n) + 1j * rng.normal(size=1 << n)
+    return v / np.linalg.norm(v)
+
+
+def random_operator(mq, n, rng, hermitian=False):
+    names = ["X", "Y", "Z", "+", "-", "I", "u", "d"] if not hermitian else ["X", "Y", "Z", "I"]
+    terms = []
+    for k in (0, 1, 2, 3, 4, 5):
+        for _ in range(3):
+            pos = [int(x) for x in rng.choice(np.arange(1, n + 1), size=k, replace=False)]
+            ops = [names[rng.integers(len(names))] for _ in range(k)]
+            c = complex(rng.normal(), 0 if hermitian else rng.normal())
+            terms.append(mq.QubitsTerm(pos, ops, c))
+    return mq.QubitsOperator(terms)
+
+
+@pytest.mark.parametrize("n", [6, 11])
+def test_expectation_pure(mq, O, n):
+    rng = np.random.default_rng(n)
+    psi = random_state(n, rng)
+    s = mq.StateVector(psi)
+    for herm in (True, False):
+        H = random_operator(mq, n, rng, herm)
+        assert abs(mq.expectation(H, s) - O.expect(psi, n, H.specs())) <= 1e-11
+
+
+def test_expectation_density(mq, O):
+    n = 5
+    rng = np.random.default_rng(1)
+    a = rng.normal(size=(32, 32)) + 1j * rng.normal(size=(32, 32))
+    rho = a @ a.conj().T
+    rho /= np.trace(rho)
+    s = mq.DensityMatrix(rho)
+    for herm in (True, False):
+        H = random_operator(mq, n, rng, herm)
+        assert abs(mq.expectation(H, s) - np.trace(H.matrix(n) @ rho)) <= 1e-11
+
+
+def test_known_expectations(mq):
+    s = mq.StateVector(4)
+    assert mq.expectation(mq.QubitsTerm([1, 2, 3, 4], ["Z"] * 4, 2.0), s) == pytest.approx(2.0)
+    assert mq.expectation(mq.QubitsTerm([], [], 2.5), s) == pytest.approx(2.5)
+    d = mq.DensityMatrix(4)
+    assert mq.expectation(mq.QubitsTerm([1, 2, 3, 4], ["Z"] * 4, 2.0), d) == pytest.approx(2.0)
+
+
+def test_observable_action(mq, O):
+    n = 7
+    rng = np.random.default_rng(2)
+    psi = random_state(n, rng)
+    H = random_operator(mq, n, rng, False)
+    out = mq.apply_observable(H, mq.StateVector(psi)).to_numpy()
+    np.testing.assert_allclose(out, O.apply_observable(psi, n, H.specs()), atol=1e-12)
+
+
+def test_probabilities(mq, O):
+    n = 9
+    rng = np.random.default_rng(3)
+    psi = random_state(n, rng)
+    s = mq.StateVector(psi)
+    for qubits in ([1, 2, 3], [9, 2], [5], list(range(1, 10)), [3, 1, 7, 9, 2, 4, 5, 6, 8]):
+        np.testing.assert_allclose(mq.probabilities(s, qubits), O.probabilities(psi, n, qubits), atol=1e-12)
+    bell = mq.apply_(mq.QCircuit([mq.HGate(1), mq.CNOTGate(1, 2)]), mq.StateVector(2))
+    np.testing.assert_allclose(mq.probabilities(bell), [0.5, 0, 0, 0.5], atol=1e-15)
+    d = mq.DensityMatrix(mq.StateVector(psi))
+    np.testing.assert_allclose(mq.probabilities(d, [2, 5]), O.probabilities(psi, n, [2, 5]), atol=1e-12)
+
+
+def test_probabilities_validation(mq):
+    s = mq.StateVector(np.array([1.0, 1.0, 0, 0]))
+    with pytest.raises(ValueError):
+        mq.probabilities(s)
+    with pytest.raises(ValueError):
+        mq.probabilities(mq.StateVector(3), [1, 1])
+    with pytest.raises(ValueError):
+        mq.probabilities(mq.StateVector(3), [4])
+
+
+def test_sampling_matches_oracle_rng(mq, O):
+    n = 6
+    psi = random_state(n, np.random.default_rng(4))
+    s = mq.StateVector(psi)
+    a = mq.sample(np.random.default_rng(99), s, 500, qubits=[2, 4, 6])
+    b = O.sample(np.random.default_rng(99), O.probabilities(psi, n, [2, 4, 6]), 500)
+    assert np.array_equal(a, b)
+    c = mq.counts(np.random.default_rng(99), s, 500, qubits=[2, 4, 6])
+    assert sum(c.values()) == 500
