@@ -120,6 +120,8 @@ class Gate(Instruction):
         if isinstance(positions, int):
             positions = (positions,)
         self.pos = tuple(int(p) for p in positions)
+        if any(p <= 0 for p in self.pos) or len(set(self.pos)) != len(self.pos):
+            raise ValueError(f"gate positions must be positive and distinct: {self.pos}")
 
     @property
     def positions(self):
