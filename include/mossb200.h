@@ -118,6 +118,22 @@ MB_API int mb_version(void);
 /* Kernel launches the library has issued since mb_init (for launch accounting). */
 MB_API int mb_launch_count(uint64_t* launches);
 
+/* The CUDA stream (cudaStream_t) every library kernel runs on, for event timing and
+ * interop; callers must not destroy it. */
+MB_API int mb_get_stream(void** stream);
+
+/* Per-kernel timing: when enabled, every launch is bracketed by CUDA events on the library
+ * stream and its algorithmic HBM bytes are recorded. mb_profile_report synchronises and
+ * fills up to `cap` entries (one per kernel name); *count receives the number of names. */
+typedef struct mb_kernel_stat {
+  char name[48];
+  uint64_t launches;
+  double total_ms;
+  double bytes;        /* algorithmic bytes summed over launches */
+} mb_kernel_stat;
+MB_API int mb_profile(int enable);
+MB_API int mb_profile_report(mb_kernel_stat* stats, int cap, int* count);
+
 /* ---- states: StateVector / DensityMatrix / batches (src/states/*.jl) ------------------ */
 /* Allocate a state of `kind` with n qubits (0..30 pure, 0..15 density) and `batch`
  * samples (ignored for single kinds). Contents are |0...0> (state_vector.jl:36-40). */

@@ -57,6 +57,11 @@ class MbTerm(ctypes.Structure):
                 ("ops", ctypes.c_void_p)]
 
 
+class MbKernelStat(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char * 48), ("launches", ctypes.c_uint64), ("total_ms", ctypes.c_double),
+                ("bytes", ctypes.c_double)]
+
+
 _lib = None
 _lock = threading.Lock()
 _initialised = False
@@ -79,6 +84,9 @@ def load():
         "mb_synchronize": ([], ctypes.c_int),
         "mb_version": ([], ctypes.c_int),
         "mb_launch_count": ([ctypes.POINTER(ctypes.c_uint64)], ctypes.c_int),
+        "mb_get_stream": ([ctypes.POINTER(vp)], ctypes.c_int),
+        "mb_profile": ([ctypes.c_int], ctypes.c_int),
+        "mb_profile_report": ([ctypes.POINTER(MbKernelStat), ctypes.c_int, ip], ctypes.c_int),
         "mb_state_create": ([ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp)], ctypes.c_int),
         "mb_state_free": ([vp], ctypes.c_int),
         "mb_state_set_zero": ([vp], ctypes.c_int),
@@ -154,6 +162,26 @@ def launch_count() -> int:
     v = ctypes.c_uint64()
     check(load().mb_launch_count(ctypes.byref(v)))
     return v.value
+
+
+def stream_handle() -> int:
+    """cudaStream_t of the library (for CUDA-event timing on the launching stream)."""
+    p = ctypes.c_void_p()
+    check(lib().mb_get_stream(ctypes.byref(p)))
+    return p.value or 0
+
+
+def profile(enable: bool) -> None:
+    check(lib().mb_profile(1 if enable else 0))
+
+
+def profile_report():
+    """{kernel name: (launches, total_ms, algorithmic bytes)} since profile(True)."""
+    cap = 64
+    arr = (MbKernelStat * cap)()
+    cnt = ctypes.c_int()
+    check(lib().mb_profile_report(arr, cap, ctypes.byref(cnt)))
+    return {arr[i].name.decode(): (arr[i].launches, arr[i].total_ms, arr[i].bytes) for i in range(min(cnt.value, cap))}
 
 
 def synchronize() -> None:

@@ -89,6 +89,15 @@ uint64_t& launch_counter();
     }                                                                  \
   } while (0)
 
+// Records a kernel launch in the optional per-kernel profile (CUDA events on `st`).
+// Construct immediately before the launch and let it go out of scope right after.
+struct ProfScope {
+  int slot;
+  cudaStream_t st;
+  ProfScope(const char* name, double bytes, cudaStream_t stream);
+  ~ProfScope();
+};
+
 inline int grid_for(int64_t work, int block, int64_t cap = int64_t(148) * 32) {
   int64_t g = (work + block - 1) / block;
   if (g < 1) g = 1;

@@ -494,7 +494,10 @@ int launch_dense(double2* v, int64_t elems, int nsamples, const Pos& pos, const 
                  int mode, cudaStream_t st) {
   if (nsamples <= 0 || elems == 0) return MB_OK;
   dim3 g = sample_grid(elems >> pos.k, nsamples);
-  MB_DISPATCH_K(pos.k, (k_dense<KK><<<g, kBlock, 0, st>>>(v, elems, pos, mats, mstride, mode)));
+  {
+    ProfScope ps("k_dense", 32.0 * elems * nsamples, st);
+    MB_DISPATCH_K(pos.k, (k_dense<KK><<<g, kBlock, 0, st>>>(v, elems, pos, mats, mstride, mode)));
+  }
   MB_LAUNCHED();
   return MB_OK;
 }
@@ -503,7 +506,10 @@ int launch_diag(double2* v, int64_t elems, int nsamples, const Pos& pos, const d
                 int mode, uint32_t active, cudaStream_t st) {
   if (nsamples <= 0 || elems == 0 || active == 0) return MB_OK;
   dim3 g = sample_grid(elems >> pos.k, nsamples);
-  MB_DISPATCH_K(pos.k, (k_diag<KK><<<g, kBlock, 0, st>>>(v, elems, pos, mats, mstride, mode, active)));
+  {
+    ProfScope ps("k_diag", 32.0 * elems * nsamples * __builtin_popcount(active) / (1 << pos.k), st);
+    MB_DISPATCH_K(pos.k, (k_diag<KK><<<g, kBlock, 0, st>>>(v, elems, pos, mats, mstride, mode, active)));
+  }
   MB_LAUNCHED();
   return MB_OK;
 }
@@ -517,7 +523,10 @@ int launch_monomial(double2* v, int64_t elems, int nsamples, const Pos& pos, con
     if (sigma[a] >= 0) { sg.from[sg.n] = a; sg.to[sg.n] = sigma[a]; ++sg.n; }
   if (sg.n == 0) return MB_OK;
   dim3 g = sample_grid(elems >> pos.k, nsamples);
-  MB_DISPATCH_K(pos.k, (k_monomial<KK><<<g, kBlock, 0, st>>>(v, elems, pos, mats, mstride, mode, sg)));
+  {
+    ProfScope ps("k_monomial", 32.0 * elems * nsamples * sg.n / (1 << pos.k), st);
+    MB_DISPATCH_K(pos.k, (k_monomial<KK><<<g, kBlock, 0, st>>>(v, elems, pos, mats, mstride, mode, sg)));
+  }
   MB_LAUNCHED();
   return MB_OK;
 }
@@ -572,6 +581,7 @@ int launch_cross_dense(const double2* c, const double2* v, int64_t elems, int ns
   if (pos.k == 0) {
     k_cross_scalar<<<g, kBlock, 0, st>>>(c, v, elems, m, ws.partials, ws.counters, ro);
   } else {
+    ProfScope ps("k_cross_dense", (c == v ? 16.0 : 32.0) * elems * nsamples, st);
     MB_DISPATCH_K(pos.k, (k_cross_dense<KK><<<g, kBlock, 0, st>>>(c, v, elems, pos, m, mstride, mode, ws.partials,
                                                                   ws.counters, ro)));
   }
