@@ -1,13 +1,874 @@
-// Fused-pass execution (filled in by the tiled kernels).
-#include "internal.h"
+// Fused-pass execution: gate-stream scheduler (host) and the K1/K2 pass kernels.
+//
+// The reference applies every gate as one full sweep over the state (threaded_short_range.jl,
+// threaded_long_range.jl). Here the compiled circuit is cut into passes; one pass reads and
+// writes the state once and applies every gate it holds:
+//   PASS_TILE (K1)  a tile of 2^t amplitudes (t = 10..12) over the bit set {0,1,2} ∪ H (H a
+//                   window of higher bits) or the low bits {0..t-1}, staged into shared memory
+//                   by TMA (cp.async.bulk.tensor, 128-byte swizzle) and processed in
+//                   register stages of 2^R amplitudes per thread;
+//   PASS_REG  (K2)  a coalesced strided sweep: each thread holds 2^R amplitudes 2^h apart
+//                   (R high bits), warps cover 32 consecutive low indices (512 B per load);
+//   PASS_PLAIN      one plain kernel for an instruction the register stages cannot hold
+//                   (dense gates on 3..5 qubits, 2-qubit channels).
+// Gates are taken into a pass greedily in circuit order; a gate may move ahead of skipped
+// gates only when it commutes with all of them (disjoint non-diagonal supports), so the
+// result equals the sequential product. Density matrices run as 2n-bit vectors: U on the
+// row bits and conj(U) on the column bits, channels as supermatrices.
+#include <cuda.h>
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+
+#include "fused_kernels.cuh"
 
 namespace mb {
-int apply_fused(mb_circuit c, mb_state s, int64_t mrow_stride) { return apply_plain(c, s, mrow_stride); }
-void release_schedules(mb_circuit) {}
+
+namespace {
+
+typedef std::complex<double> cd;
+constexpr int kThreadsMax = 256;
+
+// ---------------------------------------------------------------------------------------------
+// Kernels
+// ---------------------------------------------------------------------------------------------
+template <int R> struct TileBounds;
+template <> struct TileBounds<4> { static constexpr int threads = 256, blocks = 1; };
+template <> struct TileBounds<5> { static constexpr int threads = 128, blocks = 1; };
+
+template <int R, bool U2>
+__global__ void __launch_bounds__(TileBounds<R>::threads, TileBounds<R>::blocks)
+    k_tile_pass(const __grid_constant__ CUtensorMap tmap, const TileArgs a) {
+  // Two tile buffers: while the CTA works on tile i in one buffer, TMA stores tile i-1 and
+  // loads tile i+1 through the other.
+  extern __shared__ unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ int s_abort;
+  double2* buf0 = reinterpret_cast<double2*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  double2* bufs[2] = {buf0, buf0 + (size_t(1) << a.t)};
+  const uint32_t tile_bytes = 16u << a.t;
+  if (threadIdx.x == 0) {
+    fk::mbar_init(&bar[0], 1);
+    fk::mbar_init(&bar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    s_abort = 0;
+  }
+  __syncthreads();
+  // Tile geometry: global base index (zeros at the tile bits) and TMA coordinates.
+  auto geometry = [&](int64_t tile, int* c, uint64_t* gbase, int* sample) {
+    const int b = int(tile / a.tiles_per_sample);
+    uint64_t base = uint64_t(tile - int64_t(b) * a.tiles_per_sample);
+    for (int q = 0; q < a.t; ++q) {
+      const int p = a.bits[q];
+      const uint64_t low = base & ((uint64_t(1) << p) - 1);
+      base = ((base >> p) << (p + 1)) | low;
+    }
+    for (int d = 0; d < a.ndims; ++d) {
+      if (a.start[d] < 0) c[d] = b;
+      else if (d == 0) c[d] = int(2 * (base & ((uint64_t(1) << a.extb[0]) - 1)));
+      else c[d] = int((base >> a.start[d]) & ((uint64_t(1) << a.extb[d]) - 1));
+    }
+    *gbase = base;
+    *sample = b;
+  };
+  uint32_t phase[2] = {0u, 0u};
+  int64_t tile = blockIdx.x;
+  if (threadIdx.x == 0 && tile < a.ntiles) {
+    int c[5];
+    uint64_t gb;
+    int b;
+    geometry(tile, c, &gb, &b);
+    fk::mbar_expect_tx(&bar[0], tile_bytes);
+    fk::tma_load(&tmap, bufs[0], &bar[0], a.ndims, c);
+  }
+  for (int it = 0; tile < a.ntiles; ++it, tile += gridDim.x) {
+    const int cur = it & 1;
+    const int64_t next = tile + gridDim.x;
+    if (threadIdx.x == 0 && next < a.ntiles) {
+      int c[5];
+      uint64_t gb;
+      int b;
+      geometry(next, c, &gb, &b);
+      fk::bulk_wait_read();  // the store that last used the other buffer has read it
+      fk::mbar_expect_tx(&bar[cur ^ 1], tile_bytes);
+      fk::tma_load(&tmap, bufs[cur ^ 1], &bar[cur ^ 1], a.ndims, c);
+    }
+    int c[5];
+    uint64_t base;
+    int b;
+    geometry(tile, c, &base, &b);
+    double2* tl = bufs[cur];
+    if (!fk::mbar_wait(&bar[cur], phase[cur])) {
+      atomicOr(a.err, 1u);
+      s_abort = 1;
+    }
+    phase[cur] ^= 1u;
+    __syncthreads();
+    if (s_abort) break;
+    for (int s = 0; s < a.nstages; ++s) {
+      const StageDesc& sd = a.stages[s];
+      int reg[kMaxRegBits];
+#pragma unroll
+      for (int k = 0; k < R; ++k) reg[k] = sd.reg[k];
+      uint32_t lbase = 0;
+      for (int q = 0; q < sd.ntid; ++q) lbase |= ((threadIdx.x >> q) & 1u) << sd.tid[q];
+      double2 v[1 << R];
+#pragma unroll
+      for (int j = 0; j < (1 << R); ++j) v[j] = tl[fk::swz(lbase | uint32_t(fk::reg_offset<R>(j, reg)))];
+      fk::run_mops<R, U2>(v, a.mops + sd.op0, sd.nops, lbase, reg, base, a.table, a.tstride, b);
+#pragma unroll
+      for (int j = 0; j < (1 << R); ++j) tl[fk::swz(lbase | uint32_t(fk::reg_offset<R>(j, reg)))] = v[j];
+      __syncthreads();
+    }
+    fk::fence_async_smem();
+    __syncthreads();
+    if (threadIdx.x == 0) fk::tma_store(&tmap, tl, a.ndims, c);
+  }
+  if (threadIdx.x == 0) fk::bulk_wait_all();
+}
+
+template <int R, bool U2>
+__global__ void __launch_bounds__(128) k_reg_pass(double2* __restrict__ v, const RegArgs a) {
+  int reg[kMaxRegBits];
+#pragma unroll
+  for (int k = 0; k < R; ++k) reg[k] = a.reg[k];
+  const int64_t total = a.groups * a.nsamples;
+  for (int64_t g = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; g < total; g += int64_t(gridDim.x) * blockDim.x) {
+    const int b = int(g / a.groups);
+    uint64_t base = uint64_t(g - int64_t(b) * a.groups);
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+      const int p = reg[k];
+      const uint64_t low = base & ((uint64_t(1) << p) - 1);
+      base = ((base >> p) << (p + 1)) | low;
+    }
+    double2* vs = v + (int64_t(b) << a.N);
+    double2 x[1 << R];
+#pragma unroll
+    for (int j = 0; j < (1 << R); ++j) x[j] = vs[base | fk::reg_offset<R>(j, reg)];
+    fk::run_mops<R, U2>(x, a.mops, a.nops, base, reg, 0, a.table, a.tstride, b);
+#pragma unroll
+    for (int j = 0; j < (1 << R); ++j) vs[base | fk::reg_offset<R>(j, reg)] = x[j];
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Host: fused ops
+// ---------------------------------------------------------------------------------------------
+enum { F_UNFUSABLE = -1 };
+
+}  // namespace
+
+struct FOp {
+  int type = F_UNFUSABLE;     // MopType or F_UNFUSABLE
+  int nb = 0;                 // bits of the (ordered) local matrix
+  int bits[10] = {0};         // global bit of local bit j
+  uint64_t all = 0, nd = 0;   // all bits / non-diagonal (target) bits
+  int tgt[2] = {0, 0};
+  int ntgt = 0;
+  int ctrl[4] = {0};
+  int nctrl = 0;
+  int off[16] = {0};
+  uint32_t active = 0;
+  int conj = 0, param = 0;
+  // plain fallback
+  int cls = CLS_DENSE;
+  int mat_off = 0, mode = MAT_PLAIN;
+  uint32_t pactive = 0;
+  int sigma[32];
+  int d = 1;
+};
+
+struct Schedule {
+  int N = 0, dm = 0, t = 0, R = 0, nsamples = 1;
+  bool dagger = false;
+  std::vector<FOp> fops;
+  std::vector<Pass> passes;
+  StageDesc* d_stages = nullptr;
+  MOp* d_mops = nullptr;
+};
+
+namespace {
+
+static bool is_one(double2 x) { return x.x == 1.0 && x.y == 0.0; }
+static bool is_zero(double2 x) { return x.x == 0.0 && x.y == 0.0; }
+
+// Controlled single-target structure of a fixed ordered matrix: identity unless every
+// bit other than `tj` is 1. Returns the target local bit or -1.
+static int controlled_target(const double2* M, int k) {
+  const int d = 1 << k;
+  for (int tj = 0; tj < k; ++tj) {
+    const int tb = 1 << tj, cm = (d - 1) & ~tb;
+    bool ok = true;
+    for (int r = 0; r < d && ok; ++r)
+      for (int c = 0; c < d && ok; ++c) {
+        const double2 x = M[r + c * d];
+        if ((r & ~tb) != (c & ~tb)) ok = is_zero(x);
+        else if ((r & cm) != cm) ok = (r == c) ? is_one(x) : is_zero(x);
+      }
+    if (ok) return tj;
+  }
+  return -1;
+}
+
+static void finalize_masks(FOp& f) {
+  f.all = 0;
+  for (int j = 0; j < f.nb; ++j) f.all |= uint64_t(1) << f.bits[j];
+  f.nd = 0;
+  for (int j = 0; j < f.ntgt; ++j) f.nd |= uint64_t(1) << f.tgt[j];
+}
+
+// Fused op of one gate half (row bits or, with conj, column bits of a density matrix).
+static FOp gate_fop(mb_circuit c, const COp& op, int shift, int conj, bool dagger) {
+  FOp f;
+  f.nb = op.k;
+  for (int j = 0; j < op.k; ++j) f.bits[j] = op.pos[j] + shift;
+  f.conj = conj;
+  f.param = op.parametric ? 1 : 0;
+  f.mat_off = op.mat_off;
+  f.d = 1 << op.k;
+  f.cls = op.cls;
+  f.pactive = op.active;
+  std::memcpy(f.sigma, dagger ? op.sigma_inv : op.sigma, sizeof(f.sigma));
+  f.mode = dagger ? (conj ? MAT_TRANSPOSE : MAT_ADJOINT) : (conj ? MAT_CONJ : MAT_PLAIN);
+  const int d = f.d;
+  // Element (r, c) of the effective matrix (U, conj U, U' or U^T) as a table offset; the
+  // conj flag is toggled for the adjoint.
+  auto off = [&](int r, int cc) { return dagger ? op.mat_off + cc + r * d : op.mat_off + r + cc * d; };
+  const int fconj = dagger ? !conj : conj;
+  if (op.k == 0) return f;  // global scalar: plain path
+  if (op.cls == CLS_DIAG) {
+    if (op.k > 3) return f;
+    f.type = MOP_DIAG;
+    for (int a = 0; a < d; ++a) f.off[a] = off(a, a);
+    f.active = op.active;
+    f.conj = fconj;
+    finalize_masks(f);
+    return f;
+  }
+  int tj = -1;
+  bool is_x = false;
+  if (op.parametric) {
+    if (op.family == MB_FAM_CRX || op.family == MB_FAM_CRY) {
+      for (int j = 0; j < op.k; ++j) {
+        // the target is the bit that carries own-order bit 1 (second position)
+        const BindRec* br = nullptr;
+        for (auto& r : c->binds)
+          if (r.mat_off == op.mat_off) br = &r;
+        if (br && br->perm[1 << j] == 2) tj = j;
+      }
+    }
+  } else if (op.k >= 2) {
+    tj = controlled_target(c->fixed_table.data() + op.mat_off, op.k);
+  }
+  if (op.k == 1) tj = 0;
+  if (tj >= 0) {
+    const int tb = 1 << tj, cm = (d - 1) & ~tb;
+    f.tgt[0] = f.bits[tj];
+    f.ntgt = 1;
+    for (int j = 0; j < op.k; ++j)
+      if (j != tj) f.ctrl[f.nctrl++] = f.bits[j];
+    f.off[0] = off(cm, cm);
+    f.off[1] = off(cm | tb, cm);
+    f.off[2] = off(cm, cm | tb);
+    f.off[3] = off(cm | tb, cm | tb);
+    if (!op.parametric) {
+      const double2* M = c->fixed_table.data();
+      is_x = is_zero(M[f.off[0]]) && is_one(M[f.off[1]]) && is_one(M[f.off[2]]) && is_zero(M[f.off[3]]);
+    }
+    f.type = is_x ? MOP_CTRLX : (f.nctrl ? MOP_CTRL : MOP_U1);
+    if (f.nctrl > 4) f.type = F_UNFUSABLE;
+    f.conj = fconj;
+    finalize_masks(f);
+    return f;
+  }
+  if (op.k == 2) {
+    f.type = MOP_U2;
+    for (int r = 0; r < 4; ++r)
+      for (int cc = 0; cc < 4; ++cc) f.off[r + 4 * cc] = off(r, cc);
+    f.tgt[0] = f.bits[0];
+    f.tgt[1] = f.bits[1];
+    f.ntgt = 2;
+    f.conj = fconj;
+    finalize_masks(f);
+  }
+  return f;
+}
+
+// Unfusable ops act densely on all their bits.
+static void mark_unfusable_masks(FOp& f) {
+  if (f.type != F_UNFUSABLE) return;
+  f.all = 0;
+  for (int j = 0; j < f.nb; ++j) f.all |= uint64_t(1) << f.bits[j];
+  f.nd = f.all;
+}
+
+static void build_fops(mb_circuit c, int n, int dm, bool dagger, std::vector<FOp>& out) {
+  out.clear();
+  std::vector<FOp> seq;
+  for (const COp& op : c->ops) {
+    if (op.kind == MB_OP_CHANNEL) {
+      FOp f;
+      f.nb = 2 * op.k;
+      for (int j = 0; j < op.k; ++j) {
+        f.bits[j] = op.pos[j];
+        f.bits[j + op.k] = op.pos[j] + n;
+      }
+      f.mat_off = op.mat_off;
+      f.d = 1 << f.nb;
+      f.cls = CLS_DENSE;
+      f.mode = dagger ? MAT_ADJOINT : MAT_PLAIN;
+      if (op.k == 1) {
+        f.type = MOP_U2;
+        for (int r = 0; r < 4; ++r)
+          for (int cc = 0; cc < 4; ++cc) f.off[r + 4 * cc] = dagger ? op.mat_off + cc + 4 * r : op.mat_off + r + 4 * cc;
+        f.conj = dagger ? 1 : 0;
+        f.tgt[0] = f.bits[0];
+        f.tgt[1] = f.bits[1];
+        f.ntgt = 2;
+        finalize_masks(f);
+      }
+      seq.push_back(f);
+      continue;
+    }
+    seq.push_back(gate_fop(c, op, 0, 0, dagger));
+    if (dm) seq.push_back(gate_fop(c, op, n, 1, dagger));
+  }
+  for (FOp& f : seq) mark_unfusable_masks(f);
+  if (dagger) std::reverse(seq.begin(), seq.end());
+  out = seq;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Host: pass scheduler
+// ---------------------------------------------------------------------------------------------
+struct Cand {
+  int kind;
+  std::vector<int> bits;  // sorted global bits
+};
+
+static uint64_t mask_of(const std::vector<int>& b) {
+  uint64_t m = 0;
+  for (int x : b) m |= uint64_t(1) << x;
+  return m;
+}
+
+// Greedy take: ops that fit `tmask` and commute with every op skipped before them.
+static std::vector<int> take_ops(const std::vector<FOp>& fops, const std::vector<int>& rem, uint64_t tmask,
+                                 uint64_t full, double* score) {
+  std::vector<int> taken;
+  uint64_t b_all = 0, b_nd = 0;
+  double sc = 0;
+  const size_t limit = std::min<size_t>(rem.size(), 8192);
+  for (size_t i = 0; i < limit; ++i) {
+    const FOp& f = fops[rem[i]];
+    const bool fits = f.type != F_UNFUSABLE && (f.nd & ~tmask) == 0;
+    const bool comm = (f.nd & b_all) == 0 && (f.all & b_nd) == 0;
+    if (fits && comm) {
+      taken.push_back(rem[i]);
+      sc += f.type == MOP_DIAG ? 0.25 : (f.type == MOP_U2 ? 2.0 : 1.0);
+    } else {
+      b_all |= f.all;
+      b_nd |= f.nd;
+      if ((b_nd & full) == full) break;
+    }
+  }
+  if (score) *score = sc;
+  return taken;
+}
+
+// Dimension chunks of a tile's bit set for the TMA tensor map (dim 0 = bits 0..2).
+static bool tile_geom(const std::vector<int>& bits, int N, int nsamples, TmaGeom& g) {
+  std::vector<std::pair<int, int>> chunks;  // (start, len)
+  chunks.push_back({0, 3});
+  size_t i = 3;
+  while (i < bits.size()) {
+    int s = bits[i], len = 1;
+    while (i + len < bits.size() && bits[i + len] == s + len && len < 8) ++len;
+    chunks.push_back({s, len});
+    i += len;
+  }
+  const int nd = int(chunks.size()) + (nsamples > 1 ? 1 : 0);
+  if (nd > 5) return false;
+  g.ndims = nd;
+  for (size_t d = 0; d < chunks.size(); ++d) {
+    const int next = d + 1 < chunks.size() ? chunks[d + 1].first : N;
+    g.start[d] = chunks[d].first;
+    g.bits[d] = next - chunks[d].first;
+    g.boxb[d] = chunks[d].second;
+  }
+  if (nsamples > 1) {
+    g.start[chunks.size()] = -1;
+    g.bits[chunks.size()] = 0;
+    g.boxb[chunks.size()] = 0;
+  }
+  return true;
+}
+
+// Register stages of a tile pass: every stage loads 2^R amplitudes per thread over R
+// tile-local bits and applies the ops whose targets lie among them.
+static void plan_stages(const std::vector<FOp>& fops, const std::vector<int>& ops, Pass& p, int R) {
+  const int t = p.t;
+  std::vector<int> loc(64, -1);
+  for (int i = 0; i < t; ++i) loc[p.bits[i]] = i;
+  auto lmask = [&](uint64_t gm) {
+    uint64_t m = 0;
+    for (int g = 0; g < 64; ++g)
+      if ((gm >> g) & 1) m |= uint64_t(1) << loc[g];
+    return m;
+  };
+  std::vector<int> rem = ops;
+  while (!rem.empty()) {
+    std::vector<int> regs;
+    uint64_t rmask = 0, b_all = 0, b_nd = 0;
+    for (int idx : rem) {
+      const FOp& f = fops[idx];
+      const uint64_t need = lmask(f.nd) & ~rmask;
+      const bool comm = (lmask(f.nd) & b_all) == 0 && (lmask(f.all & mask_of(p.bits)) & b_nd) == 0;
+      if (comm && int(regs.size()) + __builtin_popcountll(need) <= R) {
+        for (int q = 0; q < t; ++q)
+          if ((need >> q) & 1) regs.push_back(q);
+        rmask |= need;
+      } else {
+        b_all |= lmask(f.all & mask_of(p.bits));
+        b_nd |= lmask(f.nd);
+      }
+      if (int(regs.size()) == R) break;
+    }
+    // Fill the register set with bank-neutral high bits first.
+    for (int q = t - 1; q >= 0 && int(regs.size()) < R; --q)
+      if (!((rmask >> q) & 1) && q >= 6) {
+        regs.push_back(q);
+        rmask |= uint64_t(1) << q;
+      }
+    for (int q = 0; q < t && int(regs.size()) < R; ++q)
+      if (!((rmask >> q) & 1)) {
+        regs.push_back(q);
+        rmask |= uint64_t(1) << q;
+      }
+    // Take the ops that fit.
+    std::vector<int> taken, left;
+    b_all = b_nd = 0;
+    for (int idx : rem) {
+      const FOp& f = fops[idx];
+      const uint64_t nd = lmask(f.nd), al = lmask(f.all & mask_of(p.bits)) | nd;
+      const bool comm = (nd & b_all) == 0 && (al & b_nd) == 0;
+      if ((nd & ~rmask) == 0 && comm) {
+        taken.push_back(idx);
+      } else {
+        left.push_back(idx);
+        b_all |= al;
+        b_nd |= nd;
+      }
+    }
+    // Lanes: three non-register bits among 0..5 with distinct residues mod 3 keep the
+    // swizzled shared-memory accesses free of bank conflicts.
+    StageDesc sd{};
+    sd.nreg = R;
+    for (int k = 0; k < R; ++k) sd.reg[k] = regs[k];
+    std::vector<int> tidb;
+    bool used_res[3] = {false, false, false};
+    for (int q = 0; q < 6 && q < t && int(tidb.size()) < 3; ++q)
+      if (!((rmask >> q) & 1) && !used_res[q % 3]) {
+        tidb.push_back(q);
+        used_res[q % 3] = true;
+      }
+    for (int q = 0; q < t; ++q)
+      if (!((rmask >> q) & 1) && std::find(tidb.begin(), tidb.end(), q) == tidb.end()) tidb.push_back(q);
+    sd.ntid = int(tidb.size());
+    for (int q = 0; q < sd.ntid; ++q) sd.tid[q] = tidb[q];
+    sd.op0 = int(p.mops.size());
+    for (int idx : taken) {
+      const FOp& f = fops[idx];
+      MOp m{};
+      m.type = int16_t(f.type);
+      m.conj = int16_t(f.conj);
+      m.param = int16_t(f.param);
+      std::memcpy(m.off, f.off, sizeof(m.off));
+      auto regidx = [&](int gbit) {
+        for (int k = 0; k < R; ++k)
+          if (regs[k] == loc[gbit]) return k;
+        return -1;
+      };
+      auto sel = [&](int gbit) { return int16_t(loc[gbit] >= 0 ? loc[gbit] : 64 + gbit); };
+      if (f.type == MOP_U2) {
+        int ra = regidx(f.tgt[0]), rb = regidx(f.tgt[1]);
+        if (ra > rb) {
+          // swap the local bits of the 4x4 matrix so that local bit 0 is the lower register
+          int o2[16];
+          const int sw[4] = {0, 2, 1, 3};
+          for (int r = 0; r < 4; ++r)
+            for (int cc = 0; cc < 4; ++cc) o2[r + 4 * cc] = f.off[sw[r] + 4 * sw[cc]];
+          std::memcpy(m.off, o2, sizeof(o2));
+          std::swap(ra, rb);
+        }
+        m.r0 = int16_t(ra);
+        m.r1 = int16_t(rb);
+      } else if (f.type == MOP_DIAG) {
+        m.nsel = int16_t(f.nb);
+        for (int j = 0; j < f.nb; ++j) m.sel[j] = sel(f.bits[j]);
+        m.active = f.active;
+      } else {
+        m.r0 = int16_t(regidx(f.tgt[0]));
+        m.nsel = int16_t(f.nctrl);
+        for (int j = 0; j < f.nctrl; ++j) m.sel[j] = sel(f.ctrl[j]);
+      }
+      p.mops.push_back(m);
+    }
+    sd.nops = int(taken.size());
+    p.stages.push_back(sd);
+    rem.swap(left);
+  }
+}
+
+static void encode_reg_pass(const std::vector<FOp>& fops, const std::vector<int>& ops, Pass& p) {
+  const int R = p.t;
+  StageDesc sd{};
+  sd.nreg = R;
+  for (int k = 0; k < R; ++k) sd.reg[k] = p.bits[k];
+  sd.op0 = 0;
+  for (int idx : ops) {
+    const FOp& f = fops[idx];
+    MOp m{};
+    m.type = int16_t(f.type);
+    m.conj = int16_t(f.conj);
+    m.param = int16_t(f.param);
+    std::memcpy(m.off, f.off, sizeof(m.off));
+    auto regidx = [&](int gbit) {
+      for (int k = 0; k < R; ++k)
+        if (p.bits[k] == gbit) return k;
+      return -1;
+    };
+    if (f.type == MOP_U2) {
+      int ra = regidx(f.tgt[0]), rb = regidx(f.tgt[1]);
+      if (ra > rb) {
+        int o2[16];
+        const int sw[4] = {0, 2, 1, 3};
+        for (int r = 0; r < 4; ++r)
+          for (int cc = 0; cc < 4; ++cc) o2[r + 4 * cc] = f.off[sw[r] + 4 * sw[cc]];
+        std::memcpy(m.off, o2, sizeof(o2));
+        std::swap(ra, rb);
+      }
+      m.r0 = int16_t(ra);
+      m.r1 = int16_t(rb);
+    } else if (f.type == MOP_DIAG) {
+      m.nsel = int16_t(f.nb);
+      for (int j = 0; j < f.nb; ++j) m.sel[j] = int16_t(f.bits[j]);
+      m.active = f.active;
+    } else {
+      m.r0 = int16_t(regidx(f.tgt[0]));
+      m.nsel = int16_t(f.nctrl);
+      for (int j = 0; j < f.nctrl; ++j) m.sel[j] = int16_t(f.ctrl[j]);
+    }
+    p.mops.push_back(m);
+  }
+  sd.nops = int(ops.size());
+  p.stages.push_back(sd);
+}
+
+static std::vector<int> window(int lo, int len, int N) {
+  std::vector<int> w;
+  for (int q = lo; q < lo + len && q < N; ++q) w.push_back(q);
+  return w;
+}
+
+static void build_schedule(Schedule& S, int nsamples) {
+  const int N = S.N, t = std::min(S.t, N), R = S.R;
+  const uint64_t full = N >= 64 ? ~uint64_t(0) : ((uint64_t(1) << N) - 1);
+  std::vector<int> rem(S.fops.size());
+  for (size_t i = 0; i < rem.size(); ++i) rem[i] = int(i);
+  S.passes.clear();
+  while (!rem.empty()) {
+    const FOp& f0 = S.fops[rem[0]];
+    if (f0.type == F_UNFUSABLE) {
+      Pass p;
+      p.kind = PASS_PLAIN;
+      p.plain_fop = rem[0];
+      S.passes.push_back(p);
+      rem.erase(rem.begin());
+      continue;
+    }
+    std::vector<Cand> cands;
+    cands.push_back({PASS_TILE, window(0, t, N)});
+    if (N > t) {
+      // first target bit not coverable by the low tile, in circuit order
+      int h0 = -1;
+      for (int idx : rem) {
+        const FOp& f = S.fops[idx];
+        for (int j = 0; j < f.ntgt && h0 < 0; ++j)
+          if (f.tgt[j] >= t) h0 = f.tgt[j];
+        if (h0 >= 0) break;
+      }
+      if (h0 >= 0) {
+        const int w = t - 3;
+        for (int lo : {std::min(h0, N - w), std::max(3, h0 - w + 1)}) {
+          lo = std::max(3, std::min(lo, N - w));
+          std::vector<int> b = {0, 1, 2};
+          for (int q : window(lo, w, N)) b.push_back(q);
+          cands.push_back({PASS_TILE, b});
+        }
+        const int rlo = std::max(5, std::min(h0, N - R));
+        if (N - 5 >= R) cands.push_back({PASS_REG, window(rlo, R, N)});
+      }
+    }
+    double best = -1;
+    int bi = -1;
+    std::vector<int> best_taken;
+    TmaGeom bg{};
+    for (size_t ci = 0; ci < cands.size(); ++ci) {
+      TmaGeom g{};
+      if (cands[ci].kind == PASS_TILE && !tile_geom(cands[ci].bits, N, nsamples, g)) continue;
+      double sc;
+      auto tk = take_ops(S.fops, rem, mask_of(cands[ci].bits), full, &sc);
+      if (cands[ci].kind == PASS_REG) sc *= 0.999;  // prefer the wider tile on ties
+      if (sc > best) {
+        best = sc;
+        bi = int(ci);
+        best_taken = tk;
+        bg = g;
+      }
+    }
+    Pass p;
+    p.kind = cands[bi].kind;
+    p.bits = cands[bi].bits;
+    p.t = int(p.bits.size());
+    p.geom = bg;
+    if (p.kind == PASS_TILE) plan_stages(S.fops, best_taken, p, R);
+    else encode_reg_pass(S.fops, best_taken, p);
+    for (const MOp& m : p.mops) p.has_u2 |= m.type == MOP_U2;
+    S.passes.push_back(p);
+    std::vector<int> left;
+    size_t k = 0;
+    for (int idx : rem) {
+      if (k < best_taken.size() && best_taken[k] == idx) ++k;
+      else left.push_back(idx);
+    }
+    rem.swap(left);
+  }
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    cudaDriverEntryPointQueryResult q;
+    void* p = nullptr;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
+static int make_tmap(const Pass& p, double2* base, int N, int nsamples, CUtensorMap* map) {
+  EncodeTiledFn enc = encode_fn();
+  if (!enc) {
+    set_error("cuTensorMapEncodeTiled is unavailable");
+    return MB_EDEVICE;
+  }
+  const TmaGeom& g = p.geom;
+  cuuint64_t dims[5], strides[4];
+  cuuint32_t box[5], estr[5] = {1, 1, 1, 1, 1};
+  for (int d = 0; d < g.ndims; ++d) {
+    if (g.start[d] < 0) {
+      dims[d] = cuuint64_t(nsamples);
+      box[d] = 1;
+      if (d > 0) strides[d - 1] = cuuint64_t(16) << N;
+      continue;
+    }
+    dims[d] = d == 0 ? (cuuint64_t(2) << g.bits[0]) : (cuuint64_t(1) << g.bits[d]);
+    box[d] = d == 0 ? 16u : (1u << g.boxb[d]);
+    if (d > 0) strides[d - 1] = cuuint64_t(16) << g.start[d];
+  }
+  CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, g.ndims, base, dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_error("cuTensorMapEncodeTiled failed (%d) for a %d-dim tile", int(r), g.ndims);
+    return MB_EDEVICE;
+  }
+  return MB_OK;
+}
+
+static int plain_fop_launch(mb_circuit c, const FOp& f, double2* v, int64_t elems, int nsamples, int64_t mstride,
+                            cudaStream_t st) {
+  Pos p{};
+  p.k = f.nb;
+  for (int j = 0; j < f.nb; ++j) p.p[j] = f.bits[j];
+  const double2* m = c->d_table + f.mat_off;
+  const int64_t ms = f.param ? mstride : 0;
+  if (f.nb == 0) return MB_EUNSUPPORTED;
+  if (f.cls == CLS_DIAG) return launch_diag(v, elems, nsamples, p, m, ms, f.mode, f.pactive, st);
+  if (f.cls == CLS_MONO) return launch_monomial(v, elems, nsamples, p, m, ms, f.mode, f.sigma, f.d, st);
+  return launch_dense(v, elems, nsamples, p, m, ms, f.mode, st);
+}
+
+// Tile bits and register bits of the fused schedule. MB_TILE_BITS / MB_REG_BITS override
+// the defaults (the autotuner sets them per register size).
+struct Tuning {
+  int t = 12, R = 4;
+};
+
+static Tuning tuning_for(int N) {
+  Tuning tu;
+  if (const char* e = getenv("MB_TILE_BITS")) tu.t = std::max(8, std::min(12, atoi(e)));
+  if (const char* e = getenv("MB_REG_BITS")) tu.R = atoi(e) == 5 ? 5 : 4;
+  tu.t = std::min(tu.t, N);
+  return tu;
+}
+
+}  // namespace
+
+int get_schedule(mb_circuit c, int n, int dm, bool dagger, int nsamples, Schedule** out) {
+  const int N = dm ? 2 * n : n;
+  Tuning tu = tuning_for(N);
+  for (Schedule* s : c->scheds)
+    if (s->N == N && s->dm == dm && s->dagger == dagger && s->t == tu.t && s->R == tu.R && s->nsamples == nsamples) {
+      *out = s;
+      return MB_OK;
+    }
+  std::unique_ptr<Schedule> S(new Schedule());
+  S->N = N;
+  S->dm = dm;
+  S->t = tu.t;
+  S->R = tu.R;
+  S->dagger = dagger;
+  S->nsamples = nsamples;
+  build_fops(c, n, dm, dagger, S->fops);
+  build_schedule(*S, nsamples);
+  std::vector<StageDesc> st;
+  std::vector<MOp> mo;
+  for (Pass& p : S->passes) {
+    p.stage_off = int(st.size());
+    p.mop_off = int(mo.size());
+    for (StageDesc sd : p.stages) {
+      sd.op0 += p.mop_off;
+      st.push_back(sd);
+    }
+    mo.insert(mo.end(), p.mops.begin(), p.mops.end());
+  }
+  int rc;
+  if (!st.empty()) {
+    if ((rc = dev_alloc((void**)&S->d_stages, sizeof(StageDesc) * st.size()))) return rc;
+    MB_CHECK_CUDA(cudaMemcpyAsync(S->d_stages, st.data(), sizeof(StageDesc) * st.size(), cudaMemcpyHostToDevice,
+                                  g_ctx.stream));
+  }
+  if (!mo.empty()) {
+    if ((rc = dev_alloc((void**)&S->d_mops, sizeof(MOp) * mo.size()))) return rc;
+    MB_CHECK_CUDA(cudaMemcpyAsync(S->d_mops, mo.data(), sizeof(MOp) * mo.size(), cudaMemcpyHostToDevice, g_ctx.stream));
+  }
+  MB_CHECK_CUDA(cudaStreamSynchronize(g_ctx.stream));
+  *out = S.get();
+  c->scheds.push_back(S.release());
+  return MB_OK;
+}
+
+int run_schedule(mb_circuit c, Schedule* S, double2* v, int nsamples, int64_t mstride) {
+  cudaStream_t st = g_ctx.stream;
+  const int N = S->N;
+  const int64_t elems = int64_t(1) << N;
+  for (const Pass& p : S->passes) {
+    int rc = MB_OK;
+    if (p.kind == PASS_PLAIN) {
+      rc = plain_fop_launch(c, S->fops[p.plain_fop], v, elems, nsamples, mstride, st);
+    } else if (p.kind == PASS_TILE) {
+      CUtensorMap map;
+      if ((rc = make_tmap(p, v, N, nsamples, &map))) return rc;
+      TileArgs a{};
+      a.t = p.t;
+      a.nstages = int(p.stages.size());
+      a.ndims = p.geom.ndims;
+      for (int d = 0; d < 5; ++d) {
+        a.start[d] = p.geom.start[d];
+        a.extb[d] = p.geom.bits[d];
+      }
+      for (int i = 0; i < p.t; ++i) a.bits[i] = p.bits[i];
+      a.tiles_per_sample = int64_t(1) << (N - p.t);
+      a.ntiles = a.tiles_per_sample * nsamples;
+      a.tstride = mstride;
+      a.stages = S->d_stages + p.stage_off;
+      a.mops = S->d_mops;
+      a.table = c->d_table;
+      a.err = g_ctx.flags + 2;
+      const int threads = 1 << (p.t - S->R);
+      const size_t shm = (size_t(32) << p.t) + 1024;  // two tile buffers + alignment slack
+      const int per_sm = std::max(1, int((227 * 1024) / (shm + 256)));
+      const int64_t grid = std::min<int64_t>(a.ntiles, int64_t(g_ctx.sm_count) * std::min(per_sm, 4));
+      ProfScope ps("k_tile_pass", 32.0 * double(elems) * nsamples, st);
+      const bool u2 = p.has_u2;
+      auto launch = [&](auto kern) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm));
+        kern<<<dim3(unsigned(grid)), threads, shm, st>>>(map, a);
+      };
+      if (S->R == 5) u2 ? launch(k_tile_pass<5, true>) : launch(k_tile_pass<5, false>);
+      else u2 ? launch(k_tile_pass<4, true>) : launch(k_tile_pass<4, false>);
+      MB_LAUNCHED();
+    } else {
+      RegArgs a{};
+      a.nbits = p.t;
+      for (int k = 0; k < p.t; ++k) a.reg[k] = p.bits[k];
+      a.N = N;
+      a.groups = int64_t(1) << (N - p.t);
+      a.nsamples = nsamples;
+      a.nops = p.stages[0].nops;
+      a.tstride = mstride;
+      a.mops = S->d_mops + p.mop_off;
+      a.table = c->d_table;
+      const int64_t work = a.groups * nsamples;
+      const int block = 128;
+      const int grid = grid_for(work, block, int64_t(g_ctx.sm_count) * 16);
+      ProfScope ps("k_reg_pass", 32.0 * double(elems) * nsamples, st);
+      if (p.t == 5) p.has_u2 ? k_reg_pass<5, true><<<grid, block, 0, st>>>(v, a)
+                             : k_reg_pass<5, false><<<grid, block, 0, st>>>(v, a);
+      else p.has_u2 ? k_reg_pass<4, true><<<grid, block, 0, st>>>(v, a) : k_reg_pass<4, false><<<grid, block, 0, st>>>(v, a);
+      MB_LAUNCHED();
+    }
+    if (rc) return rc;
+  }
+  return MB_OK;
+}
+
+int apply_fused(mb_circuit c, mb_state s, int64_t mrow_stride) {
+  const int dm = s->kind == MB_DENSITY || s->kind == MB_BATCH_DENSITY;
+  const int N = dm ? 2 * s->n : s->n;
+  if (N < 8) return apply_plain(c, s, mrow_stride);
+  for (const COp& op : c->ops)
+    if (op.kind == MB_OP_GATE && op.k == 0) return apply_plain(c, s, mrow_stride);
+  Schedule* S = nullptr;
+  int rc = get_schedule(c, s->n, dm, false, s->batch, &S);
+  if (rc) return rc;
+  return run_schedule(c, S, s->d, s->batch, mrow_stride);
+}
+
+void release_schedules(mb_circuit c) {
+  for (Schedule* s : c->scheds) {
+    dev_free(s->d_stages);
+    dev_free(s->d_mops);
+    delete s;
+  }
+  c->scheds.clear();
+}
+
 }  // namespace mb
 
 extern "C" int mb_circuit_passes(mb_circuit c, int* npasses) {
+  std::lock_guard<std::recursive_mutex> lk(mb::g_mu);
+  if (int rc = mb::check_init()) return rc;
   if (!c || !npasses) return MB_EINVAL;
-  *npasses = int(c->ops.size());
+  mb::Schedule* S = nullptr;
+  if (c->n < 8) {
+    *npasses = int(c->ops.size());
+    return MB_OK;
+  }
+  int rc = mb::get_schedule(c, c->n, 0, false, 1, &S);
+  if (rc) return rc;
+  *npasses = int(S->passes.size());
   return MB_OK;
 }

@@ -1,0 +1,63 @@
+// Fused-pass schedule shared by the host scheduler (fused.cu) and the pass kernels.
+#pragma once
+#include <cstdint>
+#include <vector>
+
+#include "internal.h"
+
+namespace mb {
+
+// Micro-op types executed on amplitudes held in registers.
+enum MopType : int16_t {
+  MOP_U1 = 0,     // dense 2x2 on register bit r0
+  MOP_CTRL = 1,   // 2x2 on register bit r0 where every control bit is 1
+  MOP_CTRLX = 2,  // swap on register bit r0 where every control bit is 1 (CNOT, TOFFOLI, X)
+  MOP_U2 = 3,     // dense 4x4 on register bits r0 < r1 (local bit 0 = r0)
+  MOP_DIAG = 4,   // diagonal on up to 3 bits anywhere: factor of local index a where active
+};
+
+// A selector names one index bit: values < 64 are bits of the pass-local amplitude index,
+// values >= 64 are bit (sel - 64) of the tile's global base index (constant per tile).
+struct MOp {
+  int16_t type, r0, r1, nsel;
+  int16_t sel[4];
+  uint32_t active;   // MOP_DIAG: local indices whose factor is applied
+  int16_t conj;      // read the matrix conjugated (density-matrix column pass)
+  int16_t param;     // per-sample matrix row (parametric gate with per-sample theta)
+  int32_t off[16];   // matrix elements (double2 offsets in a sample's matrix table)
+};
+
+constexpr int kMaxRegBits = 5;
+struct StageDesc {
+  int op0, nops;
+  int nreg;
+  int reg[kMaxRegBits];  // pass-local bit of register bit k
+  int ntid;
+  int tid[26];           // pass-local bit of thread-index bit b
+};
+
+// TMA box geometry of a tile pass over the amplitude tensor.
+struct TmaGeom {
+  int ndims;
+  int start[5];    // first amplitude bit of the dimension (batch dim: -1)
+  int bits[5];     // amplitude bits spanned by the dimension's extent
+  int boxb[5];     // amplitude bits covered by the box (tile bits of this dimension)
+};
+
+enum PassKind { PASS_TILE = 0, PASS_REG = 1, PASS_PLAIN = 2 };
+
+struct FOp;  // fused.cu
+
+struct Pass {
+  int kind;
+  int t;                        // tile bits (PASS_TILE) or register bits (PASS_REG)
+  std::vector<int> bits;        // pass-local bit i -> global amplitude bit
+  std::vector<StageDesc> stages;
+  std::vector<MOp> mops;
+  int plain_fop = -1;           // PASS_PLAIN: index into the schedule's fused ops
+  bool has_u2 = false;          // holds a 4x4 micro-op (selects the kernel variant)
+  TmaGeom geom{};
+  int stage_off = 0, mop_off = 0;  // offsets into the schedule's device buffers
+};
+
+}  // namespace mb

@@ -55,7 +55,7 @@ struct mb_circuit_s {
   size_t theta_cap = 0;
   double* h_theta = nullptr;          // pinned staging for theta uploads
   size_t h_theta_cap = 0;
-  mb::Schedule* sched = nullptr;      // fused schedule for pure states (built lazily)
+  std::vector<mb::Schedule*> scheds;  // fused schedules, built lazily per state shape
 };
 
 namespace mb {
