@@ -25,6 +25,7 @@
 #include <memory>
 
 #include "fused_kernels.cuh"
+#include "jit.h"
 
 namespace mb {
 
@@ -175,6 +176,7 @@ struct FOp {
   int off[16] = {0};
   uint32_t active = 0;
   int conj = 0, param = 0;
+  bool neg = false;           // MOP_CPHASE with factor -1 (a sign flip)
   // plain fallback
   int cls = CLS_DENSE;
   int mat_off = 0, mode = MAT_PLAIN;
@@ -185,6 +187,7 @@ struct FOp {
 
 struct Schedule {
   int N = 0, dm = 0, t = 0, R = 0, nsamples = 1;
+  int jit = 0;  // 0 not tried, 1 specialised kernels ready, -1 interpreter kernels
   bool dagger = false;
   std::vector<FOp> fops;
   std::vector<Pass> passes;
@@ -242,6 +245,43 @@ static FOp gate_fop(mb_circuit c, const COp& op, int shift, int conj, bool dagge
   const int fconj = dagger ? !conj : conj;
   if (op.k == 0) return f;  // global scalar: plain path
   if (op.cls == CLS_DIAG) {
+    const int nact = __builtin_popcount(op.active);
+    if (nact == 1 && op.active == (1u << (d - 1)) && op.k <= 4) {
+      // Phase on the all-ones entry: CZ, CPHASE, CCPHASE, PHASE, Z, S, T.
+      f.type = MOP_CPHASE;
+      f.off[0] = off(d - 1, d - 1);
+      for (int j = 0; j < op.k; ++j) f.ctrl[f.nctrl++] = f.bits[j];
+      if (!op.parametric) {
+        const double2 x = c->fixed_table[op.mat_off + (d - 1) * (d + 1)];
+        f.neg = x.x == -1.0 && x.y == 0.0;
+      }
+      f.conj = fconj;
+      finalize_masks(f);
+      return f;
+    }
+    // A diagonal that is identity unless all bits but one are set is a controlled 2x2.
+    for (int tj = 0; tj < op.k && op.k >= 1; ++tj) {
+      const int tb = 1 << tj, cm = (d - 1) & ~tb;
+      uint32_t ctl = 0;
+      for (int a = 0; a < d; ++a)
+        if ((a & cm) == cm) ctl |= 1u << a;
+      if ((op.active & ~ctl) == 0) {
+        f.tgt[0] = f.bits[tj];
+        f.ntgt = 1;
+        for (int j = 0; j < op.k; ++j)
+          if (j != tj) f.ctrl[f.nctrl++] = f.bits[j];
+        f.off[0] = off(cm, cm);
+        f.off[1] = off(cm | tb, cm);
+        f.off[2] = off(cm, cm | tb);
+        f.off[3] = off(cm | tb, cm | tb);
+        f.type = f.nctrl ? MOP_CTRL : MOP_U1;
+        if (f.nctrl > 4) f.type = F_UNFUSABLE;
+        f.conj = fconj;
+        finalize_masks(f);
+        f.nd = 0;  // diagonal: commutes with every other diagonal and control
+        return f;
+      }
+    }
     if (op.k > 3) return f;
     f.type = MOP_DIAG;
     for (int a = 0; a < d; ++a) f.off[a] = off(a, a);
@@ -512,6 +552,10 @@ static void plan_stages(const std::vector<FOp>& fops, const std::vector<int>& op
         m.nsel = int16_t(f.nb);
         for (int j = 0; j < f.nb; ++j) m.sel[j] = sel(f.bits[j]);
         m.active = f.active;
+      } else if (f.type == MOP_CPHASE) {
+        m.nsel = int16_t(f.nctrl);
+        for (int j = 0; j < f.nctrl; ++j) m.sel[j] = sel(f.ctrl[j]);
+        m.r1 = int16_t(f.neg ? 1 : 0);
       } else {
         m.r0 = int16_t(regidx(f.tgt[0]));
         m.nsel = int16_t(f.nctrl);
@@ -559,6 +603,10 @@ static void encode_reg_pass(const std::vector<FOp>& fops, const std::vector<int>
       m.nsel = int16_t(f.nb);
       for (int j = 0; j < f.nb; ++j) m.sel[j] = int16_t(f.bits[j]);
       m.active = f.active;
+    } else if (f.type == MOP_CPHASE) {
+      m.nsel = int16_t(f.nctrl);
+      for (int j = 0; j < f.nctrl; ++j) m.sel[j] = int16_t(f.ctrl[j]);
+      m.r1 = int16_t(f.neg ? 1 : 0);
     } else {
       m.r0 = int16_t(regidx(f.tgt[0]));
       m.nsel = int16_t(f.nctrl);
@@ -719,7 +767,7 @@ struct Tuning {
 static Tuning tuning_for(int N) {
   Tuning tu;
   if (const char* e = getenv("MB_TILE_BITS")) tu.t = std::max(8, std::min(12, atoi(e)));
-  if (const char* e = getenv("MB_REG_BITS")) tu.R = atoi(e) == 5 ? 5 : 4;
+  if (const char* e = getenv("MB_REG_BITS")) tu.R = std::max(3, std::min(5, atoi(e)));
   tu.t = std::min(tu.t, N);
   return tu;
 }
@@ -770,10 +818,47 @@ int get_schedule(mb_circuit c, int n, int dm, bool dagger, int nsamples, Schedul
   return MB_OK;
 }
 
+// Specialised kernels are used from MB_JIT_MIN_BITS register bits on (default 18); MB_JIT=0
+// disables them. Small states keep the interpreter kernels (no compile latency).
+static bool want_jit(int N) {
+  const char* e = getenv("MB_JIT");
+  if (e && atoi(e) == 0) return false;
+  int lo = 18;
+  if (const char* m = getenv("MB_JIT_MIN_BITS")) lo = atoi(m);
+  return N >= lo;
+}
+
+static void prepare_jit(Schedule* S) {
+  if (S->jit != 0) return;
+  S->jit = -1;
+  if (!want_jit(S->N) || !jit_available()) return;
+  std::vector<std::string> src;
+  std::vector<Pass*> who;
+  for (Pass& p : S->passes) {
+    if (p.kind == PASS_TILE) src.push_back(jit_tile_source(p, S->R, S->N));
+    else if (p.kind == PASS_REG) src.push_back(jit_reg_source(p, S->N));
+    else continue;
+    who.push_back(&p);
+  }
+  std::vector<CUfunction> fns;
+  std::string err;
+  if (jit_prepare(src, fns, &err) != MB_OK) {
+    if (getenv("MB_JIT_VERBOSE")) fprintf(stderr, "mossb200: JIT disabled for this schedule: %s\n", err.c_str());
+    return;
+  }
+  for (size_t i = 0; i < who.size(); ++i) who[i]->jit_fn = fns[i];
+  S->jit = 1;
+}
+
 int run_schedule(mb_circuit c, Schedule* S, double2* v, int nsamples, int64_t mstride) {
   cudaStream_t st = g_ctx.stream;
   const int N = S->N;
   const int64_t elems = int64_t(1) << N;
+  prepare_jit(S);
+  if (S->jit != 1 && S->R != 4 && S->R != 5) {
+    set_error("register width %d needs the specialised kernels, which are unavailable", S->R);
+    return MB_EUNSUPPORTED;
+  }
   for (const Pass& p : S->passes) {
     int rc = MB_OK;
     if (p.kind == PASS_PLAIN) {
@@ -801,6 +886,14 @@ int run_schedule(mb_circuit c, Schedule* S, double2* v, int nsamples, int64_t ms
       const size_t shm = (size_t(32) << p.t) + 1024;  // two tile buffers + alignment slack
       const int per_sm = std::max(1, int((227 * 1024) / (shm + 256)));
       const int64_t grid = std::min<int64_t>(a.ntiles, int64_t(g_ctx.sm_count) * std::min(per_sm, 4));
+      if (S->jit == 1 && p.jit_fn) {
+        ProfScope ps("k_tile_pass_jit", 32.0 * double(elems) * nsamples, st);
+        rc = jit_launch_tile((CUfunction)p.jit_fn, &map, c->d_table, mstride, a.tiles_per_sample, a.ntiles, a.err,
+                             threads, shm, int(grid), st);
+        ++launch_counter();
+        if (rc) return rc;
+        continue;
+      }
       ProfScope ps("k_tile_pass", 32.0 * double(elems) * nsamples, st);
       const bool u2 = p.has_u2;
       auto launch = [&](auto kern) {
@@ -824,6 +917,13 @@ int run_schedule(mb_circuit c, Schedule* S, double2* v, int nsamples, int64_t ms
       const int64_t work = a.groups * nsamples;
       const int block = 128;
       const int grid = grid_for(work, block, int64_t(g_ctx.sm_count) * 16);
+      if (S->jit == 1 && p.jit_fn) {
+        ProfScope ps("k_reg_pass_jit", 32.0 * double(elems) * nsamples, st);
+        rc = jit_launch_reg((CUfunction)p.jit_fn, v, c->d_table, mstride, a.groups, nsamples, grid, st);
+        ++launch_counter();
+        if (rc) return rc;
+        continue;
+      }
       ProfScope ps("k_reg_pass", 32.0 * double(elems) * nsamples, st);
       if (p.t == 5) p.has_u2 ? k_reg_pass<5, true><<<grid, block, 0, st>>>(v, a)
                              : k_reg_pass<5, false><<<grid, block, 0, st>>>(v, a);

@@ -14,6 +14,7 @@ enum MopType : int16_t {
   MOP_CTRLX = 2,  // swap on register bit r0 where every control bit is 1 (CNOT, TOFFOLI, X)
   MOP_U2 = 3,     // dense 4x4 on register bits r0 < r1 (local bit 0 = r0)
   MOP_DIAG = 4,   // diagonal on up to 3 bits anywhere: factor of local index a where active
+  MOP_CPHASE = 5, // factor off[0] (or a sign flip when r1 = 1) where every selector bit is 1
 };
 
 // A selector names one index bit: values < 64 are bits of the pass-local amplitude index,
@@ -56,6 +57,7 @@ struct Pass {
   std::vector<MOp> mops;
   int plain_fop = -1;           // PASS_PLAIN: index into the schedule's fused ops
   bool has_u2 = false;          // holds a 4x4 micro-op (selects the kernel variant)
+  void* jit_fn = nullptr;       // specialised kernel (CUfunction) when the JIT is in use
   TmaGeom geom{};
   int stage_off = 0, mop_off = 0;  // offsets into the schedule's device buffers
 };

@@ -133,6 +133,51 @@ __device__ __forceinline__ void diag(double2 (&a)[1 << R], const double2* m, con
   }
 }
 
+// Controlled-X with the control mask NEED over register bits known at compile time: the
+// swap is a renaming of registers and costs no instructions.
+template <int R, int K, int NEED>
+__device__ __forceinline__ void ctrlx_ct(double2 (&a)[1 << R]) {
+#pragma unroll
+  for (int j = 0; j < (1 << R); ++j)
+    if (!((j >> K) & 1) && (j & NEED) == NEED) {
+      const double2 x = a[j];
+      a[j] = a[j | (1 << K)];
+      a[j | (1 << K)] = x;
+    }
+}
+
+template <int R, int K, int NEED = 0>
+__device__ __forceinline__ void ctrlx_dispatch(double2 (&a)[1 << R], int need) {
+  if constexpr (NEED < (1 << R)) {
+    if constexpr (!((NEED >> K) & 1)) {
+      if (need == NEED) {
+        ctrlx_ct<R, K, NEED>(a);
+        return;
+      }
+    }
+    ctrlx_dispatch<R, K, NEED + 1>(a, need);
+  }
+}
+
+// Phase factor f on the amplitudes whose register bits cover NEED (compile-time mask).
+template <int R, int NEED>
+__device__ __forceinline__ void cphase_ct(double2 (&a)[1 << R], double2 f, bool neg) {
+#pragma unroll
+  for (int j = 0; j < (1 << R); ++j)
+    if ((j & NEED) == NEED) a[j] = neg ? make_double2(-a[j].x, -a[j].y) : cmul(f, a[j]);
+}
+
+template <int R, int NEED = 0>
+__device__ __forceinline__ void cphase_dispatch(double2 (&a)[1 << R], int need, double2 f, bool neg) {
+  if constexpr (NEED < (1 << R)) {
+    if (need == NEED) {
+      cphase_ct<R, NEED>(a, f, neg);
+      return;
+    }
+    cphase_dispatch<R, NEED + 1>(a, need, f, neg);
+  }
+}
+
 #define FK_CASE_K(R, K, CALL) case K: { constexpr int KK = K; if constexpr (KK < R) { CALL; } } break;
 
 // Runs micro-ops [0, nops) on the registers. HAS_U2 = false compiles a lean variant without
@@ -155,8 +200,32 @@ __device__ __forceinline__ void run_mops(double2 (&a)[1 << R], const MOp* __rest
         FK_CASE_K(R, 3, (u1<R, KK>(a, m00, m10, m01, m11)))
         FK_CASE_K(R, 4, (u1<R, KK>(a, m00, m10, m01, m11)))
       }
-    } else if (type == MOP_CTRL || type == MOP_CTRLX) {
-      const bool sw = type == MOP_CTRLX;
+    } else if (type == MOP_CTRLX || type == MOP_CPHASE) {
+      // Resolve the selectors: register-bit mask plus a thread-constant condition.
+      int need = 0;
+      uint32_t cst = 1;
+      for (int c = 0; c < nsel; ++c) {
+        const Sel sl = resolve<R>(op->sel[c], lbase, reg, gbase);
+        if (sl.rk >= 0) need |= 1 << sl.rk;
+        else cst &= sl.cv;
+      }
+      if (cst) {
+        if (type == MOP_CTRLX) {
+          switch (r0) {
+            FK_CASE_K(R, 0, (ctrlx_dispatch<R, KK>(a, need)))
+            FK_CASE_K(R, 1, (ctrlx_dispatch<R, KK>(a, need)))
+            FK_CASE_K(R, 2, (ctrlx_dispatch<R, KK>(a, need)))
+            FK_CASE_K(R, 3, (ctrlx_dispatch<R, KK>(a, need)))
+            FK_CASE_K(R, 4, (ctrlx_dispatch<R, KK>(a, need)))
+          }
+        } else {
+          const bool neg = op->r1 != 0;
+          const double2 f = neg ? make_double2(-1.0, 0.0) : ldm(m, op->off[0], conj);
+          cphase_dispatch<R>(a, need, f, neg);
+        }
+      }
+    } else if (type == MOP_CTRL) {
+      const bool sw = false;
       double2 m00 = make_double2(0, 0), m10 = m00, m01 = m00, m11 = m00;
       if (!sw) {
         m00 = ldm(m, op->off[0], conj);

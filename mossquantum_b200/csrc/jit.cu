@@ -1,0 +1,518 @@
+// Runtime-specialised pass kernels (NVRTC).
+//
+// The interpreter kernels (k_tile_pass / k_reg_pass) decode micro-ops at run time. For large
+// states this module instead generates one straight-line kernel per pass structure: the
+// register offsets, swizzled shared-memory slots, matrix-table offsets and control patterns
+// are compile-time constants, a controlled-X on register bits becomes a renaming of
+// variables (no instructions), and a CZ a handful of sign flips. Matrix values stay in the
+// circuit's table, so circuits that differ only in angles share one kernel. Kernels are
+// compiled with NVRTC for sm_100a, cached by their source text, and launched through the
+// driver API on the library stream.
+#include <cuda.h>
+#include <dlfcn.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cstdio>
+#include <cstring>
+#include <functional>
+#include <map>
+#include <mutex>
+#include <sstream>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "jit.h"
+
+namespace mb {
+namespace {
+
+// ---- NVRTC (dlopen'ed) -----------------------------------------------------------------------
+typedef int nvrtcResult_t;
+typedef struct _nvrtcProgram* nvrtcProgram_t;
+struct Nvrtc {
+  void* h = nullptr;
+  nvrtcResult_t (*create)(nvrtcProgram_t*, const char*, const char*, int, const char* const*, const char* const*);
+  nvrtcResult_t (*compile)(nvrtcProgram_t, int, const char* const*);
+  nvrtcResult_t (*log_size)(nvrtcProgram_t, size_t*);
+  nvrtcResult_t (*log)(nvrtcProgram_t, char*);
+  nvrtcResult_t (*cubin_size)(nvrtcProgram_t, size_t*);
+  nvrtcResult_t (*cubin)(nvrtcProgram_t, char*);
+  nvrtcResult_t (*destroy)(nvrtcProgram_t*);
+  bool ok = false;
+};
+
+Nvrtc& nvrtc() {
+  static Nvrtc n;
+  static bool tried = false;
+  if (tried) return n;
+  tried = true;
+  const char* paths[] = {"libnvrtc.so.12", "/usr/local/cuda/lib64/libnvrtc.so.12", "libnvrtc.so"};
+  for (const char* p : paths) {
+    n.h = dlopen(p, RTLD_NOW | RTLD_LOCAL);
+    if (n.h) break;
+  }
+  if (!n.h) return n;
+  n.create = (decltype(n.create))dlsym(n.h, "nvrtcCreateProgram");
+  n.compile = (decltype(n.compile))dlsym(n.h, "nvrtcCompileProgram");
+  n.log_size = (decltype(n.log_size))dlsym(n.h, "nvrtcGetProgramLogSize");
+  n.log = (decltype(n.log))dlsym(n.h, "nvrtcGetProgramLog");
+  n.cubin_size = (decltype(n.cubin_size))dlsym(n.h, "nvrtcGetCUBINSize");
+  n.cubin = (decltype(n.cubin))dlsym(n.h, "nvrtcGetCUBIN");
+  n.destroy = (decltype(n.destroy))dlsym(n.h, "nvrtcDestroyProgram");
+  n.ok = n.create && n.compile && n.log_size && n.log && n.cubin_size && n.cubin && n.destroy;
+  return n;
+}
+
+// ---- driver API (through the runtime's entry-point query) -----------------------------------
+struct Drv {
+  CUresult (*load)(CUmodule*, const void*) = nullptr;
+  CUresult (*getfn)(CUfunction*, CUmodule, const char*) = nullptr;
+  CUresult (*launch)(CUfunction, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned, CUstream,
+                     void**, void**) = nullptr;
+  CUresult (*setattr)(CUfunction, CUfunction_attribute, int) = nullptr;
+  bool ok = false;
+};
+
+Drv& drv() {
+  static Drv d;
+  static bool tried = false;
+  if (tried) return d;
+  tried = true;
+  cudaDriverEntryPointQueryResult q;
+  void* p = nullptr;
+  if (cudaGetDriverEntryPoint("cuModuleLoadData", &p, cudaEnableDefault, &q) == cudaSuccess && p) d.load = (decltype(d.load))p;
+  if (cudaGetDriverEntryPoint("cuModuleGetFunction", &p, cudaEnableDefault, &q) == cudaSuccess && p) d.getfn = (decltype(d.getfn))p;
+  if (cudaGetDriverEntryPoint("cuLaunchKernel", &p, cudaEnableDefault, &q) == cudaSuccess && p) d.launch = (decltype(d.launch))p;
+  if (cudaGetDriverEntryPoint("cuFuncSetAttribute", &p, cudaEnableDefault, &q) == cudaSuccess && p) d.setattr = (decltype(d.setattr))p;
+  d.ok = d.load && d.getfn && d.launch && d.setattr;
+  return d;
+}
+
+std::mutex g_jit_mu;
+std::map<std::string, CUfunction> g_cache;
+
+const char* kPrelude = R"PRE(
+typedef unsigned long long u64;
+typedef unsigned int u32;
+struct __align__(64) TMap { u64 v[16]; };
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cfma(double2 a, double2 b, double2 c) {
+  return make_double2(fma(a.x, b.x, fma(-a.y, b.y, c.x)), fma(a.x, b.y, fma(a.y, b.x, c.y)));
+}
+__device__ __forceinline__ double2 ld(const double2* p) { return __ldg(p); }
+__device__ __forceinline__ double2 ldc(const double2* p) { double2 x = __ldg(p); return make_double2(x.x, -x.y); }
+__device__ __forceinline__ double2 neg(double2 a) { return make_double2(-a.x, -a.y); }
+__device__ __forceinline__ u32 swz(u32 i) { return i ^ ((i >> 3) & 7u); }
+__device__ __forceinline__ u32 sa(const void* p) { return (u32)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(u64* b) { asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(sa(b)) : "memory"); }
+__device__ __forceinline__ void mbar_tx(u64* b, u32 n) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(sa(b)), "r"(n) : "memory");
+}
+__device__ __forceinline__ bool mbar_wait(u64* b, u32 ph) {
+  for (u32 it = 0; it < (1u << 26); ++it) {
+    u32 done;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+                 : "=r"(done) : "r"(sa(b)), "r"(ph) : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+)PRE";
+
+std::string tma_ld(int nd) {
+  std::ostringstream o;
+  o << "asm volatile(\"cp.async.bulk.tensor." << nd
+    << "d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {";
+  for (int d = 0; d < nd; ++d) o << (d ? ", " : "") << "%" << (2 + d);
+  o << "}], [%" << (2 + nd) << "];\" :: \"r\"(sa(DST)), \"l\"((u64)&tmap)";
+  for (int d = 0; d < nd; ++d) o << ", \"r\"(c" << d << ")";
+  o << ", \"r\"(sa(BAR)) : \"memory\");";
+  return o.str();
+}
+
+std::string tma_st(int nd) {
+  std::ostringstream o;
+  o << "asm volatile(\"cp.async.bulk.tensor." << nd << "d.global.shared::cta.tile.bulk_group [%0, {";
+  for (int d = 0; d < nd; ++d) o << (d ? ", " : "") << "%" << (2 + d);
+  o << "}], [%1];\" :: \"l\"((u64)&tmap), \"r\"(sa(SRC))";
+  for (int d = 0; d < nd; ++d) o << ", \"r\"(c" << d << ")";
+  o << " : \"memory\"); asm volatile(\"cp.async.bulk.commit_group;\" ::: \"memory\");";
+  return o.str();
+}
+
+// Generates the body of one register stage. Variables a0..a{2^R-1} hold the amplitudes; nm
+// maps logical register index j to the variable currently holding it (controlled-X on
+// register bits only permutes nm).
+struct StageGen {
+  int R;
+  const int* reg;      // pass-local bit of register bit k
+  std::ostringstream& o;
+  bool lb64;           // pass-local index is a 64-bit global index (register sweep)
+  std::vector<int> nm;
+
+  // Selector classification: register bit k (>= 0), or -1 with a runtime expression.
+  int regbit(int sel) const {
+    if (sel >= 64) return -1;
+    for (int k = 0; k < R; ++k)
+      if (reg[k] == sel) return k;
+    return -1;
+  }
+  std::string rt(int sel) const {
+    std::ostringstream e;
+    if (sel >= 64) e << "(u32)((gb >> " << (sel - 64) << ") & 1ull)";
+    else e << "(u32)((lb >> " << sel << ") & 1" << (lb64 ? "ull" : "u") << ")";
+    return e.str();
+  }
+  // Splits selectors into a compile-time register mask and a runtime condition string.
+  void split(const MOp& m, int& need, std::string& cond) const {
+    need = 0;
+    cond.clear();
+    for (int c = 0; c < m.nsel; ++c) {
+      const int k = regbit(m.sel[c]);
+      if (k >= 0) need |= 1 << k;
+      else cond += (cond.empty() ? "" : " & ") + rt(m.sel[c]);
+    }
+  }
+  std::string v(int j) const { return "a" + std::to_string(nm[j]); }
+  std::string ldm(const MOp& m, int e) const {
+    return std::string(m.conj ? "ldc" : "ld") + "(" + (m.param ? "tb" : "tab") + " + " + std::to_string(m.off[e]) + ")";
+  }
+
+  void emit(const MOp& m) {
+    const int A = 1 << R;
+    switch (m.type) {
+      case MOP_U1: {
+        const int b = 1 << m.r0;
+        o << "{ const double2 m00 = " << ldm(m, 0) << ", m10 = " << ldm(m, 1) << ", m01 = " << ldm(m, 2)
+          << ", m11 = " << ldm(m, 3) << ";\n";
+        for (int j = 0; j < A; ++j)
+          if (!(j & b))
+            o << "  { const double2 x = " << v(j) << ", y = " << v(j | b) << "; " << v(j)
+              << " = cfma(m01, y, cmul(m00, x)); " << v(j | b) << " = cfma(m11, y, cmul(m10, x)); }\n";
+        o << "}\n";
+        break;
+      }
+      case MOP_CTRL: {
+        const int b = 1 << m.r0;
+        int need;
+        std::string cond;
+        split(m, need, cond);
+        o << "{ const double2 m00 = " << ldm(m, 0) << ", m10 = " << ldm(m, 1) << ", m01 = " << ldm(m, 2)
+          << ", m11 = " << ldm(m, 3) << ";\n";
+        if (!cond.empty()) o << " if (" << cond << ") {\n";
+        for (int j = 0; j < A; ++j)
+          if (!(j & b) && (j & need) == need)
+            o << "  { const double2 x = " << v(j) << ", y = " << v(j | b) << "; " << v(j)
+              << " = cfma(m01, y, cmul(m00, x)); " << v(j | b) << " = cfma(m11, y, cmul(m10, x)); }\n";
+        if (!cond.empty()) o << " }\n";
+        o << "}\n";
+        break;
+      }
+      case MOP_CTRLX: {
+        const int b = 1 << m.r0;
+        int need;
+        std::string cond;
+        split(m, need, cond);
+        if (cond.empty()) {
+          for (int j = 0; j < A; ++j)
+            if (!(j & b) && (j & need) == need) std::swap(nm[j], nm[j | b]);
+        } else {
+          o << "{ const bool pr = (" << cond << ") != 0u;\n";
+          for (int j = 0; j < A; ++j)
+            if (!(j & b) && (j & need) == need)
+              o << "  { const double2 x = " << v(j) << ", y = " << v(j | b) << "; " << v(j) << " = pr ? y : x; "
+                << v(j | b) << " = pr ? x : y; }\n";
+          o << "}\n";
+        }
+        break;
+      }
+      case MOP_CPHASE: {
+        int need;
+        std::string cond;
+        split(m, need, cond);
+        o << "{ ";
+        if (!m.r1) o << "const double2 f = " << ldm(m, 0) << "; ";
+        if (!cond.empty()) o << "if (" << cond << ") {";
+        o << "\n";
+        for (int j = 0; j < A; ++j)
+          if ((j & need) == need) o << "  " << v(j) << " = " << (m.r1 ? "neg(" + v(j) + ")" : "cmul(f, " + v(j) + ")") << ";\n";
+        if (!cond.empty()) o << " }";
+        o << "}\n";
+        break;
+      }
+      case MOP_U2: {
+        const int b0 = 1 << m.r0, b1 = 1 << m.r1;
+        o << "{ double2 u[16];\n";
+        for (int e = 0; e < 16; ++e) o << " u[" << e << "] = " << ldm(m, e) << ";";
+        o << "\n";
+        for (int j = 0; j < A; ++j)
+          if (!(j & b0) && !(j & b1)) {
+            const int i[4] = {j, j | b0, j | b1, j | b0 | b1};
+            o << "  { const double2 x0 = " << v(i[0]) << ", x1 = " << v(i[1]) << ", x2 = " << v(i[2]) << ", x3 = " << v(i[3])
+              << ";\n";
+            for (int r = 0; r < 4; ++r)
+              o << "    " << v(i[r]) << " = cfma(u[" << (12 + r) << "], x3, cfma(u[" << (8 + r) << "], x2, cfma(u["
+                << (4 + r) << "], x1, cmul(u[" << r << "], x0))));\n";
+            o << "  }\n";
+          }
+        o << "}\n";
+        break;
+      }
+      case MOP_DIAG: {
+        // index = compile-time register part | runtime part
+        int rk[4];
+        std::string rtpart;
+        for (int c = 0; c < m.nsel; ++c) {
+          rk[c] = regbit(m.sel[c]);
+          if (rk[c] < 0) rtpart += (rtpart.empty() ? "" : " | ") + std::string("(") + rt(m.sel[c]) + " << " + std::to_string(c) + ")";
+        }
+        o << "{ double2 F[8]; ";
+        for (int e = 0; e < (1 << m.nsel); ++e)
+          o << "F[" << e << "] = " << (((m.active >> e) & 1) ? ldm(m, e) : std::string("make_double2(1.0, 0.0)")) << "; ";
+        o << "const u32 ri = " << (rtpart.empty() ? std::string("0u") : rtpart) << ";\n";
+        for (int j = 0; j < A; ++j) {
+          int ct = 0;
+          for (int c = 0; c < m.nsel; ++c)
+            if (rk[c] >= 0 && ((j >> rk[c]) & 1)) ct |= 1 << c;
+          o << "  " << v(j) << " = cmul(F[" << ct << "u | ri], " << v(j) << ");\n";
+        }
+        o << "}\n";
+        break;
+      }
+    }
+  }
+};
+
+std::string reg_off_const(int j, int R, const int* reg) {
+  unsigned long long c = 0;
+  for (int k = 0; k < R; ++k)
+    if ((j >> k) & 1) c |= 1ull << reg[k];
+  return std::to_string(c) + "ull";
+}
+
+// Compiles (or fetches) a kernel; returns nullptr on any failure.
+CUfunction compile_kernel(const std::string& src, std::string* err) {
+  {
+    std::lock_guard<std::mutex> lk(g_jit_mu);
+    auto it = g_cache.find(src);
+    if (it != g_cache.end()) return it->second;
+  }
+  Nvrtc& n = nvrtc();
+  Drv& d = drv();
+  if (!n.ok || !d.ok) {
+    *err = "NVRTC or driver entry points unavailable";
+    return nullptr;
+  }
+  nvrtcProgram_t prog;
+  if (n.create(&prog, src.c_str(), "mbk.cu", 0, nullptr, nullptr) != 0) {
+    *err = "nvrtcCreateProgram failed";
+    return nullptr;
+  }
+  const char* opts[] = {"--gpu-architecture=sm_100a", "-std=c++17", "--fmad=true", "-default-device"};
+  const int rc = n.compile(prog, 4, opts);
+  if (rc != 0) {
+    size_t ls = 0;
+    n.log_size(prog, &ls);
+    std::string log(ls, '\0');
+    n.log(prog, &log[0]);
+    *err = "NVRTC compile failed: " + log.substr(0, 2000);
+    n.destroy(&prog);
+    return nullptr;
+  }
+  size_t cs = 0;
+  n.cubin_size(prog, &cs);
+  std::vector<char> cubin(cs);
+  n.cubin(prog, cubin.data());
+  n.destroy(&prog);
+  CUmodule mod;
+  CUfunction fn;
+  if (d.load(&mod, cubin.data()) != CUDA_SUCCESS || d.getfn(&fn, mod, "mbk") != CUDA_SUCCESS) {
+    *err = "module load failed";
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> lk(g_jit_mu);
+  g_cache[src] = fn;
+  return fn;
+}
+
+}  // namespace
+
+bool jit_available() { return nvrtc().ok && drv().ok; }
+
+std::string jit_tile_source(const Pass& p, int R, int N) {
+  std::ostringstream o;
+  const int A = 1 << R;
+  const int threads = 1 << (p.t - R);
+  const TmaGeom& g = p.geom;
+  o << kPrelude;
+  o << "extern \"C\" __global__ void __launch_bounds__(" << threads << ", 1) mbk(const __grid_constant__ TMap tmap, "
+    << "const double2* __restrict__ tab, long long tstride, long long tps, long long ntiles, u32* err) {\n";
+  o << "  extern __shared__ unsigned char smem_raw[];\n  __shared__ __align__(8) u64 bar[2];\n  __shared__ int s_abort;\n";
+  o << "  double2* buf0 = (double2*)(((unsigned long long)smem_raw + 1023ull) & ~1023ull);\n";
+  o << "  double2* bufs[2] = {buf0, buf0 + " << (1 << p.t) << "};\n";
+  o << "  const u32 tx = threadIdx.x;\n";
+  o << "  if (tx == 0) { mbar_init(&bar[0]); mbar_init(&bar[1]); asm volatile(\"fence.mbarrier_init.release.cluster;\" ::: \"memory\"); s_abort = 0; }\n";
+  o << "  __syncthreads();\n";
+  // geometry: base index with zeros at the tile bits, TMA coordinates
+  auto geom = [&](const char* tile, const char* pre) {
+    std::ostringstream e;
+    e << "  const int " << pre << "b = (int)(" << tile << " / tps);\n";
+    e << "  u64 " << pre << "gb = (u64)(" << tile << " - (long long)" << pre << "b * tps);\n";
+    for (int q = 0; q < p.t; ++q) {
+      const int bit = p.bits[q];
+      e << "  " << pre << "gb = ((" << pre << "gb >> " << bit << ") << " << (bit + 1) << ") | (" << pre << "gb & "
+        << ((1ull << bit) - 1) << "ull);\n";
+    }
+    for (int d = 0; d < g.ndims; ++d) {
+      e << "  const int " << pre << "c" << d << " = ";
+      if (g.start[d] < 0) e << pre << "b;\n";
+      else if (d == 0) e << "(int)(2ull * (" << pre << "gb & " << ((1ull << g.bits[0]) - 1) << "ull));\n";
+      else e << "(int)((" << pre << "gb >> " << g.start[d] << ") & " << ((1ull << g.bits[d]) - 1) << "ull);\n";
+    }
+    return e.str();
+  };
+  auto with_prefix = [&](std::string s, const char* pre) {
+    // rename c{d} in the TMA strings to pre c{d}
+    for (int d = 0; d < g.ndims; ++d) {
+      const std::string from = "\"r\"(c" + std::to_string(d) + ")", to = std::string("\"r\"(") + pre + "c" + std::to_string(d) + ")";
+      size_t pos;
+      while ((pos = s.find(from)) != std::string::npos) s.replace(pos, from.size(), to);
+    }
+    return s;
+  };
+  std::string ld = tma_ld(g.ndims), st = tma_st(g.ndims);
+  const unsigned bytes = 16u << p.t;
+  o << "  u32 ph0 = 0, ph1 = 0;\n  long long tile = blockIdx.x;\n";
+  o << "  if (tx == 0 && tile < ntiles) {\n" << geom("tile", "p_");
+  {
+    std::string s = with_prefix(ld, "p_");
+    size_t pos;
+    while ((pos = s.find("DST")) != std::string::npos) s.replace(pos, 3, "bufs[0]");
+    while ((pos = s.find("BAR")) != std::string::npos) s.replace(pos, 3, "&bar[0]");
+    o << "    mbar_tx(&bar[0], " << bytes << "u); " << s << "\n  }\n";
+  }
+  o << "  for (int it = 0; tile < ntiles; ++it, tile += gridDim.x) {\n";
+  o << "    const int cur = it & 1;\n    const long long nxt = tile + gridDim.x;\n";
+  o << "    if (tx == 0 && nxt < ntiles) {\n" << geom("nxt", "n_");
+  {
+    std::string s = with_prefix(ld, "n_");
+    size_t pos;
+    while ((pos = s.find("DST")) != std::string::npos) s.replace(pos, 3, "bufs[cur ^ 1]");
+    while ((pos = s.find("BAR")) != std::string::npos) s.replace(pos, 3, "&bar[cur ^ 1]");
+    o << "      asm volatile(\"cp.async.bulk.wait_group.read 0;\" ::: \"memory\");\n      mbar_tx(&bar[cur ^ 1], " << bytes
+      << "u); " << s << "\n    }\n";
+  }
+  o << geom("tile", "");
+  o << "    const double2* tb = tab + (long long)b * tstride;\n    (void)tb;\n";
+  o << "    double2* tl = bufs[cur];\n";
+  o << "    if (!mbar_wait(&bar[cur], cur ? ph1 : ph0)) { atomicOr(err, 1u); s_abort = 1; }\n";
+  o << "    if (cur) ph1 ^= 1u; else ph0 ^= 1u;\n    __syncthreads();\n    if (s_abort) break;\n";
+  o << "    double2 ";
+  for (int j = 0; j < A; ++j) o << (j ? ", " : "") << "a" << j;
+  o << ";\n";
+  for (const StageDesc& sd : p.stages) {
+    o << "    {\n      const u32 lb = 0u";
+    for (int q = 0; q < sd.ntid; ++q) o << " | (((tx >> " << q << ") & 1u) << " << sd.tid[q] << ")";
+    o << ";\n";
+    for (int j = 0; j < A; ++j) o << "      a" << j << " = tl[swz(lb | " << reg_off_const(j, R, sd.reg) << ")];\n";
+    StageGen sg{R, sd.reg, o, false, std::vector<int>(A)};
+    for (int j = 0; j < A; ++j) sg.nm[j] = j;
+    for (int q = 0; q < sd.nops; ++q) sg.emit(p.mops[sd.op0 + q]);
+    for (int j = 0; j < A; ++j) o << "      tl[swz(lb | " << reg_off_const(j, R, sd.reg) << ")] = " << sg.v(j) << ";\n";
+    o << "      __syncthreads();\n    }\n";
+  }
+  o << "    asm volatile(\"fence.proxy.async.shared::cta;\" ::: \"memory\");\n    __syncthreads();\n";
+  {
+    std::string s = st;
+    size_t pos;
+    while ((pos = s.find("SRC")) != std::string::npos) s.replace(pos, 3, "tl");
+    o << "    if (tx == 0) { " << s << " }\n";
+  }
+  o << "  }\n  if (tx == 0) asm volatile(\"cp.async.bulk.wait_group 0;\" ::: \"memory\");\n}\n";
+  (void)N;
+  return o.str();
+}
+
+std::string jit_reg_source(const Pass& p, int N) {
+  std::ostringstream o;
+  const int R = p.t, A = 1 << R;
+  o << kPrelude;
+  o << "extern \"C\" __global__ void __launch_bounds__(128) mbk(double2* __restrict__ v, const double2* __restrict__ tab, "
+    << "long long tstride, long long groups, int nsamples) {\n";
+  o << "  const long long total = groups * nsamples;\n";
+  o << "  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < total; g += (long long)gridDim.x * blockDim.x) {\n";
+  o << "    const int b = (int)(g / groups);\n    u64 lb = (u64)(g - (long long)b * groups);\n";
+  for (int k = 0; k < R; ++k) {
+    const int bit = p.bits[k];
+    o << "    lb = ((lb >> " << bit << ") << " << (bit + 1) << ") | (lb & " << ((1ull << bit) - 1) << "ull);\n";
+  }
+  o << "    const u64 gb = 0ull; (void)gb;\n";
+  o << "    double2* vs = v + ((long long)b << " << N << ");\n";
+  o << "    const double2* tb = tab + (long long)b * tstride; (void)tb;\n";
+  int reg[kMaxRegBits];
+  for (int k = 0; k < R; ++k) reg[k] = p.bits[k];
+  for (int j = 0; j < A; ++j) o << "    double2 a" << j << " = vs[lb | " << reg_off_const(j, R, reg) << "];\n";
+  StageGen sg{R, reg, o, true, std::vector<int>(A)};
+  for (int j = 0; j < A; ++j) sg.nm[j] = j;
+  for (const MOp& m : p.mops) sg.emit(m);
+  for (int j = 0; j < A; ++j) o << "    vs[lb | " << reg_off_const(j, R, reg) << "] = " << sg.v(j) << ";\n";
+  o << "  }\n}\n";
+  return o.str();
+}
+
+int jit_prepare(std::vector<std::string>& sources, std::vector<CUfunction>& out, std::string* err) {
+  out.assign(sources.size(), nullptr);
+  std::vector<std::string> errs(sources.size());
+  std::vector<std::thread> pool;
+  const size_t nthreads = std::max<size_t>(1, std::min<size_t>(sources.size(), std::thread::hardware_concurrency()));
+  // Compilation runs on worker threads; modules load on the worker threads too, which is
+  // fine because the runtime's primary context is current on every thread of the process.
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::atomic<size_t> next{0};
+  for (size_t w = 0; w < nthreads; ++w)
+    pool.emplace_back([&] {
+      cudaSetDevice(dev);
+      cudaFree(nullptr);
+      for (size_t i = next++; i < sources.size(); i = next++) out[i] = compile_kernel(sources[i], &errs[i]);
+    });
+  for (auto& t : pool) t.join();
+  for (size_t i = 0; i < sources.size(); ++i)
+    if (!out[i]) {
+      *err = errs[i];
+      return MB_EUNSUPPORTED;
+    }
+  return MB_OK;
+}
+
+int jit_launch_tile(CUfunction fn, const CUtensorMap* map, const double2* tab, int64_t tstride, int64_t tps,
+                    int64_t ntiles, unsigned* err, int threads, size_t shm, int grid, cudaStream_t st) {
+  Drv& d = drv();
+  if (d.setattr(fn, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, int(shm)) != CUDA_SUCCESS) return MB_EDEVICE;
+  long long ts = tstride, tp = tps, nt = ntiles;
+  void* params[] = {(void*)map, (void*)&tab, &ts, &tp, &nt, &err};
+  if (d.launch(fn, grid, 1, 1, threads, 1, 1, unsigned(shm), (CUstream)st, params, nullptr) != CUDA_SUCCESS) {
+    set_error("JIT tile launch failed");
+    return MB_EDEVICE;
+  }
+  return MB_OK;
+}
+
+int jit_launch_reg(CUfunction fn, double2* v, const double2* tab, int64_t tstride, int64_t groups, int nsamples,
+                   int grid, cudaStream_t st) {
+  Drv& d = drv();
+  long long ts = tstride, gr = groups;
+  int ns = nsamples;
+  void* params[] = {&v, (void*)&tab, &ts, &gr, &ns};
+  if (d.launch(fn, grid, 1, 1, 128, 1, 1, 0, (CUstream)st, params, nullptr) != CUDA_SUCCESS) {
+    set_error("JIT sweep launch failed");
+    return MB_EDEVICE;
+  }
+  return MB_OK;
+}
+
+}  // namespace mb

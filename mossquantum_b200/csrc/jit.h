@@ -1,0 +1,20 @@
+// NVRTC-specialised pass kernels (jit.cu).
+#pragma once
+#include <cuda.h>
+
+#include <string>
+#include <vector>
+
+#include "fused.h"
+
+namespace mb {
+bool jit_available();
+std::string jit_tile_source(const Pass& p, int R, int N);
+std::string jit_reg_source(const Pass& p, int N);
+// Compiles every source (in parallel, cached by text); fills out[i] or fails with err.
+int jit_prepare(std::vector<std::string>& sources, std::vector<CUfunction>& out, std::string* err);
+int jit_launch_tile(CUfunction fn, const CUtensorMap* map, const double2* tab, int64_t tstride, int64_t tps,
+                    int64_t ntiles, unsigned* err, int threads, size_t shm, int grid, cudaStream_t st);
+int jit_launch_reg(CUfunction fn, double2* v, const double2* tab, int64_t tstride, int64_t groups, int nsamples,
+                   int grid, cudaStream_t st);
+}  // namespace mb
