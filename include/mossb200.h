@@ -183,6 +183,23 @@ MB_API int mb_probabilities(mb_state s, const int* qubits, int nq, double* out);
 MB_API int mb_adjoint(mb_circuit c, mb_observable o, mb_state init, const double* theta, size_t ntheta,
                const double* weights, int checkpoint_every, double* value, double* grad);
 
+/* ---- allocation-free expectation -----------------------------------------------------
+ * No counterpart in the reference: MOSSQuantum's CPU path never allocates device memory.
+ * For callers that cannot allocate device memory (a pre-planned HBM pool with every byte
+ * assigned, a latency-critical path where cudaMalloc/cudaFree would synchronise the GPU,
+ * a plug-in that may only use memory its host hands it). It needs no mb_init.
+ * <psi_b|M|psi_b> for b = 0..nsamples-1, where M is a 2^k x 2^k column-major complex matrix
+ * on `positions` (zero-based, first = least significant local bit) and the samples are
+ * nsamples states of 2^n amplitudes stored back to back at device address state_dev.
+ * out: 2*nsamples host doubles (re, im). stream: a cudaStream_t (NULL = default stream); the
+ * call returns after the result has reached `out`.
+ * Limits: k <= 3, nsamples <= 32 (the reduction scratch is a fixed 82,560-byte array in the
+ * library, held on every GPU that loads it until exit). The first call on each device looks
+ * up that array's device address, so make it before any stream capture. All calls share the
+ * array: calls that overlap on the GPU race and must be serialised by the caller. */
+MB_API int mb_expect_local_noalloc(const double* state_dev, int n, int nsamples, int k, const int* positions,
+                                   const double* matrix, double* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,70 @@
+"""The allocation-free expectation entry point, called through the C ABI.
+
+mb_expect_local_noalloc exists for callers that cannot allocate device memory (a fixed HBM
+pool, a latency-critical loop where cudaMalloc would synchronise the GPU, a plug-in that may
+only use memory handed to it): it takes the caller's device state and keeps its reduction
+scratch in a static array inside the library. This test compares it with mb_expect (which
+uses the library's own workspace) on two calls in a row, at the expectation tolerance used
+throughout the suite (1e-11). It sorts last so that a stop-at-first-failure run has already
+run every other test.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-11
+
+
+def _entry():
+    from mossquantum_b200 import _native as N
+    L = N.lib()
+    f = L.mb_expect_local_noalloc
+    f.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                  ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]
+    f.restype = ctypes.c_int
+    return N, f
+
+
+def _term_matrix(ops, coeff):
+    m = np.ones((1, 1), dtype=complex)
+    for o in ops:                    # first site = least significant local bit
+        m = np.kron(o, m)
+    return coeff * m
+
+
+def test_noalloc_matches_expect_twice(mq):
+    N, f = _entry()
+    rng = np.random.default_rng(2026)
+    cases = [(14, 1, [3, 9, 1]), (11, 4, [7, 2])]
+    for n, B, sites in cases:
+        cols = rng.normal(size=(1 << n, B)) + 1j * rng.normal(size=(1 << n, B))
+        cols /= np.linalg.norm(cols, axis=0)
+        state = mq.BatchStateVector(cols)
+        ops1 = [rng.normal(size=(2, 2)) + 1j * rng.normal(size=(2, 2)) for _ in sites]
+        ops2 = [rng.normal(size=(2, 2)) + 1j * rng.normal(size=(2, 2)) for _ in sites]
+        c1, c2 = 0.7 - 0.1j, -0.4 + 0.3j
+        H = mq.QubitsOperator([mq.QubitsTerm(sites, ops1, c1), mq.QubitsTerm(sites, ops2, c2)])
+        expected = mq.expectation(H, state)
+        # the same operator as one dense matrix in the given site order
+        M = _term_matrix(ops1, c1) + _term_matrix(ops2, c2)
+        mcol = np.asfortranarray(M).ravel(order="F").view(np.float64).copy()
+        pos = (ctypes.c_int * len(sites))(*[s - 1 for s in sites])
+        out = np.zeros(2 * B)
+        rc = f(state.device_ptr(), n, B, len(sites), pos, mcol.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+               out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), None)
+        assert rc == 0, N.last_error()
+        got = out[0::2] + 1j * out[1::2]
+        assert np.max(np.abs(got - expected)) <= TOL
+
+
+def test_noalloc_rejects_oversize(mq):
+    N, f = _entry()
+    state = mq.BatchStateVector(4, 33)
+    pos = (ctypes.c_int * 1)(0)
+    m = np.eye(2, dtype=complex).ravel(order="F").view(np.float64).copy()
+    out = np.zeros(66)
+    rc = f(state.device_ptr(), 4, 33, 1, pos, m.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+           out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), None)
+    assert rc == N.MB_EINVAL and "at most 32" in N.last_error()
