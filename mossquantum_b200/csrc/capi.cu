@@ -4,6 +4,7 @@
 #include <cmath>
 #include <complex>
 #include <cstdarg>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -816,7 +817,7 @@ extern "C" int mb_observable_free(mb_observable o) {
   if (!o) return MB_OK;
   if (g_ctx.init) {
     dev_free(o->d_mats);
-    dev_free(o->d_pauli);
+    pauli_free(o);
   }
   delete o;
   return MB_OK;
@@ -870,7 +871,8 @@ extern "C" int mb_expect(mb_observable o, mb_state s, double* out) {
     return MB_EUNSUPPORTED;
   }
   const int is_dm = s->kind == MB_DENSITY || s->kind == MB_BATCH_DENSITY;
-  int rc = (!is_dm && o->pauli_ok) ? expect_pauli(o, s) : expect_keys(o, s);
+  const bool keys_only = getenv("MB_EXPECT_KEYS") && atoi(getenv("MB_EXPECT_KEYS")) != 0;
+  int rc = (!is_dm && o->pauli_ok && !keys_only) ? expect_pauli(o, s) : expect_keys(o, s);
   if (rc) return rc;
   MB_CHECK_CUDA(cudaMemcpyAsync(out, g_ctx.results, sizeof(double2) * s->batch, cudaMemcpyDeviceToHost, g_ctx.stream));
   MB_CHECK_CUDA(cudaStreamSynchronize(g_ctx.stream));

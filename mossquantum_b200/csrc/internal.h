@@ -64,7 +64,7 @@ struct OKey {
   int pos[5];
   int mat_off;
 };
-struct PauliGroup;   // pauli.cu
+struct PauliData;    // pauli.cu
 }  // namespace mb
 
 struct mb_observable_s {
@@ -73,11 +73,9 @@ struct mb_observable_s {
   double2* d_mats = nullptr;
   bool hermitian = true;
   int max_site = -1;
-  // Pauli-string form for the fused expectation kernel.
+  // Pauli-string form for the fused expectation kernel (pauli.cu).
   bool pauli_ok = false;
-  void* d_pauli = nullptr;
-  std::vector<char> h_pauli;          // serialized groups (pauli.cu owns the layout)
-  int pauli_ngroups = 0;
+  mb::PauliData* pauli = nullptr;
 };
 
 namespace mb {
@@ -121,6 +119,7 @@ void release_schedules(mb_circuit c);
 
 // pauli.cu
 int pauli_compile(mb_observable o, const mb_term* terms, size_t nterms);
+void pauli_free(mb_observable o);
 int expect_pauli(mb_observable o, mb_state s);
 
 }  // namespace mb

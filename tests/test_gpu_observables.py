@@ -98,3 +98,29 @@ def test_sampling_matches_oracle_rng(mq, O):
     assert np.array_equal(a, b)
     c = mq.counts(np.random.default_rng(99), s, 500, qubits=[2, 4, 6])
     assert sum(c.values()) == 500
+
+
+def test_pauli_pass_matches_dense_keys(mq, O):
+    """The fused Pauli-string kernel and the per-key dense kernel agree with the oracle."""
+    import os
+    from mossquantum_b200 import workloads as W
+    rng = np.random.default_rng(77)
+    for n in (10, 13, 17):
+        psi = random_state(n, rng)
+        s = mq.StateVector(psi)
+        for H in (W.tfim(n), W.xxz(n), random_operator(mq, n, rng, False)):
+            ref = O.expect(psi, n, H.specs())
+            fused = mq.expectation(H, s)
+            os.environ["MB_EXPECT_KEYS"] = "1"
+            try:
+                keys = mq.expectation(H, s)
+            finally:
+                del os.environ["MB_EXPECT_KEYS"]
+            assert abs(fused - ref) <= 1e-11 and abs(keys - ref) <= 1e-11
+    # batch of states through the fused kernel
+    B, n = 3, 11
+    cols = rng.normal(size=(1 << n, B)) + 1j * rng.normal(size=(1 << n, B))
+    cols /= np.linalg.norm(cols, axis=0)
+    ev = mq.expectation(W.xxz(n), mq.BatchStateVector(cols))
+    for b in range(B):
+        assert abs(ev[b] - O.expect(cols[:, b], n, W.xxz(n).specs())) <= 1e-11
