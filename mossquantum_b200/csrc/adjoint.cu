@@ -13,6 +13,7 @@
 // parameter gradient as promoting at the first channel.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <memory>
 #include <vector>
 
@@ -108,6 +109,58 @@ extern "C" int mb_adjoint(mb_circuit c, mb_observable o, mb_state init, const do
     if ((rc = launch_to_density(init->d, y.p, n, B, st))) return rc;
   } else {
     MB_CHECK_CUDA(cudaMemcpyAsync(y.p, init->d, sbytes, cudaMemcpyDeviceToDevice, st));
+  }
+
+  // Fused path: pure single states with unitary circuits (specialised dual-state passes).
+  const int nops_all = int(c->ops.size());
+  const char* plain_env = getenv("MB_ADJOINT_PLAIN");
+  if (!is_dm && B == 1 && !c->has_channel && n >= 9 && nops_all > 0 && !(plain_env && atoi(plain_env))) {
+    const int kf = checkpoint_every > 0 ? checkpoint_every : nops_all;
+    const int Sf = (nops_all + kf - 1) / kf;
+    std::vector<Schedule*> adj(Sf, nullptr), fwd(Sf, nullptr);
+    bool ok = true;
+    for (int s2 = 0; s2 < Sf && ok; ++s2) {
+      const int lo = s2 * kf, hi = std::min(nops_all, (s2 + 1) * kf);
+      ok = adjoint_prepare(c, n, lo, hi, &adj[s2]) == MB_OK && get_schedule_ex(c, n, 0, 0, lo, hi, 1, &fwd[s2]) == MB_OK;
+    }
+    if (ok) {
+      std::vector<std::unique_ptr<Buf>> ck(Sf);
+      for (int s2 = 0; s2 < Sf; ++s2) {
+        if (checkpoint_every > 0) {
+          ck[s2].reset(new Buf());
+          if ((rc = ck[s2]->alloc(sbytes))) return rc;
+          MB_CHECK_CUDA(cudaMemcpyAsync(ck[s2]->p, y.p, sbytes, cudaMemcpyDeviceToDevice, st));
+        }
+        if ((rc = run_schedule(c, fwd[s2], y.p, 1, 0))) return rc;
+      }
+      mb_state_s view;
+      view.kind = MB_PURE;
+      view.n = n;
+      view.batch = 1;
+      view.dim = int64_t(1) << n;
+      view.elems = elems;
+      view.d = y.p;
+      if ((rc = o->pauli_ok ? expect_pauli(o, &view) : expect_keys(o, &view))) return rc;
+      double2 r0;
+      MB_CHECK_CUDA(cudaMemcpyAsync(&r0, g_ctx.results, sizeof(double2), cudaMemcpyDeviceToHost, st));
+      MB_CHECK_CUDA(cudaStreamSynchronize(st));
+      *value = w[0] * r0.x;
+      bool seeded = false;
+      if (o->pauli_ok && (rc = pauli_apply(o, y.p, delta.p, n, 1, 2.0, &seeded))) return rc;
+      if (!seeded) {
+        if ((rc = observable_apply(o, y.p, delta.p, n, 0, 1))) return rc;
+        if ((rc = launch_scale(delta.p, elems, 2.0, st))) return rc;
+      }
+      for (int s2 = Sf - 1; s2 >= 0; --s2) {
+        if ((rc = run_adjoint_schedule(c, adj[s2], y.p, delta.p, d_g))) return rc;
+        if (ck[s2]) MB_CHECK_CUDA(cudaMemcpyAsync(y.p, ck[s2]->p, sbytes, cudaMemcpyDeviceToDevice, st));
+      }
+      std::vector<double> gh(std::max(1, c->nslots));
+      if (c->nslots) MB_CHECK_CUDA(cudaMemcpyAsync(gh.data(), d_g, sizeof(double) * c->nslots, cudaMemcpyDeviceToHost, st));
+      MB_CHECK_CUDA(cudaStreamSynchronize(st));
+      for (int q = 0; q < c->nslots; ++q) grad[q] = w[0] * gh[q];
+      return MB_OK;
+    }
   }
 
   // Segments of k instructions; checkpoint where a segment holds a channel or k was given.

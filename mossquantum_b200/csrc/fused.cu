@@ -177,6 +177,7 @@ struct FOp {
   uint32_t active = 0;
   int conj = 0, param = 0;
   bool neg = false;           // MOP_CPHASE with factor -1 (a sign flip)
+  int slot = -1;              // MOP_GRAD: parameter slot
   // plain fallback
   int cls = CLS_DENSE;
   int mat_off = 0, mode = MAT_PLAIN;
@@ -187,6 +188,10 @@ struct FOp {
 
 struct Schedule {
   int N = 0, dm = 0, t = 0, R = 0, nsamples = 1;
+  int lo = 0, hi = -1;  // instruction range [lo, hi) of the circuit
+  int adjoint = 0;      // reverse sweep with gradient accumulators
+  int* d_gslots = nullptr;
+  int max_grad = 0;     // most gradient accumulators in one pass
   int jit = 0;  // 0 not tried, 1 specialised kernels ready, -1 interpreter kernels
   bool dagger = false;
   std::vector<FOp> fops;
@@ -347,10 +352,12 @@ static void mark_unfusable_masks(FOp& f) {
   f.nd = f.all;
 }
 
-static void build_fops(mb_circuit c, int n, int dm, bool dagger, std::vector<FOp>& out) {
+static void build_fops(mb_circuit c, int n, int dm, bool dagger, std::vector<FOp>& out, int lo = 0, int hi = -1) {
   out.clear();
   std::vector<FOp> seq;
-  for (const COp& op : c->ops) {
+  if (hi < 0) hi = int(c->ops.size());
+  for (int oi = lo; oi < hi; ++oi) {
+    const COp& op = c->ops[oi];
     if (op.kind == MB_OP_CHANNEL) {
       FOp f;
       f.nb = 2 * op.k;
@@ -381,6 +388,37 @@ static void build_fops(mb_circuit c, int n, int dm, bool dagger, std::vector<FOp
   for (FOp& f : seq) mark_unfusable_masks(f);
   if (dagger) std::reverse(seq.begin(), seq.end());
   out = seq;
+}
+
+// Reverse sweep of a pure-state circuit range: U' of every gate in reverse order, each active
+// parameter followed by its gradient accumulator (generator D in ordered form at gen_off).
+static bool build_adjoint_fops(mb_circuit c, int lo, int hi, std::vector<FOp>& out) {
+  out.clear();
+  for (int oi = hi - 1; oi >= lo; --oi) {
+    const COp& op = c->ops[oi];
+    if (op.kind != MB_OP_GATE) return false;
+    FOp u = gate_fop(c, op, 0, 0, true);
+    mark_unfusable_masks(u);
+    out.push_back(u);
+    if (op.gen_off >= 0) {
+      if (op.k > 2) return false;
+      FOp g;
+      g.type = MOP_GRAD;
+      g.nb = op.k;
+      for (int j = 0; j < op.k; ++j) g.bits[j] = op.pos[j];
+      g.ntgt = op.k;
+      for (int j = 0; j < op.k; ++j) g.tgt[j] = g.bits[j];
+      const int d = 1 << op.k;
+      for (int r = 0; r < d; ++r)
+        for (int cc = 0; cc < d; ++cc) g.off[r + d * cc] = op.gen_off + r + d * cc;
+      g.param = op.parametric ? 1 : 0;
+      g.slot = op.slot;
+      finalize_masks(g);
+      g.nd = g.all;
+      out.push_back(g);
+    }
+  }
+  return true;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -535,7 +573,22 @@ static void plan_stages(const std::vector<FOp>& fops, const std::vector<int>& op
         return -1;
       };
       auto sel = [&](int gbit) { return int16_t(loc[gbit] >= 0 ? loc[gbit] : 64 + gbit); };
-      if (f.type == MOP_U2) {
+      if (f.type == MOP_GRAD) {
+        m.nsel = int16_t(f.nb);
+        m.active = uint32_t(p.grad_slots.size());
+        p.grad_slots.push_back(f.slot);
+        int ra = regidx(f.tgt[0]), rb = f.nb > 1 ? regidx(f.tgt[1]) : -1;
+        if (f.nb > 1 && ra > rb) {
+          int o2[16];
+          const int sw[4] = {0, 2, 1, 3};
+          for (int r = 0; r < 4; ++r)
+            for (int cc = 0; cc < 4; ++cc) o2[r + 4 * cc] = f.off[sw[r] + 4 * sw[cc]];
+          std::memcpy(m.off, o2, sizeof(o2));
+          std::swap(ra, rb);
+        }
+        m.r0 = int16_t(ra);
+        m.r1 = int16_t(rb);
+      } else if (f.type == MOP_U2) {
         int ra = regidx(f.tgt[0]), rb = regidx(f.tgt[1]);
         if (ra > rb) {
           // swap the local bits of the 4x4 matrix so that local bit 0 is the lower register
@@ -624,7 +677,7 @@ static std::vector<int> window(int lo, int len, int N) {
   return w;
 }
 
-static void build_schedule(Schedule& S, int nsamples) {
+static void build_schedule(Schedule& S, int nsamples, bool allow_reg = true) {
   const int N = S.N, t = std::min(S.t, N), R = S.R;
   const uint64_t full = N >= 64 ? ~uint64_t(0) : ((uint64_t(1) << N) - 1);
   std::vector<int> rem(S.fops.size());
@@ -660,7 +713,7 @@ static void build_schedule(Schedule& S, int nsamples) {
           cands.push_back({PASS_TILE, b});
         }
         const int rlo = std::max(5, std::min(h0, N - R));
-        if (N - 5 >= R) cands.push_back({PASS_REG, window(rlo, R, N)});
+        if (allow_reg && N - 5 >= R) cands.push_back({PASS_REG, window(rlo, R, N)});
       }
     }
     double best = -1;
@@ -774,11 +827,14 @@ static Tuning tuning_for(int N) {
 
 }  // namespace
 
-int get_schedule(mb_circuit c, int n, int dm, bool dagger, int nsamples, Schedule** out) {
+int get_schedule_ex(mb_circuit c, int n, int dm, int adjoint, int lo, int hi, int nsamples, Schedule** out) {
   const int N = dm ? 2 * n : n;
+  if (hi < 0) hi = int(c->ops.size());
   Tuning tu = tuning_for(N);
+  if (adjoint) tu.t = std::min(tu.t, 11);  // y and delta tiles, double-buffered
   for (Schedule* s : c->scheds)
-    if (s->N == N && s->dm == dm && s->dagger == dagger && s->t == tu.t && s->R == tu.R && s->nsamples == nsamples) {
+    if (s->N == N && s->dm == dm && !s->dagger && s->t == tu.t && s->R == tu.R && s->nsamples == nsamples &&
+        s->lo == lo && s->hi == hi && s->adjoint == adjoint) {
       *out = s;
       return MB_OK;
     }
@@ -787,20 +843,33 @@ int get_schedule(mb_circuit c, int n, int dm, bool dagger, int nsamples, Schedul
   S->dm = dm;
   S->t = tu.t;
   S->R = tu.R;
-  S->dagger = dagger;
   S->nsamples = nsamples;
-  build_fops(c, n, dm, dagger, S->fops);
-  build_schedule(*S, nsamples);
+  S->lo = lo;
+  S->hi = hi;
+  S->adjoint = adjoint;
+  if (adjoint) {
+    if (dm || !build_adjoint_fops(c, lo, hi, S->fops)) {
+      set_error("the fused adjoint supports pure-state circuits with 1- and 2-qubit parameters");
+      return MB_EUNSUPPORTED;
+    }
+  } else {
+    build_fops(c, n, dm, false, S->fops, lo, hi);
+  }
+  build_schedule(*S, nsamples, !adjoint);
   std::vector<StageDesc> st;
   std::vector<MOp> mo;
+  std::vector<int> gs;
   for (Pass& p : S->passes) {
     p.stage_off = int(st.size());
     p.mop_off = int(mo.size());
+    p.grad_off = int(gs.size());
     for (StageDesc sd : p.stages) {
       sd.op0 += p.mop_off;
       st.push_back(sd);
     }
     mo.insert(mo.end(), p.mops.begin(), p.mops.end());
+    gs.insert(gs.end(), p.grad_slots.begin(), p.grad_slots.end());
+    S->max_grad = std::max(S->max_grad, int(p.grad_slots.size()));
   }
   int rc;
   if (!st.empty()) {
@@ -812,10 +881,19 @@ int get_schedule(mb_circuit c, int n, int dm, bool dagger, int nsamples, Schedul
     if ((rc = dev_alloc((void**)&S->d_mops, sizeof(MOp) * mo.size()))) return rc;
     MB_CHECK_CUDA(cudaMemcpyAsync(S->d_mops, mo.data(), sizeof(MOp) * mo.size(), cudaMemcpyHostToDevice, g_ctx.stream));
   }
+  if (!gs.empty()) {
+    if ((rc = dev_alloc((void**)&S->d_gslots, sizeof(int) * gs.size()))) return rc;
+    MB_CHECK_CUDA(cudaMemcpyAsync(S->d_gslots, gs.data(), sizeof(int) * gs.size(), cudaMemcpyHostToDevice, g_ctx.stream));
+  }
   MB_CHECK_CUDA(cudaStreamSynchronize(g_ctx.stream));
   *out = S.get();
   c->scheds.push_back(S.release());
   return MB_OK;
+}
+
+int get_schedule(mb_circuit c, int n, int dm, bool dagger, int nsamples, Schedule** out) {
+  (void)dagger;
+  return get_schedule_ex(c, n, dm, 0, 0, -1, nsamples, out);
 }
 
 // Specialised kernels are used from MB_JIT_MIN_BITS register bits on (default 18); MB_JIT=0
@@ -831,11 +909,12 @@ static bool want_jit(int N) {
 static void prepare_jit(Schedule* S) {
   if (S->jit != 0) return;
   S->jit = -1;
-  if (!want_jit(S->N) || !jit_available()) return;
+  if ((!want_jit(S->N) && !S->adjoint) || !jit_available()) return;
   std::vector<std::string> src;
   std::vector<Pass*> who;
   for (Pass& p : S->passes) {
-    if (p.kind == PASS_TILE) src.push_back(jit_tile_source(p, S->R, S->N));
+    if (p.kind == PASS_TILE && S->adjoint) src.push_back(jit_adjoint_source(p, S->R, S->N));
+    else if (p.kind == PASS_TILE) src.push_back(jit_tile_source(p, S->R, S->N));
     else if (p.kind == PASS_REG) src.push_back(jit_reg_source(p, S->N));
     else continue;
     who.push_back(&p);
@@ -935,6 +1014,72 @@ int run_schedule(mb_circuit c, Schedule* S, double2* v, int nsamples, int64_t ms
   return MB_OK;
 }
 
+// Reverse sweep over an adjoint schedule: U' on y and delta in every pass, gradient
+// contributions added into d_grad (one entry per parameter slot).
+int run_adjoint_schedule(mb_circuit c, Schedule* S, double2* y, double2* d, double* d_grad) {
+  cudaStream_t st = g_ctx.stream;
+  const int N = S->N;
+  const int64_t elems = int64_t(1) << N;
+  prepare_jit(S);
+  if (S->jit != 1) {
+    set_error("the fused adjoint needs the specialised kernels");
+    return MB_EUNSUPPORTED;
+  }
+  const int threads_chk = 1 << (S->t - S->R);
+  if (threads_chk < 32) {
+    set_error("state too small for the fused adjoint");
+    return MB_EUNSUPPORTED;
+  }
+  double* gpart = nullptr;
+  unsigned* gcount = nullptr;
+  const int grid_max = g_ctx.sm_count * 4;
+  int rc;
+  if ((rc = dev_alloc((void**)&gpart, sizeof(double) * std::max(1, S->max_grad) * grid_max))) return rc;
+  if ((rc = dev_alloc((void**)&gcount, sizeof(unsigned)))) {
+    dev_free(gpart);
+    return rc;
+  }
+  cudaMemsetAsync(gcount, 0, sizeof(unsigned), st);
+  for (const Pass& p : S->passes) {
+    if (p.kind == PASS_PLAIN) {
+      if ((rc = plain_fop_launch(c, S->fops[p.plain_fop], y, elems, 1, 0, st))) break;
+      if ((rc = plain_fop_launch(c, S->fops[p.plain_fop], d, elems, 1, 0, st))) break;
+      continue;
+    }
+    CUtensorMap my, md;
+    if ((rc = make_tmap(p, y, N, 1, &my)) || (rc = make_tmap(p, d, N, 1, &md))) break;
+    const int threads = 1 << (p.t - S->R);
+    const int nw = std::max(1, threads / 32);
+    const size_t shm = (size_t(64) << p.t) + 1024 + sizeof(double) * std::max<size_t>(1, p.grad_slots.size() * nw);
+    const int per_sm = std::max(1, int((227 * 1024) / (shm + 256)));
+    const int64_t ntiles = int64_t(1) << (N - p.t);
+    const int grid = int(std::min<int64_t>(ntiles, int64_t(g_ctx.sm_count) * std::min(per_sm, 4)));
+    ProfScope ps("k_adjoint_pass_jit", 64.0 * double(elems), st);
+    rc = jit_launch_adjoint((CUfunction)p.jit_fn, &my, &md, c->d_table, 0, ntiles, ntiles, g_ctx.flags + 2, gpart, gcount,
+                            d_grad, S->d_gslots + p.grad_off, threads, shm, grid, st);
+    ++launch_counter();
+    if (rc) break;
+  }
+  dev_free(gpart);
+  dev_free(gcount);
+  return rc;
+}
+
+// Adjoint schedule for instructions [lo, hi) with its specialised kernels compiled; fails
+// (MB_EUNSUPPORTED) when the range cannot run fused.
+int adjoint_prepare(mb_circuit c, int n, int lo, int hi, Schedule** out) {
+  Schedule* S = nullptr;
+  int rc = get_schedule_ex(c, n, 0, 1, lo, hi, 1, &S);
+  if (rc) return rc;
+  prepare_jit(S);
+  if (S->jit != 1 || (1 << (S->t - S->R)) < 32) {
+    set_error("the fused adjoint is unavailable for this circuit");
+    return MB_EUNSUPPORTED;
+  }
+  *out = S;
+  return MB_OK;
+}
+
 int apply_fused(mb_circuit c, mb_state s, int64_t mrow_stride) {
   const int dm = s->kind == MB_DENSITY || s->kind == MB_BATCH_DENSITY;
   const int N = dm ? 2 * s->n : s->n;
@@ -951,6 +1096,7 @@ void release_schedules(mb_circuit c) {
   for (Schedule* s : c->scheds) {
     dev_free(s->d_stages);
     dev_free(s->d_mops);
+    dev_free(s->d_gslots);
     delete s;
   }
   c->scheds.clear();

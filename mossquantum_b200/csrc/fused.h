@@ -15,6 +15,8 @@ enum MopType : int16_t {
   MOP_U2 = 3,     // dense 4x4 on register bits r0 < r1 (local bit 0 = r0)
   MOP_DIAG = 4,   // diagonal on up to 3 bits anywhere: factor of local index a where active
   MOP_CPHASE = 5, // factor off[0] (or a sign flip when r1 = 1) where every selector bit is 1
+  MOP_GRAD = 6,   // adjoint sweep: accumulate Re<y|D|delta> over register bits r0 (,r1);
+                  // nsel = 1 or 2 bits, active = gradient accumulator index within the pass
 };
 
 // A selector names one index bit: values < 64 are bits of the pass-local amplitude index,
@@ -58,6 +60,8 @@ struct Pass {
   int plain_fop = -1;           // PASS_PLAIN: index into the schedule's fused ops
   bool has_u2 = false;          // holds a 4x4 micro-op (selects the kernel variant)
   void* jit_fn = nullptr;       // specialised kernel (CUfunction) when the JIT is in use
+  std::vector<int> grad_slots;  // adjoint passes: parameter slot of each gradient accumulator
+  int grad_off = 0;             // offset of grad_slots in the schedule's device slot array
   TmaGeom geom{};
   int stage_off = 0, mop_off = 0;  // offsets into the schedule's device buffers
 };

@@ -115,11 +115,16 @@ int observable_apply(mb_observable o, const double2* in, double2* out, int n, in
 
 // fused.cu
 int apply_fused(mb_circuit c, mb_state s, int64_t mrow_stride);
+int get_schedule_ex(mb_circuit c, int n, int dm, int adjoint, int lo, int hi, int nsamples, Schedule** out);
+int run_schedule(mb_circuit c, Schedule* S, double2* v, int nsamples, int64_t mstride);
+int run_adjoint_schedule(mb_circuit c, Schedule* S, double2* y, double2* d, double* d_grad);
+int adjoint_prepare(mb_circuit c, int n, int lo, int hi, Schedule** out);
 void release_schedules(mb_circuit c);
 
 // pauli.cu
 int pauli_compile(mb_observable o, const mb_term* terms, size_t nterms);
 void pauli_free(mb_observable o);
 int expect_pauli(mb_observable o, mb_state s);
+int pauli_apply(mb_observable o, const double2* in, double2* out, int n, int nsamples, double scale, bool* done);
 
 }  // namespace mb

@@ -153,6 +153,7 @@ struct StageGen {
   std::ostringstream& o;
   bool lb64;           // pass-local index is a 64-bit global index (register sweep)
   std::vector<int> nm;
+  std::string pre = "a";  // variable prefix
 
   // Selector classification: register bit k (>= 0), or -1 with a runtime expression.
   int regbit(int sel) const {
@@ -177,7 +178,7 @@ struct StageGen {
       else cond += (cond.empty() ? "" : " & ") + rt(m.sel[c]);
     }
   }
-  std::string v(int j) const { return "a" + std::to_string(nm[j]); }
+  std::string v(int j) const { return pre + std::to_string(nm[j]); }
   std::string ldm(const MOp& m, int e) const {
     return std::string(m.conj ? "ldc" : "ld") + "(" + (m.param ? "tb" : "tab") + " + " + std::to_string(m.off[e]) + ")";
   }
@@ -435,6 +436,171 @@ std::string jit_tile_source(const Pass& p, int R, int N) {
   o << "  }\n  if (tx == 0) asm volatile(\"cp.async.bulk.wait_group 0;\" ::: \"memory\");\n}\n";
   (void)N;
   return o.str();
+}
+
+// Gradient accumulation of one MOP_GRAD op: thread sum of Re<y|D|delta> over its register
+// amplitudes, reduced across the warp and added to the warp's shared-memory slot.
+static void emit_grad(std::ostringstream& o, const MOp& m, const StageGen& gy, const StageGen& gd, int R, int nw) {
+  const int A = 1 << R;
+  const std::string tabn = m.param ? "tb" : "tab";
+  auto L = [&](int e) { return "ld(" + tabn + " + " + std::to_string(m.off[e]) + ")"; };
+  o << "{ double gs = 0.0;\n";
+  if (m.nsel == 1) {
+    const int b = 1 << m.r0;
+    o << "  const double2 D00 = " << L(0) << ", D10 = " << L(1) << ", D01 = " << L(2) << ", D11 = " << L(3) << ";\n";
+    for (int j = 0; j < A; ++j)
+      if (!(j & b))
+        o << "  { const double2 x0 = " << gd.v(j) << ", x1 = " << gd.v(j | b) << ", y0 = " << gy.v(j) << ", y1 = "
+          << gy.v(j | b) << "; const double2 e0 = cfma(D01, x1, cmul(D00, x0)), e1 = cfma(D11, x1, cmul(D10, x0)); "
+          << "gs += y0.x * e0.x + y0.y * e0.y + y1.x * e1.x + y1.y * e1.y; }\n";
+  } else {
+    const int b0 = 1 << m.r0, b1 = 1 << m.r1;
+    o << "  double2 D[16];";
+    for (int e = 0; e < 16; ++e) o << " D[" << e << "] = " << L(e) << ";";
+    o << "\n";
+    for (int j = 0; j < A; ++j)
+      if (!(j & b0) && !(j & b1)) {
+        const int i[4] = {j, j | b0, j | b1, j | b0 | b1};
+        o << "  { const double2 x0 = " << gd.v(i[0]) << ", x1 = " << gd.v(i[1]) << ", x2 = " << gd.v(i[2]) << ", x3 = "
+          << gd.v(i[3]) << ";\n";
+        for (int r = 0; r < 4; ++r)
+          o << "    { const double2 e = cfma(D[" << (12 + r) << "], x3, cfma(D[" << (8 + r) << "], x2, cfma(D[" << (4 + r)
+            << "], x1, cmul(D[" << r << "], x0)))); const double2 yy = " << gy.v(i[r])
+            << "; gs += yy.x * e.x + yy.y * e.y; }\n";
+        o << "  }\n";
+      }
+  }
+  o << "  for (int off = 16; off > 0; off >>= 1) gs += __shfl_xor_sync(0xffffffffu, gs, off);\n";
+  o << "  if ((tx & 31u) == 0u) gw[" << m.active << " * " << nw << " + (tx >> 5)] += gs;\n}\n";
+}
+
+std::string jit_adjoint_source(const Pass& p, int R, int N) {
+  std::ostringstream o;
+  const int A = 1 << R;
+  const int threads = 1 << (p.t - R);
+  const int nw = std::max(1, threads / 32);
+  const int ngrad = int(p.grad_slots.size());
+  const TmaGeom& g = p.geom;
+  o << kPrelude;
+  o << "extern \"C\" __global__ void __launch_bounds__(" << threads << ", 1) mbk(const __grid_constant__ TMap tmy, "
+    << "const __grid_constant__ TMap tmd, const double2* __restrict__ tab, long long tstride, long long tps, "
+    << "long long ntiles, u32* err, double* gpart, u32* gcount, double* gout, const int* __restrict__ gslot) {\n";
+  o << "  extern __shared__ unsigned char smem_raw[];\n  __shared__ __align__(8) u64 bar[2];\n  __shared__ int s_abort;\n"
+    << "  __shared__ bool lastcta;\n";
+  const unsigned T = 1u << p.t;
+  o << "  double2* base0 = (double2*)(((unsigned long long)smem_raw + 1023ull) & ~1023ull);\n";
+  o << "  double2* ybuf[2] = {base0, base0 + " << T << "};\n  double2* dbuf[2] = {base0 + " << 2 * T << ", base0 + "
+    << 3 * T << "};\n";
+  o << "  double* gw = (double*)(base0 + " << 4 * T << ");\n";
+  o << "  const u32 tx = threadIdx.x;\n";
+  o << "  for (int i = tx; i < " << std::max(1, ngrad * nw) << "; i += blockDim.x) gw[i] = 0.0;\n";
+  o << "  if (tx == 0) { mbar_init(&bar[0]); mbar_init(&bar[1]); asm volatile(\"fence.mbarrier_init.release.cluster;\" ::: \"memory\"); s_abort = 0; }\n";
+  o << "  __syncthreads();\n";
+  auto geom = [&](const char* tile, const char* pre) {
+    std::ostringstream e;
+    e << "  const int " << pre << "b = (int)(" << tile << " / tps);\n";
+    e << "  u64 " << pre << "gb = (u64)(" << tile << " - (long long)" << pre << "b * tps);\n";
+    for (int q = 0; q < p.t; ++q) {
+      const int bit = p.bits[q];
+      e << "  " << pre << "gb = ((" << pre << "gb >> " << bit << ") << " << (bit + 1) << ") | (" << pre << "gb & "
+        << ((1ull << bit) - 1) << "ull);\n";
+    }
+    for (int d = 0; d < g.ndims; ++d) {
+      e << "  const int " << pre << "c" << d << " = ";
+      if (g.start[d] < 0) e << pre << "b;\n";
+      else if (d == 0) e << "(int)(2ull * (" << pre << "gb & " << ((1ull << g.bits[0]) - 1) << "ull));\n";
+      else e << "(int)((" << pre << "gb >> " << g.start[d] << ") & " << ((1ull << g.bits[d]) - 1) << "ull);\n";
+    }
+    return e.str();
+  };
+  auto subst = [&](std::string s, const char* pre, const char* map, const char* dst, const char* bar) {
+    for (int d = 0; d < g.ndims && pre[0]; ++d) {
+      const std::string from = "\"r\"(c" + std::to_string(d) + ")", to = std::string("\"r\"(") + pre + "c" + std::to_string(d) + ")";
+      size_t pos;
+      while ((pos = s.find(from)) != std::string::npos) s.replace(pos, from.size(), to);
+    }
+    size_t pos;
+    while ((pos = s.find("&tmap")) != std::string::npos) s.replace(pos, 5, map);
+    while ((pos = s.find("DST")) != std::string::npos) s.replace(pos, 3, dst);
+    while ((pos = s.find("SRC")) != std::string::npos) s.replace(pos, 3, dst);
+    while ((pos = s.find("BAR")) != std::string::npos) s.replace(pos, 3, bar);
+    return s;
+  };
+  const std::string ld = tma_ld(g.ndims), st = tma_st(g.ndims);
+  const unsigned bytes = 32u << p.t;  // y and delta tiles
+  o << "  u32 ph0 = 0, ph1 = 0;\n  long long tile = blockIdx.x;\n";
+  o << "  if (tx == 0 && tile < ntiles) {\n" << geom("tile", "p_") << "    mbar_tx(&bar[0], " << bytes << "u);\n    "
+    << subst(ld, "p_", "&tmy", "ybuf[0]", "&bar[0]") << "\n    " << subst(ld, "p_", "&tmd", "dbuf[0]", "&bar[0]")
+    << "\n  }\n";
+  o << "  for (int it = 0; tile < ntiles; ++it, tile += gridDim.x) {\n    const int cur = it & 1;\n"
+    << "    const long long nxt = tile + gridDim.x;\n";
+  o << "    if (tx == 0 && nxt < ntiles) {\n" << geom("nxt", "n_")
+    << "      asm volatile(\"cp.async.bulk.wait_group.read 0;\" ::: \"memory\");\n      mbar_tx(&bar[cur ^ 1], " << bytes
+    << "u);\n      " << subst(ld, "n_", "&tmy", "ybuf[cur ^ 1]", "&bar[cur ^ 1]") << "\n      "
+    << subst(ld, "n_", "&tmd", "dbuf[cur ^ 1]", "&bar[cur ^ 1]") << "\n    }\n";
+  o << geom("tile", "");
+  o << "    const double2* tb = tab + (long long)b * tstride;\n    (void)tb; (void)gb;\n";
+  o << "    double2* ty = ybuf[cur]; double2* td = dbuf[cur];\n";
+  o << "    if (!mbar_wait(&bar[cur], cur ? ph1 : ph0)) { atomicOr(err, 1u); s_abort = 1; }\n";
+  o << "    if (cur) ph1 ^= 1u; else ph0 ^= 1u;\n    __syncthreads();\n    if (s_abort) break;\n";
+  o << "    double2 ";
+  for (int j = 0; j < A; ++j) o << (j ? ", " : "") << "y" << j << ", d" << j;
+  o << ";\n";
+  for (const StageDesc& sd : p.stages) {
+    o << "    {\n      const u32 lb = 0u";
+    for (int q = 0; q < sd.ntid; ++q) o << " | (((tx >> " << q << ") & 1u) << " << sd.tid[q] << ")";
+    o << ";\n";
+    for (int j = 0; j < A; ++j)
+      o << "      y" << j << " = ty[swz(lb | " << reg_off_const(j, R, sd.reg) << ")]; d" << j << " = td[swz(lb | "
+        << reg_off_const(j, R, sd.reg) << ")];\n";
+    StageGen gy{R, sd.reg, o, false, std::vector<int>(A), "y"};
+    StageGen gd{R, sd.reg, o, false, std::vector<int>(A), "d"};
+    for (int j = 0; j < A; ++j) gy.nm[j] = gd.nm[j] = j;
+    for (int q = 0; q < sd.nops; ++q) {
+      const MOp& m = p.mops[sd.op0 + q];
+      if (m.type == MOP_GRAD) {
+        emit_grad(o, m, gy, gd, R, nw);
+      } else {
+        gy.emit(m);
+        gd.emit(m);
+      }
+    }
+    for (int j = 0; j < A; ++j)
+      o << "      ty[swz(lb | " << reg_off_const(j, R, sd.reg) << ")] = " << gy.v(j) << "; td[swz(lb | "
+        << reg_off_const(j, R, sd.reg) << ")] = " << gd.v(j) << ";\n";
+    o << "      __syncthreads();\n    }\n";
+  }
+  o << "    asm volatile(\"fence.proxy.async.shared::cta;\" ::: \"memory\");\n    __syncthreads();\n";
+  o << "    if (tx == 0) { " << subst(st, "", "&tmy", "ty", "") << " " << subst(st, "", "&tmd", "td", "") << " }\n";
+  o << "  }\n  if (tx == 0) asm volatile(\"cp.async.bulk.wait_group 0;\" ::: \"memory\");\n";
+  // Gradient partials: per CTA, then the last CTA sums over CTAs in order.
+  if (ngrad > 0) {
+    o << "  __syncthreads();\n";
+    o << "  for (int gi = tx; gi < " << ngrad << "; gi += blockDim.x) { double s = 0.0; for (int w = 0; w < " << nw
+      << "; ++w) s += gw[gi * " << nw << " + w]; gpart[(long long)gi * gridDim.x + blockIdx.x] = s; }\n";
+    o << "  __threadfence();\n  __syncthreads();\n";
+    o << "  if (tx == 0) lastcta = atomicAdd(gcount, 1u) == gridDim.x - 1;\n  __syncthreads();\n";
+    o << "  if (lastcta) {\n    __threadfence();\n    for (int gi = tx; gi < " << ngrad
+      << "; gi += blockDim.x) { double s = 0.0; for (unsigned c = 0; c < gridDim.x; ++c) s += __ldcg(&gpart[(long long)gi * gridDim.x + c]); atomicAdd(&gout[gslot[gi]], s); }\n";
+    o << "    __syncthreads();\n    if (tx == 0) *gcount = 0u;\n  }\n";
+  }
+  o << "}\n";
+  (void)N;
+  return o.str();
+}
+
+int jit_launch_adjoint(CUfunction fn, const CUtensorMap* my, const CUtensorMap* md, const double2* tab, int64_t tstride,
+                       int64_t tps, int64_t ntiles, unsigned* err, double* gpart, unsigned* gcount, double* gout,
+                       const int* gslot, int threads, size_t shm, int grid, cudaStream_t st) {
+  Drv& d = drv();
+  if (d.setattr(fn, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, int(shm)) != CUDA_SUCCESS) return MB_EDEVICE;
+  long long ts = tstride, tp = tps, nt = ntiles;
+  void* params[] = {(void*)my, (void*)md, (void*)&tab, &ts, &tp, &nt, &err, &gpart, &gcount, &gout, (void*)&gslot};
+  if (d.launch(fn, grid, 1, 1, threads, 1, 1, unsigned(shm), (CUstream)st, params, nullptr) != CUDA_SUCCESS) {
+    set_error("JIT adjoint launch failed");
+    return MB_EDEVICE;
+  }
+  return MB_OK;
 }
 
 std::string jit_reg_source(const Pass& p, int N) {

@@ -152,6 +152,63 @@ __global__ void __launch_bounds__(kPThreads) k_pauli_pass(const double2* __restr
   }
 }
 
+// Seed variant: out (+)= scale * H psi, with (P psi)_j = i^{#Y} (-1)^{|(j^x)&z|} psi_{j^x}.
+// Same pass structure as k_pauli_pass; each pass adds the groups it holds.
+__global__ void __launch_bounds__(kPThreads) k_pauli_apply(const double2* __restrict__ v, double2* __restrict__ out,
+                                                          const PPassArgs a, double scale, int first) {
+  __shared__ double2 mirror[1 << kPR][kPThreads];
+  const int b = blockIdx.y, G = gridDim.x;
+  const double2* vs = v + (int64_t(b) << a.n);
+  double2* os = out + (int64_t(b) << a.n);
+  int reg[kPR];
+#pragma unroll
+  for (int k = 0; k < kPR; ++k) reg[k] = a.reg[k];
+  for (int64_t t0 = int64_t(blockIdx.x) * blockDim.x; t0 < a.threads_per_sample; t0 += int64_t(G) * blockDim.x) {
+    const int64_t t = t0 + threadIdx.x;
+    if (t >= a.threads_per_sample) break;
+    uint64_t base = uint64_t(t);
+#pragma unroll
+    for (int k = 0; k < kPR; ++k) {
+      const int p = reg[k];
+      base = ((base >> p) << (p + 1)) | (base & ((uint64_t(1) << p) - 1));
+    }
+#pragma unroll
+    for (int j = 0; j < (1 << kPR); ++j) {
+      uint64_t o = 0;
+#pragma unroll
+      for (int k = 0; k < kPR; ++k)
+        if ((j >> k) & 1) o |= uint64_t(1) << reg[k];
+      mirror[j][threadIdx.x] = vs[base | o];
+    }
+#pragma unroll
+    for (int j = 0; j < (1 << kPR); ++j) {
+      uint64_t o = 0;
+#pragma unroll
+      for (int k = 0; k < kPR; ++k)
+        if ((j >> k) & 1) o |= uint64_t(1) << reg[k];
+      double2 r = first ? cz() : os[base | o];
+      for (int gi = 0; gi < a.ngroups; ++gi) {
+        const PGroup g = a.groups[a.g0 + gi];
+        double2 p = mirror[j ^ g.xreg][threadIdx.x];
+        if (g.xlow) {
+          p.x = __shfl_xor_sync(0xffffffffu, p.x, g.xlow);
+          p.y = __shfl_xor_sync(0xffffffffu, p.y, g.xlow);
+        }
+        const uint64_t k_idx = (base | o) ^ g.x;
+        double2 f = cz();
+        for (int s = 0; s < g.ns; ++s) {
+          const PString ps = a.strings[g.s0 + s];
+          const bool odd = __popcll(k_idx & ps.z) & 1;
+          f.x += odd ? -ps.c.x : ps.c.x;
+          f.y += odd ? -ps.c.y : ps.c.y;
+        }
+        r = cfma(cscale(f, scale), p, r);
+      }
+      os[base | o] = r;
+    }
+  }
+}
+
 // Pauli coefficients of a 2x2 matrix M = sum_P a_P P with a_P = tr(P M)/2 (P in I,X,Y,Z).
 void pauli_decompose(const double* m, cdd a[4]) {
   const cdd m00(m[0], m[1]), m10(m[2], m[3]), m01(m[4], m[5]), m11(m[6], m[7]);
@@ -328,4 +385,29 @@ int expect_pauli(mb_observable o, mb_state s) {
   return MB_OK;
 }
 
+}  // namespace mb
+
+namespace mb {
+// out = scale * H in for pure states (the adjoint seed 2H psi); false when the fused form
+// does not apply to this register size (the caller then uses the per-key kernels).
+int pauli_apply(mb_observable o, const double2* in, double2* out, int n, int nsamples, double scale, bool* done) {
+  *done = false;
+  PauliProgram* P = nullptr;
+  int rc = pauli_program(o, n, &P);
+  if (rc || !P) return rc;
+  cudaStream_t st = g_ctx.stream;
+  bool first = true;
+  for (const PPassArgs& pa : P->passes) {
+    if (pa.ngroups == 0) continue;
+    const int64_t blocks = (pa.threads_per_sample + kPThreads - 1) / kPThreads;
+    const int G = int(std::min<int64_t>(blocks, int64_t(g_ctx.sm_count) * 16));
+    ProfScope ps("k_pauli_apply", (first ? 32.0 : 48.0) * double(int64_t(1) << n) * nsamples, st);
+    k_pauli_apply<<<dim3(G, nsamples), kPThreads, 0, st>>>(in, out, pa, scale, first ? 1 : 0);
+    MB_LAUNCHED();
+    first = false;
+  }
+  if (first) MB_CHECK_CUDA(cudaMemsetAsync(out, 0, sizeof(double2) * (size_t(1) << n) * nsamples, st));
+  *done = true;
+  return MB_OK;
+}
 }  // namespace mb

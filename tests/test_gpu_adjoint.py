@@ -134,3 +134,57 @@ def test_value_and_pullback(mq):
     v, back = mq.value_and_pullback(mq.AdjointGradient(), obj, [0.37])
     assert back(2.0)[0] == pytest.approx(-2 * np.sin(0.37), abs=1e-13)
     assert back(0.0)[0] == 0.0
+
+
+def _with_env(key, value, fn):
+    import os
+    old = os.environ.get(key)
+    os.environ[key] = value
+    try:
+        return fn()
+    finally:
+        if old is None:
+            del os.environ[key]
+        else:
+            os.environ[key] = old
+
+
+@pytest.mark.parametrize("n,depth,ck", [(10, 3, 0), (13, 4, 17), (16, 2, 0)])
+def test_fused_adjoint_vs_plain_and_oracle(mq, O, n, depth, ck):
+    """The fused dual-state reverse sweep equals the plain per-gate sweep and the oracle."""
+    from mossquantum_b200 import workloads as W
+    rng = np.random.default_rng(n)
+    c = W.hea_circuit(n, depth, W.hea_angles(n, depth, W.rng_for(13, n)))
+    t = lambda: float(rng.uniform(-np.pi, np.pi))
+    c.push(mq.CRxGate(2, 5, t(), isparas=True))
+    c.push(mq.CRyGate(n, 1, t(), isparas=True))
+    c.push(mq.CPHASEGate(3, 4, t(), isparas=True))
+    c.push(mq.RyGate(6, t(), isparas=True).adjoint())
+    c.push(mq.QuantumGate((1, 2, 3), np.linalg.qr(rng.normal(size=(8, 8)) + 1j * rng.normal(size=(8, 8)))[0]))
+    c.push(mq.PHASEGate(n, t(), isparas=True))
+    H = W.tfim(n) + W.xxz(n) * 0.5
+    obj = mq.ExpectationObjective(c, H, mq.StateVector(n))
+    theta = np.array(c.active_parameters())
+    v, g = mq.value_and_gradient(mq.AdjointGradient(checkpoint_every=ck), obj, theta)
+    vp, gp = _with_env("MB_ADJOINT_PLAIN", "1",
+                       lambda: mq.value_and_gradient(mq.AdjointGradient(checkpoint_every=ck), obj, theta))
+    vr, gr = O.adjoint(c.specs(), O.zero_state(n), n, H.specs())
+    assert abs(v - vr) <= 1e-11 and abs(vp - vr) <= 1e-11
+    assert np.max(np.abs(g - gr)) <= 1e-10 and np.max(np.abs(gp - gr)) <= 1e-10
+
+
+def test_fused_adjoint_shared_parameters(mq, O):
+    from mossquantum_b200 import workloads as W
+    n, depth = 11, 3
+    c = W.hea_circuit(n, depth, W.hea_angles(n, depth, W.rng_for(14)))
+    P = c.nparameters()
+    ids = [(i % (P // 3)) + 1 for i in range(P)]
+    pm = mq.ParameterMap(c, ids)
+    obj = mq.ExpectationObjective(c, W.tfim(n), mq.StateVector(n), parameter_map=pm)
+    x = np.random.default_rng(1).uniform(0, 2 * np.pi, size=pm.nparameters())
+    v, g = mq.value_and_gradient(mq.AdjointGradient(), obj, x)
+    slots = pm.expand(x)
+    cb = c.copy().reset_parameters(slots)
+    vr, gr = O.adjoint(cb.specs(), O.zero_state(n), n, W.tfim(n).specs())
+    assert abs(v - vr) <= 1e-11
+    assert np.max(np.abs(g - mq.accumulate_parameter_gradients(pm, gr))) <= 1e-10
