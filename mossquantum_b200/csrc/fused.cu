@@ -282,8 +282,7 @@ static FOp gate_fop(mb_circuit c, const COp& op, int shift, int conj, bool dagge
         f.type = f.nctrl ? MOP_CTRL : MOP_U1;
         if (f.nctrl > 4) f.type = F_UNFUSABLE;
         f.conj = fconj;
-        finalize_masks(f);
-        f.nd = 0;  // diagonal: commutes with every other diagonal and control
+        finalize_masks(f);  // the target must sit in a register like any 2x2 op
         return f;
       }
     }
@@ -856,6 +855,19 @@ int get_schedule_ex(mb_circuit c, int n, int dm, int adjoint, int lo, int hi, in
     build_fops(c, n, dm, false, S->fops, lo, hi);
   }
   build_schedule(*S, nsamples, !adjoint);
+  // Every register op must name register bits inside the stage width.
+  for (const Pass& p : S->passes) {
+    const int R = p.kind == PASS_REG ? p.t : S->R;
+    for (const MOp& m : p.mops) {
+      const bool needs = m.type == MOP_U1 || m.type == MOP_CTRL || m.type == MOP_CTRLX || m.type == MOP_U2 ||
+                         m.type == MOP_GRAD;
+      const bool two = m.type == MOP_U2 || (m.type == MOP_GRAD && m.nsel == 2);
+      if (needs && (m.r0 < 0 || m.r0 >= R || (two && (m.r1 <= m.r0 || m.r1 >= R)))) {
+        set_error("internal scheduling error: micro-op %d without a register target", int(m.type));
+        return MB_EUNSUPPORTED;
+      }
+    }
+  }
   std::vector<StageDesc> st;
   std::vector<MOp> mo;
   std::vector<int> gs;
