@@ -192,8 +192,8 @@ struct StageGen {
           << ", m11 = " << ldm(m, 3) << ";\n";
         for (int j = 0; j < A; ++j)
           if (!(j & b))
-            o << "  { const double2 x = " << v(j) << ", y = " << v(j | b) << "; " << v(j)
-              << " = cfma(m01, y, cmul(m00, x)); " << v(j | b) << " = cfma(m11, y, cmul(m10, x)); }\n";
+            o << "  { const double2 ux = " << v(j) << ", uy = " << v(j | b) << "; " << v(j)
+              << " = cfma(m01, uy, cmul(m00, ux)); " << v(j | b) << " = cfma(m11, uy, cmul(m10, ux)); }\n";
         o << "}\n";
         break;
       }
@@ -207,8 +207,8 @@ struct StageGen {
         if (!cond.empty()) o << " if (" << cond << ") {\n";
         for (int j = 0; j < A; ++j)
           if (!(j & b) && (j & need) == need)
-            o << "  { const double2 x = " << v(j) << ", y = " << v(j | b) << "; " << v(j)
-              << " = cfma(m01, y, cmul(m00, x)); " << v(j | b) << " = cfma(m11, y, cmul(m10, x)); }\n";
+            o << "  { const double2 ux = " << v(j) << ", uy = " << v(j | b) << "; " << v(j)
+              << " = cfma(m01, uy, cmul(m00, ux)); " << v(j | b) << " = cfma(m11, uy, cmul(m10, ux)); }\n";
         if (!cond.empty()) o << " }\n";
         o << "}\n";
         break;
@@ -225,8 +225,8 @@ struct StageGen {
           o << "{ const bool pr = (" << cond << ") != 0u;\n";
           for (int j = 0; j < A; ++j)
             if (!(j & b) && (j & need) == need)
-              o << "  { const double2 x = " << v(j) << ", y = " << v(j | b) << "; " << v(j) << " = pr ? y : x; "
-                << v(j | b) << " = pr ? x : y; }\n";
+              o << "  { const double2 ux = " << v(j) << ", uy = " << v(j | b) << "; " << v(j) << " = pr ? uy : ux; "
+                << v(j | b) << " = pr ? ux : uy; }\n";
           o << "}\n";
         }
         break;
@@ -450,9 +450,9 @@ static void emit_grad(std::ostringstream& o, const MOp& m, const StageGen& gy, c
     o << "  const double2 D00 = " << L(0) << ", D10 = " << L(1) << ", D01 = " << L(2) << ", D11 = " << L(3) << ";\n";
     for (int j = 0; j < A; ++j)
       if (!(j & b))
-        o << "  { const double2 x0 = " << gd.v(j) << ", x1 = " << gd.v(j | b) << ", y0 = " << gy.v(j) << ", y1 = "
-          << gy.v(j | b) << "; const double2 e0 = cfma(D01, x1, cmul(D00, x0)), e1 = cfma(D11, x1, cmul(D10, x0)); "
-          << "gs += y0.x * e0.x + y0.y * e0.y + y1.x * e1.x + y1.y * e1.y; }\n";
+        o << "  { const double2 gq0 = " << gd.v(j) << ", gq1 = " << gd.v(j | b) << ", gl0 = " << gy.v(j) << ", gl1 = "
+          << gy.v(j | b) << "; const double2 e0 = cfma(D01, gq1, cmul(D00, gq0)), e1 = cfma(D11, gq1, cmul(D10, gq0)); "
+          << "gs += gl0.x * e0.x + gl0.y * e0.y + gl1.x * e1.x + gl1.y * e1.y; }\n";
   } else {
     const int b0 = 1 << m.r0, b1 = 1 << m.r1;
     o << "  double2 D[16];";
@@ -461,12 +461,12 @@ static void emit_grad(std::ostringstream& o, const MOp& m, const StageGen& gy, c
     for (int j = 0; j < A; ++j)
       if (!(j & b0) && !(j & b1)) {
         const int i[4] = {j, j | b0, j | b1, j | b0 | b1};
-        o << "  { const double2 x0 = " << gd.v(i[0]) << ", x1 = " << gd.v(i[1]) << ", x2 = " << gd.v(i[2]) << ", x3 = "
+        o << "  { const double2 gq0 = " << gd.v(i[0]) << ", gq1 = " << gd.v(i[1]) << ", gq2 = " << gd.v(i[2]) << ", gq3 = "
           << gd.v(i[3]) << ";\n";
         for (int r = 0; r < 4; ++r)
-          o << "    { const double2 e = cfma(D[" << (12 + r) << "], x3, cfma(D[" << (8 + r) << "], x2, cfma(D[" << (4 + r)
-            << "], x1, cmul(D[" << r << "], x0)))); const double2 yy = " << gy.v(i[r])
-            << "; gs += yy.x * e.x + yy.y * e.y; }\n";
+          o << "    { const double2 e = cfma(D[" << (12 + r) << "], gq3, cfma(D[" << (8 + r) << "], gq2, cfma(D[" << (4 + r)
+            << "], gq1, cmul(D[" << r << "], gq0)))); const double2 gl = " << gy.v(i[r])
+            << "; gs += gl.x * e.x + gl.y * e.y; }\n";
         o << "  }\n";
       }
   }
