@@ -162,6 +162,33 @@ MB_API int mb_circuit_passes(mb_circuit c, int* npasses);
  * mirroring StateVector -> DensityMatrix in execution/channels.jl:19). */
 MB_API int mb_apply(mb_circuit c, mb_state s, const double* theta, size_t ntheta, int flags);
 
+/* ---- prepared execution: device-side inputs/outputs and CUDA-graph replay ---------------
+ * (the B200 counterpart of prepared plans / sweeps, src/execution/execution_plans.jl:12-240).
+ * A caller warms a sequence of calls up once (schedules, specialised kernels, buffers), then
+ * records it between mb_graph_begin and mb_graph_end and replays it with mb_graph_launch.
+ * Inside a recording only calls that neither synchronise nor allocate are allowed: mb_apply
+ * with MB_APPLY_DEVICE_THETA, mb_state_set_zero, mb_expect_to_device. */
+#define MB_APPLY_DEVICE_THETA 4  /* use the parameters last given to mb_theta_upload        */
+MB_API int mb_theta_upload(mb_circuit c, const double* theta, size_t ntheta, int rows);
+MB_API int mb_buffer_alloc(size_t bytes, void** dev);
+MB_API int mb_buffer_free(void* dev);
+MB_API int mb_buffer_download(const void* dev, void* host, size_t bytes);
+/* <H> per sample written as complex doubles to device memory (no host synchronisation). */
+MB_API int mb_expect_to_device(mb_observable o, mb_state s, double* dev_out);
+typedef struct mb_graph_s* mb_graph;
+MB_API int mb_graph_begin(void);
+MB_API int mb_graph_end(mb_graph* out);
+MB_API int mb_graph_launch(mb_graph g);
+MB_API int mb_graph_free(mb_graph g);
+
+/* ---- tuning: tile bits t (10..12) and register bits R (3..5) per register size ---------- */
+MB_API int mb_tuning_set(int nbits, int tile_bits, int reg_bits);
+MB_API int mb_tuning_get(int nbits, int* tile_bits, int* reg_bits);
+/* Times the fused execution of c on s for each candidate (t, R) and records the fastest for
+ * s's register size; best_ms receives its time per apply. */
+MB_API int mb_autotune(mb_circuit c, mb_state s, const double* theta, size_t ntheta, int flags, int* best_t,
+                       int* best_r, double* best_ms);
+
 /* ---- observables (QubitsOperator, src/observables/expectation.jl:1-73) ---------------- */
 MB_API int mb_observable_create(const mb_term* terms, size_t nterms, mb_observable* out);
 MB_API int mb_observable_free(mb_observable o);

@@ -30,7 +30,7 @@ MB_OP_GATE, MB_OP_CHANNEL = 0, 1
 FAMILIES = {"MATRIX": 0, "RX": 1, "RY": 2, "RZ": 3, "PHASE": 4, "CRX": 5, "CRY": 6, "CRZ": 7,
             "CPHASE": 8, "CCPHASE": 9}
 MB_OPF_ADJOINT = 1
-MB_APPLY_FUSED, MB_APPLY_PLAIN, MB_APPLY_PER_SAMPLE = 0, 1, 2
+MB_APPLY_FUSED, MB_APPLY_PLAIN, MB_APPLY_PER_SAMPLE, MB_APPLY_DEVICE_THETA = 0, 1, 2, 4
 
 
 class BackendError(RuntimeError):
@@ -107,6 +107,18 @@ def load():
         "mb_observable_apply": ([vp, vp, vp], ctypes.c_int),
         "mb_probabilities": ([vp, ip, ctypes.c_int, dp], ctypes.c_int),
         "mb_adjoint": ([vp, vp, vp, dp, sz, dp, ctypes.c_int, dp, dp], ctypes.c_int),
+        "mb_theta_upload": ([vp, dp, sz, ctypes.c_int], ctypes.c_int),
+        "mb_buffer_alloc": ([sz, ctypes.POINTER(vp)], ctypes.c_int),
+        "mb_buffer_free": ([vp], ctypes.c_int),
+        "mb_buffer_download": ([vp, vp, sz], ctypes.c_int),
+        "mb_expect_to_device": ([vp, vp, vp], ctypes.c_int),
+        "mb_graph_begin": ([], ctypes.c_int),
+        "mb_graph_end": ([ctypes.POINTER(vp)], ctypes.c_int),
+        "mb_graph_launch": ([vp], ctypes.c_int),
+        "mb_graph_free": ([vp], ctypes.c_int),
+        "mb_tuning_set": ([ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+        "mb_tuning_get": ([ctypes.c_int, ip, ip], ctypes.c_int),
+        "mb_autotune": ([vp, vp, dp, sz, ctypes.c_int, ip, ip, dp], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

@@ -1,0 +1,119 @@
+"""Uneven-size batches with per-sample parameters, replayed from a captured CUDA graph.
+
+MOSSQuantum's batches share one register size and one parameter vector
+(src/states/batch_state_vector.jl, docs/architecture.md). A ``BatchPlan`` accepts samples
+of different qubit counts, each with its own parameters: samples are grouped by size into
+device batches, every group runs the fused pass kernels over all of its samples at once
+(one launch per pass, tiles of every sample in the same persistent grid), and the whole
+sequence (reset, parameter binding, passes, expectations) is recorded once into a CUDA graph.
+``run`` uploads the parameters and replays the graph: one launch for the entire batch.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _native as N
+from .backend import apply_
+from .circuit import QCircuit
+from .operators import as_operator
+from .states import BatchDensityMatrix, BatchStateVector
+
+
+class BatchPlan:
+    """groups: {n: (template circuit for n qubits, samples B_n)}; observable_for(n) gives the
+    observable evaluated on every sample of size n. kind: "pure" or "density"."""
+
+    def __init__(self, groups, observable_for, kind="pure"):
+        self.kind = kind
+        self.groups = []
+        total = 0
+        for n in sorted(groups):
+            circuit, B = groups[n]
+            if not isinstance(circuit, QCircuit):
+                raise TypeError("each group needs a QCircuit")
+            state = BatchDensityMatrix(n, B) if kind == "density" else BatchStateVector(n, B)
+            obs = as_operator(observable_for(n))
+            compiled = circuit.compiled(n)
+            self.groups.append(dict(n=n, B=B, circuit=circuit, compiled=compiled, state=state, obs=obs,
+                                    offset=total))
+            total += B
+        self.total = total
+        buf = ctypes.c_void_p()
+        N.check(N.lib().mb_buffer_alloc(16 * max(1, total), ctypes.byref(buf)), "mb_buffer_alloc")
+        self.results = buf
+        self.graph = None
+        # Eager warm-up with zero parameters: builds schedules, kernels and reduction plans.
+        self._stage({g["n"]: np.zeros((g["B"], g["circuit"].nparameters())) for g in self.groups})
+        self._record_body()
+        N.synchronize()
+        self._capture()
+
+    def _stage(self, thetas):
+        for g in self.groups:
+            th = np.asarray(thetas[g["n"]], dtype=np.float64)
+            if th.shape != (g["B"], g["circuit"].nparameters()):
+                raise ValueError(f"parameters for n={g['n']} must have shape {(g['B'], g['circuit'].nparameters())}")
+            slots = np.ascontiguousarray(g["compiled"].theta_from(th))
+            N.check(N.lib().mb_theta_upload(g["compiled"].handle, N.dptr(slots), slots.size, g["B"]),
+                    "mb_theta_upload")
+
+    def _record_body(self):
+        L = N.lib()
+        for g in self.groups:
+            st = g["state"]
+            N.check(L.mb_state_set_zero(st.handle))
+            N.check(L.mb_apply(g["compiled"].handle, st.handle, None, 0,
+                               N.MB_APPLY_DEVICE_THETA | N.MB_APPLY_PER_SAMPLE), "apply (recorded)")
+            out = ctypes.c_void_p(self.results.value + 16 * g["offset"])
+            N.check(L.mb_expect_to_device(g["obs"].handle().handle, st.handle, out), "expectation (recorded)")
+
+    def _capture(self):
+        L = N.lib()
+        N.check(L.mb_graph_begin(), "mb_graph_begin")
+        try:
+            self._record_body()
+        except Exception:
+            h = ctypes.c_void_p()
+            L.mb_graph_end(ctypes.byref(h))
+            if h.value:
+                L.mb_graph_free(h)
+            raise
+        h = ctypes.c_void_p()
+        N.check(L.mb_graph_end(ctypes.byref(h)), "mb_graph_end")
+        self.graph = h
+
+    def run(self, thetas):
+        """thetas: {n: (B_n, P_n) per-sample parameters}. Returns {n: real <H> per sample}."""
+        self._stage(thetas)
+        N.check(N.lib().mb_graph_launch(self.graph), "mb_graph_launch")
+        host = np.zeros(2 * max(1, self.total))
+        N.check(N.lib().mb_buffer_download(self.results, host.ctypes.data_as(ctypes.c_void_p), 16 * self.total))
+        vals = host[0::2] + 1j * host[1::2]
+        return {g["n"]: vals[g["offset"]:g["offset"] + g["B"]] for g in self.groups}
+
+    def close(self):
+        if self.graph is not None:
+            N.lib().mb_graph_free(self.graph)
+            self.graph = None
+        if self.results:
+            N.lib().mb_buffer_free(self.results)
+            self.results = ctypes.c_void_p()
+
+
+def run_plain(groups, observable_for, thetas, kind="pure"):
+    """The plain per-call path: every sample separately, one plain kernel launch per gate."""
+    from .backend import expectation
+    from .states import DensityMatrix, StateVector
+    out = {}
+    for n in sorted(groups):
+        circuit, B = groups[n]
+        obs = observable_for(n)
+        vals = []
+        for b in range(B):
+            s = DensityMatrix(n) if kind == "density" else StateVector(n)
+            apply_(circuit, s, theta=thetas[n][b], plain=True)
+            vals.append(expectation(obs, s))
+        out[n] = np.array(vals)
+    return out

@@ -258,6 +258,7 @@ int state_alloc(int kind, int n, int batch, mb_state* out) {
 extern "C" int mb_state_create(int kind, int n, int batch, mb_state* out) {
   std::lock_guard<std::recursive_mutex> lk(g_mu);
   if (int rc = check_init()) return rc;
+  if (int rc = check_not_capturing("mb_state_create")) return rc;
   if (!out) return MB_EINVAL;
   int rc = state_alloc(kind, n, batch, out);
   if (rc) return rc;
@@ -282,6 +283,7 @@ extern "C" int mb_state_set_zero(mb_state s) {
 extern "C" int mb_state_upload(mb_state s, const double* host, size_t n_doubles) {
   std::lock_guard<std::recursive_mutex> lk(g_mu);
   if (int rc = check_init()) return rc;
+  if (int rc = check_not_capturing("mb_state_upload")) return rc;
   if (!s || (!host && n_doubles)) return MB_EINVAL;
   if (n_doubles != size_t(s->elems) * s->batch * 2) {
     set_error("upload of %zu doubles into a state of %zu doubles", n_doubles, size_t(s->elems) * s->batch * 2);
@@ -295,6 +297,7 @@ extern "C" int mb_state_upload(mb_state s, const double* host, size_t n_doubles)
 extern "C" int mb_state_download(mb_state s, double* host, size_t n_doubles) {
   std::lock_guard<std::recursive_mutex> lk(g_mu);
   if (int rc = check_init()) return rc;
+  if (int rc = check_not_capturing("mb_state_download")) return rc;
   if (!s || (!host && n_doubles)) return MB_EINVAL;
   if (n_doubles != size_t(s->elems) * s->batch * 2) {
     set_error("download of %zu doubles from a state of %zu doubles", n_doubles, size_t(s->elems) * s->batch * 2);
@@ -351,6 +354,7 @@ extern "C" int mb_state_to_density(mb_state src, mb_state dst) {
 extern "C" int mb_circuit_create(const mb_op* ops, size_t nops, int n, mb_circuit* out) {
   std::lock_guard<std::recursive_mutex> lk(g_mu);
   if (int rc = check_init()) return rc;
+  if (int rc = check_not_capturing("mb_circuit_create")) return rc;
   if (!out || (!ops && nops)) return MB_EINVAL;
   if (n < 0 || n > 32) {
     set_error("register size %d out of range", n);
@@ -564,7 +568,17 @@ namespace mb {
 
 // Uploads theta and evaluates every parametric matrix into the circuit's table.
 // rows = 1 (shared parameters) or the batch size (per-sample parameters).
-int bind_circuit(mb_circuit c, const double* theta, size_t ntheta, int rows) {
+int check_not_capturing(const char* what) {
+  if (g_ctx.capturing) {
+    set_error("%s synchronises or allocates and cannot be recorded into a CUDA graph", what);
+    return MB_EUNSUPPORTED;
+  }
+  return MB_OK;
+}
+
+// Validates theta and stages it into the circuit's device parameter buffer (asynchronously,
+// through pinned memory); makes room for `rows` matrix-table rows.
+int theta_stage(mb_circuit c, const double* theta, size_t ntheta, int rows) {
   if (ntheta != size_t(c->nslots) * rows) {
     set_error("expected %zu parameter values, got %zu", size_t(c->nslots) * rows, ntheta);
     return MB_EINVAL;
@@ -584,6 +598,7 @@ int bind_circuit(mb_circuit c, const double* theta, size_t ntheta, int rows) {
     c->d_table = t;
     c->table_rows = rows;
   }
+  c->theta_rows = rows;
   if (c->binds.empty()) return MB_OK;
   size_t need = std::max<size_t>(ntheta, 1);
   if (need > c->theta_cap) {
@@ -593,7 +608,6 @@ int bind_circuit(mb_circuit c, const double* theta, size_t ntheta, int rows) {
     c->theta_cap = need;
   }
   if (ntheta) {
-    // Pinned staging keeps the upload asynchronous with respect to the host.
     if (c->h_theta_cap < ntheta) {
       if (c->h_theta) cudaFreeHost(c->h_theta);
       MB_CHECK_CUDA(cudaMallocHost((void**)&c->h_theta, sizeof(double) * ntheta));
@@ -604,8 +618,20 @@ int bind_circuit(mb_circuit c, const double* theta, size_t ntheta, int rows) {
     MB_CHECK_CUDA(cudaMemcpyAsync(c->d_theta, c->h_theta, sizeof(double) * ntheta, cudaMemcpyHostToDevice,
                                   g_ctx.stream));
   }
+  return MB_OK;
+}
+
+// Evaluates every parametric matrix from the staged theta into the table (one launch).
+int bind_launch(mb_circuit c, int rows) {
+  if (c->binds.empty() || rows == 0) return MB_OK;
   return launch_bind(c->d_binds, int(c->binds.size()), c->d_theta, c->nslots, rows, c->d_table, c->table_elems,
                      g_ctx.stream);
+}
+
+int bind_circuit(mb_circuit c, const double* theta, size_t ntheta, int rows) {
+  int rc = theta_stage(c, theta, ntheta, rows);
+  if (rc) return rc;
+  return bind_launch(c, rows);
 }
 
 // Launches one instruction with the plain per-gate kernels. dagger applies U' (S' for
@@ -719,7 +745,16 @@ extern "C" int mb_apply(mb_circuit c, mb_state s, const double* theta, size_t nt
   }
   const int rows = per_sample ? s->batch : 1;
   if (rows == 0) return MB_OK;
-  if (int rc = bind_circuit(c, theta, ntheta, rows)) return rc;
+  if (flags & MB_APPLY_DEVICE_THETA) {
+    if (c->theta_rows != rows) {
+      set_error("mb_apply: staged parameters have %d rows, the state needs %d", c->theta_rows, rows);
+      return MB_EINVAL;
+    }
+    if (int rc = bind_launch(c, rows)) return rc;
+  } else {
+    if (int rc = check_not_capturing("mb_apply without MB_APPLY_DEVICE_THETA")) return rc;
+    if (int rc = bind_circuit(c, theta, ntheta, rows)) return rc;
+  }
   const int64_t stride = per_sample ? c->table_elems : 0;
   if (flags & MB_APPLY_PLAIN) return apply_plain(c, s, stride);
   return apply_fused(c, s, stride);
@@ -731,6 +766,7 @@ extern "C" int mb_apply(mb_circuit c, mb_state s, const double* theta, size_t nt
 extern "C" int mb_observable_create(const mb_term* terms, size_t nterms, mb_observable* out) {
   std::lock_guard<std::recursive_mutex> lk(g_mu);
   if (int rc = check_init()) return rc;
+  if (int rc = check_not_capturing("mb_observable_create")) return rc;
   if (!out || (!terms && nterms)) return MB_EINVAL;
   std::unique_ptr<mb_observable_s> o(new mb_observable_s());
   // Group terms by sorted site tuple and sum their dense local matrices
@@ -826,12 +862,13 @@ extern "C" int mb_observable_free(mb_observable o) {
 namespace mb {
 
 // <H> per sample into g_ctx.results[0..B-1] (device) using the dense-key kernels.
-int expect_keys(mb_observable o, mb_state s) {
+int expect_keys(mb_observable o, mb_state s, double2* out) {
   const int is_dm = s->kind == MB_DENSITY || s->kind == MB_BATCH_DENSITY;
   cudaStream_t st = g_ctx.stream;
-  MB_CHECK_CUDA(cudaMemsetAsync(g_ctx.results, 0, sizeof(double2) * s->batch, st));
+  if (!out) out = g_ctx.results;
+  MB_CHECK_CUDA(cudaMemsetAsync(out, 0, sizeof(double2) * s->batch, st));
   for (const OKey& k : o->keys) {
-    ReduceOut ro{g_ctx.results, nullptr, nullptr, 1};
+    ReduceOut ro{out, nullptr, nullptr, 1};
     Pos p{};
     p.k = k.k;
     for (int j = 0; j < k.k; ++j) p.p[j] = k.pos[j];
@@ -863,6 +900,7 @@ int validate_observable(mb_observable o, mb_state s) {
 extern "C" int mb_expect(mb_observable o, mb_state s, double* out) {
   std::lock_guard<std::recursive_mutex> lk(g_mu);
   if (int rc = check_init()) return rc;
+  if (int rc = check_not_capturing("mb_expect")) return rc;
   if (!o || !s || !out) return MB_EINVAL;
   if (int rc = validate_observable(o, s)) return rc;
   if (s->batch == 0) return MB_OK;
@@ -918,6 +956,7 @@ extern "C" int mb_observable_apply(mb_observable o, mb_state in, mb_state out) {
 extern "C" int mb_probabilities(mb_state s, const int* qubits, int nq, double* out) {
   std::lock_guard<std::recursive_mutex> lk(g_mu);
   if (int rc = check_init()) return rc;
+  if (int rc = check_not_capturing("mb_probabilities")) return rc;
   if (!s || !out || nq < 0 || (nq && !qubits)) return MB_EINVAL;
   // _readout_qubits (probabilities.jl:1-6)
   for (int j = 0; j < nq; ++j) {

@@ -22,7 +22,9 @@
 #include <complex>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <memory>
+#include <mutex>
 
 #include "fused_kernels.cuh"
 #include "jit.h"
@@ -816,8 +818,19 @@ struct Tuning {
   int t = 12, R = 4;
 };
 
+std::mutex g_tune_mu;
+std::map<int, std::pair<int, int>> g_tuning;  // register bits -> (tile bits, register bits)
+
 static Tuning tuning_for(int N) {
   Tuning tu;
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tuning.find(N);
+    if (it != g_tuning.end()) {
+      tu.t = it->second.first;
+      tu.R = it->second.second;
+    }
+  }
   if (const char* e = getenv("MB_TILE_BITS")) tu.t = std::max(8, std::min(12, atoi(e)));
   if (const char* e = getenv("MB_REG_BITS")) tu.R = std::max(3, std::min(5, atoi(e)));
   tu.t = std::min(tu.t, N);
@@ -837,6 +850,10 @@ int get_schedule_ex(mb_circuit c, int n, int dm, int adjoint, int lo, int hi, in
       *out = s;
       return MB_OK;
     }
+  if (g_ctx.capturing) {
+    set_error("run this circuit once on a state of this shape before capturing it (schedules are built lazily)");
+    return MB_EUNSUPPORTED;
+  }
   std::unique_ptr<Schedule> S(new Schedule());
   S->N = N;
   S->dm = dm;
@@ -1128,5 +1145,23 @@ extern "C" int mb_circuit_passes(mb_circuit c, int* npasses) {
   int rc = mb::get_schedule(c, c->n, 0, false, 1, &S);
   if (rc) return rc;
   *npasses = int(S->passes.size());
+  return MB_OK;
+}
+
+extern "C" int mb_tuning_set(int nbits, int tile_bits, int reg_bits) {
+  if (nbits < 1 || nbits > 40 || tile_bits < 8 || tile_bits > 12 || reg_bits < 3 || reg_bits > 5) {
+    mb::set_error("tuning out of range (tile bits 8..12, register bits 3..5)");
+    return MB_EINVAL;
+  }
+  std::lock_guard<std::mutex> lk(mb::g_tune_mu);
+  mb::g_tuning[nbits] = {tile_bits, reg_bits};
+  return MB_OK;
+}
+
+extern "C" int mb_tuning_get(int nbits, int* tile_bits, int* reg_bits) {
+  if (!tile_bits || !reg_bits) return MB_EINVAL;
+  mb::Tuning tu = mb::tuning_for(nbits);
+  *tile_bits = tu.t;
+  *reg_bits = tu.R;
   return MB_OK;
 }

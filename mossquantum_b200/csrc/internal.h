@@ -55,6 +55,7 @@ struct mb_circuit_s {
   size_t theta_cap = 0;
   double* h_theta = nullptr;          // pinned staging for theta uploads
   size_t h_theta_cap = 0;
+  int theta_rows = 0;                 // rows staged by the last theta upload
   std::vector<mb::Schedule*> scheds;  // fused schedules, built lazily per state shape
 };
 
@@ -93,6 +94,7 @@ struct Ctx {
   int ncounters = 0;
   double2* results = nullptr;
   unsigned* flags = nullptr;
+  bool capturing = false;           // the library stream is recording a CUDA graph
 };
 
 extern Ctx g_ctx;
@@ -105,12 +107,15 @@ ReduceWs ws();
 
 int state_alloc(int kind, int n, int batch, mb_state* out);
 int bind_circuit(mb_circuit c, const double* theta, size_t ntheta, int rows);
+int theta_stage(mb_circuit c, const double* theta, size_t ntheta, int rows);
+int bind_launch(mb_circuit c, int rows);
+int check_not_capturing(const char* what);
 int plain_op(mb_circuit c, const COp& op, double2* v, int n, int is_dm, int nsamples, int64_t mrow_stride,
              bool dagger);
 int apply_plain(mb_circuit c, mb_state s, int64_t mrow_stride);
 int validate_apply(mb_circuit c, mb_state s);
 int validate_observable(mb_observable o, mb_state s);
-int expect_keys(mb_observable o, mb_state s);
+int expect_keys(mb_observable o, mb_state s, double2* out = nullptr);
 int observable_apply(mb_observable o, const double2* in, double2* out, int n, int is_dm, int nsamples);
 
 // fused.cu
@@ -124,7 +129,7 @@ void release_schedules(mb_circuit c);
 // pauli.cu
 int pauli_compile(mb_observable o, const mb_term* terms, size_t nterms);
 void pauli_free(mb_observable o);
-int expect_pauli(mb_observable o, mb_state s);
+int expect_pauli(mb_observable o, mb_state s, double2* out = nullptr);
 int pauli_apply(mb_observable o, const double2* in, double2* out, int n, int nsamples, double scale, bool* done);
 
 }  // namespace mb

@@ -361,13 +361,23 @@ bool pauli_usable(mb_observable o, mb_state s) {
   return p != nullptr;
 }
 
-int expect_pauli(mb_observable o, mb_state s) {
+int expect_pauli(mb_observable o, mb_state s, double2* out) {
+  if (!out) out = g_ctx.results;
   PauliProgram* P = nullptr;
-  int rc = pauli_program(o, s->n, &P);
-  if (rc) return rc;
-  if (!P) return expect_keys(o, s);
+  if (g_ctx.capturing) {
+    for (PauliProgram* q : o->pauli->programs)
+      if (q->n == s->n) P = q;
+    if (!P && s->n >= 5 + kPR) {
+      set_error("record the expectation once before capturing it (its pass plan is built lazily)");
+      return MB_EUNSUPPORTED;
+    }
+  } else {
+    int rc = pauli_program(o, s->n, &P);
+    if (rc) return rc;
+  }
+  if (!P) return expect_keys(o, s, out);
   cudaStream_t st = g_ctx.stream;
-  MB_CHECK_CUDA(cudaMemsetAsync(g_ctx.results, 0, sizeof(double2) * s->batch, st));
+  MB_CHECK_CUDA(cudaMemsetAsync(out, 0, sizeof(double2) * s->batch, st));
   for (const PPassArgs& pa : P->passes) {
     if (pa.ngroups == 0) continue;
     const int64_t blocks = (pa.threads_per_sample + kPThreads - 1) / kPThreads;
@@ -379,7 +389,7 @@ int expect_pauli(mb_observable o, mb_state s) {
       return MB_EUNSUPPORTED;
     }
     ProfScope ps("k_pauli_pass", 16.0 * double(s->elems) * s->batch, st);
-    k_pauli_pass<<<dim3(G, s->batch), kPThreads, 0, st>>>(s->d, pa, g_ctx.partials, g_ctx.counters, g_ctx.results);
+    k_pauli_pass<<<dim3(G, s->batch), kPThreads, 0, st>>>(s->d, pa, g_ctx.partials, g_ctx.counters, out);
     MB_LAUNCHED();
   }
   return MB_OK;

@@ -1,0 +1,168 @@
+// Prepared execution: device-side parameters and results, CUDA-graph capture and replay
+// on the library stream, and the autotuner for the fused passes' tile/register widths.
+//
+// The reference prepares plans and sweeps on the host (src/execution/execution_plans.jl,
+// experiments.jl). Here a caller runs a sequence once eagerly (building schedules,
+// specialised kernels and reduction plans), records the same sequence into a CUDA graph and
+// replays it with new parameters: one graph launch per evaluation of a whole batch.
+#include <cstring>
+#include <vector>
+
+#include "internal.h"
+
+struct mb_graph_s {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+using namespace mb;
+
+extern "C" int mb_theta_upload(mb_circuit c, const double* theta, size_t ntheta, int rows) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (int rc = check_init()) return rc;
+  if (int rc = check_not_capturing("mb_theta_upload")) return rc;
+  if (!c || (!theta && ntheta) || rows < 1) return MB_EINVAL;
+  return theta_stage(c, theta, ntheta, rows);
+}
+
+extern "C" int mb_buffer_alloc(size_t bytes, void** dev) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (int rc = check_init()) return rc;
+  if (int rc = check_not_capturing("mb_buffer_alloc")) return rc;
+  if (!dev) return MB_EINVAL;
+  int rc = dev_alloc(dev, bytes);
+  if (rc) return rc;
+  MB_CHECK_CUDA(cudaMemsetAsync(*dev, 0, bytes, g_ctx.stream));
+  MB_CHECK_CUDA(cudaStreamSynchronize(g_ctx.stream));
+  return MB_OK;
+}
+
+extern "C" int mb_buffer_free(void* dev) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (!g_ctx.init || !dev) return MB_OK;
+  dev_free(dev);
+  return MB_OK;
+}
+
+extern "C" int mb_buffer_download(const void* dev, void* host, size_t bytes) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (int rc = check_init()) return rc;
+  if (int rc = check_not_capturing("mb_buffer_download")) return rc;
+  if ((!dev || !host) && bytes) return MB_EINVAL;
+  MB_CHECK_CUDA(cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, g_ctx.stream));
+  MB_CHECK_CUDA(cudaStreamSynchronize(g_ctx.stream));
+  return MB_OK;
+}
+
+extern "C" int mb_expect_to_device(mb_observable o, mb_state s, double* dev_out) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (int rc = check_init()) return rc;
+  if (!o || !s || !dev_out) return MB_EINVAL;
+  if (int rc = validate_observable(o, s)) return rc;
+  if (s->batch == 0) return MB_OK;
+  const int is_dm = s->kind == MB_DENSITY || s->kind == MB_BATCH_DENSITY;
+  double2* out = reinterpret_cast<double2*>(dev_out);
+  return (!is_dm && o->pauli_ok) ? expect_pauli(o, s, out) : expect_keys(o, s, out);
+}
+
+extern "C" int mb_graph_begin(void) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (int rc = check_init()) return rc;
+  if (g_ctx.capturing) {
+    set_error("a graph recording is already in progress");
+    return MB_EINVAL;
+  }
+  MB_CHECK_CUDA(cudaStreamSynchronize(g_ctx.stream));
+  MB_CHECK_CUDA(cudaStreamBeginCapture(g_ctx.stream, cudaStreamCaptureModeThreadLocal));
+  g_ctx.capturing = true;
+  return MB_OK;
+}
+
+extern "C" int mb_graph_end(mb_graph* out) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (int rc = check_init()) return rc;
+  if (!g_ctx.capturing || !out) {
+    set_error("no graph recording in progress");
+    return MB_EINVAL;
+  }
+  g_ctx.capturing = false;
+  auto g = new mb_graph_s();
+  cudaError_t e = cudaStreamEndCapture(g_ctx.stream, &g->graph);
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&g->exec, g->graph, 0);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    if (g->graph) cudaGraphDestroy(g->graph);
+    delete g;
+    set_error("graph recording failed: %s", cudaGetErrorString(e));
+    return MB_EDEVICE;
+  }
+  *out = g;
+  return MB_OK;
+}
+
+extern "C" int mb_graph_launch(mb_graph g) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (int rc = check_init()) return rc;
+  if (!g) return MB_EINVAL;
+  MB_CHECK_CUDA(cudaGraphLaunch(g->exec, g_ctx.stream));
+  ++launch_counter();
+  return MB_OK;
+}
+
+extern "C" int mb_graph_free(mb_graph g) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (!g) return MB_OK;
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  if (g->graph) cudaGraphDestroy(g->graph);
+  delete g;
+  return MB_OK;
+}
+
+// Candidate widths: tile bits t (shared-memory tile of 2^t amplitudes) and register bits R
+// (amplitudes per thread 2^R, i.e. how many gate qubits one register stage fuses).
+extern "C" int mb_autotune(mb_circuit c, mb_state s, const double* theta, size_t ntheta, int flags, int* best_t,
+                           int* best_r, double* best_ms) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (int rc = check_init()) return rc;
+  if (int rc = check_not_capturing("mb_autotune")) return rc;
+  if (!c || !s || !best_t || !best_r || !best_ms) return MB_EINVAL;
+  const int dm = s->kind == MB_DENSITY || s->kind == MB_BATCH_DENSITY;
+  const int N = dm ? 2 * s->n : s->n;
+  int t0 = 0, r0 = 0;
+  mb_tuning_get(N, &t0, &r0);
+  const int cand[][2] = {{12, 4}, {11, 4}, {10, 4}, {12, 3}, {11, 3}, {10, 3}};
+  double best = 1e300;
+  int bt = t0, br = r0;
+  cudaEvent_t a, b;
+  MB_CHECK_CUDA(cudaEventCreate(&a));
+  MB_CHECK_CUDA(cudaEventCreate(&b));
+  int rc = MB_OK;
+  for (auto& cd : cand) {
+    if (cd[0] > N) continue;
+    if ((rc = mb_tuning_set(N, cd[0], cd[1]))) break;
+    // warm-up builds the schedule and its kernels; then two timed applies
+    if ((rc = mb_apply(c, s, theta, ntheta, flags & ~MB_APPLY_PLAIN))) {
+      rc = MB_OK;  // a width this circuit cannot use (e.g. no specialised kernels): skip it
+      continue;
+    }
+    cudaEventRecord(a, g_ctx.stream);
+    for (int k = 0; k < 2 && !rc; ++k) rc = mb_apply(c, s, theta, ntheta, flags & ~MB_APPLY_PLAIN);
+    cudaEventRecord(b, g_ctx.stream);
+    cudaEventSynchronize(b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    if (!rc && ms / 2 < best) {
+      best = ms / 2;
+      bt = cd[0];
+      br = cd[1];
+    }
+    if (rc) break;
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  mb_tuning_set(N, bt, br);
+  *best_t = bt;
+  *best_r = br;
+  *best_ms = best;
+  return rc;
+}

@@ -1,0 +1,56 @@
+"""Uneven batches replayed from a CUDA graph, and the autotuner, vs the oracle.
+
+Per-sample parameters and mixed register sizes go beyond the reference's batches (one size,
+one parameter vector); each sample is checked against the oracle run alone. Tolerance
+1e-11 on expectations.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def test_ragged_plan_two_replays(mq, O):
+    from mossquantum_b200 import workloads as W
+    from mossquantum_b200.batch import BatchPlan
+    sizes = {9: 3, 10: 2, 12: 2, 13: 1}
+    depth = 2
+    groups = {n: (W.hea_circuit(n, depth), B) for n, B in sizes.items()}
+    plan = BatchPlan(groups, W.xxz)
+    rng = np.random.default_rng(5)
+    for _ in range(2):
+        thetas = {n: rng.uniform(0, 2 * np.pi, size=(B, groups[n][0].nparameters())) for n, B in sizes.items()}
+        res = plan.run(thetas)
+        for n, B in sizes.items():
+            for b in range(B):
+                c = groups[n][0].copy().reset_parameters(thetas[n][b])
+                ref = O.expect(O.apply(c.specs(), O.zero_state(n), n), n, W.xxz(n).specs())
+                assert abs(res[n][b] - ref) <= 1e-11
+    plan.close()
+
+
+def test_density_plan(mq, O):
+    from mossquantum_b200 import workloads as W
+    from mossquantum_b200.batch import BatchPlan
+    n, B = 4, 3
+    c = W.hea_circuit(n, 1, noise=(0.01, 0.02))
+    plan = BatchPlan({n: (c, B)}, W.xxz, kind="density")
+    th = np.random.default_rng(6).uniform(0, 2 * np.pi, size=(B, c.nparameters()))
+    res = plan.run({n: th})
+    for b in range(B):
+        cb = c.copy().reset_parameters(th[b])
+        rho = O.apply(cb.specs(), O.zero_state(n, True), n, True)
+        assert abs(res[n][b] - O.expect(rho, n, W.xxz(n).specs(), dm=True)) <= 1e-11
+    plan.close()
+
+
+def test_autotune_keeps_results(mq, O):
+    from mossquantum_b200 import autotune
+    from mossquantum_b200 import workloads as W
+    n = 14
+    c = W.u3_brickwork(n, 4, W.u3_params(n, 4, W.rng_for(20)))
+    t, r, ms = autotune.autotune(c, mq.StateVector(n))
+    assert (t, r) == autotune.get(n) and ms > 0
+    s = mq.apply_(c, mq.StateVector(n))
+    ref = O.apply(c.specs(), O.zero_state(n), n)
+    assert np.max(np.abs(s.to_numpy() - ref)) <= 1e-12
