@@ -40,9 +40,13 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
-    ap.add_argument("--workload", default="scale", choices=["scale", "batch"],
-                    help="scale: 28-qubit U3+CZ circuit (headline); batch: uneven batch of 512 pure + 64 density states")
+    ap.add_argument("--workload", default="scale", choices=["scale", "batch", "grad", "serve"],
+                    help="scale: 28-qubit U3+CZ circuit (headline); batch: uneven batch of 512 pure + 64 density "
+                         "states; grad: adjoint gradients (24 qubits, 1152 angles; 64 noisy density matrices); "
+                         "serve: Poisson request stream through the continuous-batching server")
     ap.add_argument("--plain-samples", type=int, default=48)
+    ap.add_argument("--rates", default="4,8,16", help="serve: arrival rates (requests/s) to sweep")
+    ap.add_argument("--requests", type=int, default=96, help="serve: requests per rate")
     return ap.parse_args()
 
 
@@ -115,6 +119,41 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def dominant_roofline(N, step, size_key):
+    """Roofline of the kernel with the largest share of one profiled step (CUDA events on the
+    library stream around every launch). Both views are reported: HBM (algorithmic bytes per
+    launch / duration vs the measured copy peak) and FP64 (algorithmic flops per launch /
+    duration vs the FP64 rate of a DFMA-only kernel measured here); `bound` is the view with
+    the larger fraction."""
+    N.profile(True)
+    step()
+    rep = N.profile_report()
+    N.profile(False)
+    if not rep:
+        return None
+    name, (lc, tms, byts, flops) = max(rep.items(), key=lambda kv: kv[1][1])
+    peak, peak_kind = load_peaks()
+    fp64_peak = N.measure_fp64_peak()
+    sec = tms / 1e3
+    hbm = {"achieved": byts / sec / 1e9, "peak": peak, "unit": "GB/s", "frac": byts / sec / 1e9 / peak,
+           "peak_kind": peak_kind}
+    fp = {"achieved": flops / sec / 1e12, "peak": fp64_peak, "unit": "TFLOP/s",
+          "frac": flops / sec / 1e12 / fp64_peak if fp64_peak else None,
+          "peak_kind": "measured here (DFMA-only kernel, mb_measure_fp64_peak)"}
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            ent = json.load(f).get(f"{name}@{size_key}")
+        traffic = ent.get("bytes_per_launch") if ent else None
+    main = fp if (fp["frac"] or 0) > hbm["frac"] else hbm
+    return {"bound": "fp64" if main is fp else "hbm", "kernel": name, "achieved": main["achieved"],
+            "peak": main["peak"], "unit": main["unit"], "frac": main["frac"], "peak_kind": main["peak_kind"],
+            "traffic": traffic, "hbm": hbm, "fp64": fp, "launches_per_step": lc,
+            "algorithmic_bytes_per_launch": byts / lc, "algorithmic_flops_per_launch": flops / lc,
+            "share_of_step": tms / sum(v[1] for v in rep.values()), "avg_launch_ms": tms / lc}
+
+
 def build_workload(mq, W, n, depth, seed_stream):
     params = W.u3_params(n, depth, W.rng_for(1, *seed_stream))
     return W.u3_brickwork(n, depth, params)
@@ -180,9 +219,12 @@ def batch_workload(args):
     groups = {n: (W.hea_circuit(n, depth), B) for n, B in counts.items()}
     dm_groups = {10: (W.hea_circuit(10, depth, noise=(0.01, 0.02)), 64)}
     t0 = time.perf_counter()
+    log("building the pure-state plan")
     plan = BatchPlan(groups, W.xxz)
+    log(f"pure plan ready after {time.perf_counter() - t0:.1f} s; building the density plan")
     plan_dm = BatchPlan(dm_groups, W.xxz, kind="density")
     prep_s = time.perf_counter() - t0
+    log(f"plans ready after {prep_s:.1f} s")
     def thetas(gr, seed):
         r = np.random.default_rng(seed)
         return {n: r.uniform(0, 2 * np.pi, size=(B, c.nparameters())) for n, (c, B) in gr.items()}
@@ -203,6 +245,7 @@ def batch_workload(args):
         end.synchronize()
         wall = (time.perf_counter() - t1) / args.steps
     ms_step = start.elapsed_time(end) / args.steps
+    log(f"timed {args.steps} steps: {ms_step:.2f} ms per step; timing the plain path")
     evals = 512 + 64
     # plain per-call path on a bounded sample (uniform over the same sizes), extrapolated per sample
     sub = {}
@@ -244,12 +287,218 @@ def batch_workload(args):
     return 0
 
 
+def log(msg):
+    print(f"[bench {time.strftime('%H:%M:%S')}] {msg}", file=sys.stderr, flush=True)
+
+
+def grad_workload(args):
+    """Config 3: adjoint gradient of the TFIM loss of a 24-qubit depth-16 hardware-efficient
+    ansatz (1152 independent angles) with forward checkpoints every 4 layers, and the
+    shared-parameter gradient of 64 ten-qubit density matrices with depolarizing noise
+    (p = 0.005) after every gate. One step = one value_and_gradient of each; the plain
+    per-call path (one plain kernel per gate and per reverse step) is timed beside it."""
+    import torch
+    import mossquantum_b200 as mq
+    from mossquantum_b200 import _native as N
+    from mossquantum_b200 import workloads as W
+    mq.init(0)
+    n, depth = 24, 16
+    angles = W.hea_angles(n, depth, W.rng_for(3))
+    c = W.hea_circuit(n, depth, angles)
+    H = W.tfim(n)
+    per_layer = 3 * n + (n - 1)
+    obj = mq.ExpectationObjective(c, H, mq.StateVector(n))
+    theta = c.active_parameters()
+    cdm = W.hea_circuit(10, 4, W.hea_angles(10, 4, W.rng_for(3, 1)), noise=(0.005, 0.0))
+    objb = mq.BatchExpectationObjective(cdm, W.tfim(10), mq.BatchDensityMatrix(10, 64))
+    thb = cdm.active_parameters()
+    method = mq.AdjointGradient(checkpoint_every=4 * per_layer)
+    stream = torch.cuda.ExternalStream(N.stream_handle())
+
+    def step():
+        mq.value_and_gradient(method, obj, theta)
+        mq.value_and_gradient(mq.AdjointGradient(), objb, thb)
+
+    for _ in range(args.warmup):
+        step()
+    l0 = N.launch_count()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(0) as clk:
+        t0 = time.perf_counter()
+        start.record(stream)
+        for _ in range(args.steps):
+            step()
+        end.record(stream)
+        end.synchronize()
+        wall = (time.perf_counter() - t0) / args.steps
+    ms = start.elapsed_time(end) / args.steps
+    launches = N.launch_count() - l0
+    t1 = time.perf_counter()
+    mq.value_and_gradient(method, obj, theta)
+    t_pure = time.perf_counter() - t1
+    t1 = time.perf_counter()
+    mq.value_and_gradient(mq.AdjointGradient(), objb, thb)
+    t_dm = time.perf_counter() - t1
+    os.environ["MB_ADJOINT_PLAIN"] = "1"
+    mq.value_and_gradient(method, obj, theta)
+    t1 = time.perf_counter()
+    mq.value_and_gradient(method, obj, theta)
+    t_plain = time.perf_counter() - t1
+    del os.environ["MB_ADJOINT_PLAIN"]
+    roofline = dominant_roofline(N, lambda: mq.value_and_gradient(method, obj, theta), f"n{n}")
+    line = {"metric": "adjoint gradient evaluations/s", "value": 1e3 / ms, "unit": "gradients/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "complex128 (f64)", "data": "synthetic (seeded)",
+            "config": {"workload": "adjoint: 24q HEA depth 16 (1152 angles, checkpoints every 4 layers) + "
+                                   "64 x 10q density matrices (depolarizing p=0.005, shared angles)",
+                       "l2": "24-qubit states (256 MiB each) exceed L2"},
+            "pure_24q_ms": t_pure * 1e3, "density_batch_ms": t_dm * 1e3,
+            "plain_per_call": {"pure_24q_ms": t_plain * 1e3, "speedup": t_plain / t_pure},
+            "roofline": roofline,
+            "e2e": {"value": 1.0 / wall, "unit": "gradients/s", "h2d_bytes_per_step": 8 * (len(theta) + len(thb)),
+                    "d2h_bytes_per_step": 8 * (len(theta) + len(thb) + 2)},
+            "gpu_launches": launches, "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def serve_workload(args):
+    """Config 4: Poisson arrivals at each swept rate; 70% pure requests (8..26 qubits), 30%
+    density-matrix requests (6..12 qubits, depolarizing p=0.01 and amplitude damping
+    gamma=0.02 after every gate); 4..32 hardware-efficient layers with random angles; TFIM
+    or XXZ; expectation or adjoint gradient (50/50). Requests go through the continuous-
+    batching server (HBM admission budget 160 GB). The plain per-request path (each request
+    alone through the per-call API with one plain kernel per gate) is timed on a sample of the
+    same requests and its latency under the same arrivals follows from a FIFO queue."""
+    import mossquantum_b200 as mq
+    from mossquantum_b200 import _native as N
+    from mossquantum_b200 import workloads as W
+    from mossquantum_b200.serving import Server
+    mq.init(0)
+    budget = min(160 * 10**9, int(mq.memory_info()[1] * 0.9))
+    blocks = {}
+
+    def block(kind, n):
+        if (kind, n) not in blocks:
+            blocks[(kind, n)] = W.hea_layer(n, noise=W.SERVING_NOISE if kind == "density" else None)
+        return blocks[(kind, n)]
+    obs = {}
+
+    def observable(name, n):
+        if (name, n) not in obs:
+            obs[(name, n)] = W.tfim(n) if name == "tfim" else W.xxz(n)
+        return obs[(name, n)]
+    rates = [float(r) for r in args.rates.split(",")]
+    srv = Server(budget_bytes=budget)
+    # warm-up: every class once alone and in a batch (schedules, specialised kernels)
+    t0 = time.perf_counter()
+    warm = []
+    for n in range(8, 27):
+        for g in (False, True):
+            th = np.zeros((2, 3 * n))
+            warm += [srv.submit(block("pure", n), n, observable("tfim", n), th, gradient=g) for _ in range(2)]
+    for n in range(6, 13):
+        for g in (False, True):
+            th = np.zeros((2, 3 * n))
+            warm += [srv.submit(block("density", n), n, observable("xxz", n), th, kind="density", gradient=g)
+                     for _ in range(2)]
+    for t in warm:
+        srv.wait(t)
+    log(f"serve warm-up {time.perf_counter() - t0:.1f} s")
+    levels = []
+    l0 = N.launch_count()
+    all_reqs = []
+    with ClockSampler(0) as clk:
+        for li, rate in enumerate(rates):
+            rng = W.rng_for(5, li)
+            reqs = W.serving_requests(args.requests, rng)
+            gaps = rng.exponential(1.0 / rate, size=len(reqs))
+            srv.reset_stats()
+            tickets = []
+            t_start = time.perf_counter()
+            t_next = t_start
+            for (k, n, L, o, g, th), gap in zip(reqs, gaps):
+                t_next += gap
+                d = t_next - time.perf_counter()
+                if d > 0:
+                    time.sleep(d)
+                tickets.append(srv.submit(block(k, n), n, observable(o, n), th, kind=k, gradient=g))
+            results = [srv.wait(t) for t in tickets]
+            span = time.perf_counter() - t_start
+            st = srv.stats()
+            levels.append({"rate_req_per_s": rate, "requests": len(reqs), "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
+                           "evals_per_s": st["evals_per_s"], "span_s": span, "iterations": st["iterations"],
+                           "peak_hbm_bytes": st["peak_bytes"]})
+            all_reqs += [(r, a, res) for r, a, res in zip(reqs, np.cumsum(gaps), results)]
+            log(f"rate {rate}: p50 {st['p50_ms']:.1f} ms p99 {st['p99_ms']:.1f} ms {st['evals_per_s']:.1f} evals/s")
+    launches = N.launch_count() - l0
+    srv.close()
+    # Plain per-request path on a sample (same requests, each alone, one plain kernel per gate).
+    rng = W.rng_for(5, 99)
+    sample = [all_reqs[i] for i in rng.choice(len(all_reqs), size=min(args.plain_samples, len(all_reqs)), replace=False)]
+    os.environ["MB_ADJOINT_PLAIN"] = "1"
+    service = []
+    max_err = 0.0
+    for (k, n, L, o, g, th), _, res in sample:
+        noise = W.SERVING_NOISE if k == "density" else None
+        circ = W.unrolled(lambda row: W.hea_layer_bound(n, row, noise=noise), th)
+        t1 = time.perf_counter()
+        init = mq.DensityMatrix(n) if k == "density" else mq.StateVector(n)
+        if g:
+            tmpl = W.unrolled(lambda row: W.hea_layer(n, noise=noise), th)
+            objp = mq.ExpectationObjective(tmpl, observable(o, n), init)
+            v, grad = mq.value_and_gradient(mq.AdjointGradient(), objp, th.reshape(-1))
+            max_err = max(max_err, float(np.max(np.abs(grad - res.gradient.reshape(-1)))))
+        else:
+            st_ = mq.apply_(circ, init, plain=True)
+            v = mq.expectation(observable(o, n), st_).real
+        service.append(time.perf_counter() - t1)
+        max_err = max(max_err, abs(v - res.value.real))
+    del os.environ["MB_ADJOINT_PLAIN"]
+    mean_service = float(np.mean(service))
+    plain_levels = []
+    for lv in levels:
+        # FIFO single-server queue with the sampled service times under the same arrival rate
+        rng = W.rng_for(5, 77)
+        arr = np.cumsum(rng.exponential(1.0 / lv["rate_req_per_s"], size=lv["requests"]))
+        svc = rng.choice(service, size=lv["requests"])
+        done, lat = 0.0, []
+        for a, sv in zip(arr, svc):
+            done = max(done, a) + sv
+            lat.append((done - a) * 1e3)
+        plain_levels.append({"rate_req_per_s": lv["rate_req_per_s"], "p50_ms": float(np.percentile(lat, 50)),
+                             "p99_ms": float(np.percentile(lat, 99)), "evals_per_s": lv["requests"] / done})
+    best = max(levels, key=lambda lv: lv["evals_per_s"])
+    line = {"metric": "serving circuit-evals/s (continuous batching) with p50/p99 latency", "value": best["evals_per_s"],
+            "unit": "evals/s", "n_gpus": 1, "steps": len(rates), "warmup": 1, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "complex128 (f64)", "data": "synthetic (seeded)",
+            "config": {"workload": "Poisson stream: 70% pure 8..26q, 30% density 6..12q (noisy), 4..32 layers, "
+                                   "TFIM/XXZ, 50% adjoint gradients", "hbm_budget_bytes": budget,
+                       "requests_per_rate": args.requests},
+            "levels": levels, "plain_per_request": {"mean_service_ms": mean_service * 1e3,
+                                                    "evals_per_s": 1.0 / mean_service, "levels": plain_levels,
+                                                    "sample": f"{len(sample)} requests timed alone"},
+            "max_abs_diff_vs_plain": max_err,
+            "e2e": {"value": best["evals_per_s"], "unit": "evals/s",
+                    "h2d_bytes_per_step": int(sum(8 * r[0][5].size for r in all_reqs) / max(1, len(rates))),
+                    "d2h_bytes_per_step": int(sum(16 + (8 * r[0][5].size if r[0][4] else 0) for r in all_reqs)
+                                              / max(1, len(rates))),
+                    "note": "requests submitted from host memory, results read back on the host"},
+            "gpu_launches": launches, "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return reference_arm(args)
     if args.workload == "batch":
         return batch_workload(args)
+    if args.workload == "grad":
+        return grad_workload(args)
+    if args.workload == "serve":
+        return serve_workload(args)
     import torch
     import torch.distributed as dist
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -297,29 +546,7 @@ def main():
     bytes_step = plain_bytes(n, depth)
     value = world * bytes_step / (ms_step / 1e3) / 1e9
 
-    # Per-kernel roofline of the dominant kernel (one profiled step, events on the library stream).
-    N.profile(True)
-    step()
-    rep = N.profile_report()
-    N.profile(False)
-    dom = max(rep.items(), key=lambda kv: kv[1][1]) if rep else None
-    peak, peak_kind = load_peaks()
-    roofline = None
-    if dom:
-        name, (lc, tms, byts) = dom
-        achieved = byts / (tms / 1e3) / 1e9
-        traffic = None
-        tpath = os.path.join(ROOT, "profiles", "traffic.json")
-        if os.path.exists(tpath):
-            with open(tpath) as f:
-                tj = json.load(f)
-            ent = tj.get(f"{name}@n{n}")
-            traffic = ent.get("bytes_per_launch") if ent else None
-        share = tms / sum(v[1] for v in rep.values())
-        roofline = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                    "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
-                    "launches_per_step": lc, "algorithmic_bytes_per_launch": byts / lc, "share_of_step": share,
-                    "avg_launch_ms": tms / lc}
+    roofline = dominant_roofline(N, step, f"n{n}")
 
     # End to end through the public API: host circuit in, probabilities of 10 qubits out.
     e2e = None

@@ -130,9 +130,14 @@ typedef struct mb_kernel_stat {
   uint64_t launches;
   double total_ms;
   double bytes;        /* algorithmic bytes summed over launches */
+  double flops;        /* algorithmic FP64 flops summed over launches (8*2^k per amplitude */
+                       /* for a dense k-qubit complex gate; sign flips and swaps count 0)  */
 } mb_kernel_stat;
 MB_API int mb_profile(int enable);
 MB_API int mb_profile_report(mb_kernel_stat* stats, int cap, int* count);
+/* Times a DFMA-only kernel on every SM and returns the FP64 rate it reaches (TFLOP/s):
+ * the measured denominator for passes bound by the FP64 pipe. */
+MB_API int mb_measure_fp64_peak(double* tflops);
 
 /* ---- states: StateVector / DensityMatrix / batches (src/states/*.jl) ------------------ */
 /* Allocate a state of `kind` with n qubits (0..30 pure, 0..15 density) and `batch`
@@ -209,6 +214,72 @@ MB_API int mb_probabilities(mb_state s, const int* qubits, int nq, double* out);
  * checkpoint_every: forward checkpoints every k instructions (<= 0 picks automatically). */
 MB_API int mb_adjoint(mb_circuit c, mb_observable o, mb_state init, const double* theta, size_t ntheta,
                const double* weights, int checkpoint_every, double* value, double* grad);
+
+/* ---- serving: continuous batching of circuit evaluations ------------------------------
+ * Replaces the one-call-at-a-time objective evaluation of the reference
+ * (evaluate / value_and_gradient, src/api/objectives.jl:15-244,
+ * src/differentiation/objectives.jl:183-296) for a stream of independent requests.
+ * A request is an ansatz: `repeats` repetitions of a parametrised block circuit (one layer),
+ * each repetition with its own parameters, applied to |0...0> of a pure state or a density
+ * matrix, followed by <H> and optionally its adjoint gradient.
+ * A scheduler thread owned by the library admits requests in arrival order against the
+ * server's HBM byte budget (16*2^n per pure state, 16*4^n per density matrix, plus gradient
+ * buffers and checkpoints), keeps their states resident, and on every iteration advances
+ * every admitted request by one layer: requests of the same block and kind share one
+ * batched launch per fused pass with per-sample parameters, gradient requests run one
+ * reverse layer each. Requests join and leave between iterations.
+ * The block and observable handles of a request must stay valid until it completes. */
+typedef struct mb_server_config {
+  size_t hbm_budget_bytes;  /* admission budget in bytes; 0 = what the library budget leaves   */
+  int max_active;           /* most admitted requests at once; 0 = 4096                         */
+  int reserved[7];
+} mb_server_config;
+
+typedef struct mb_request {
+  mb_circuit block;         /* one layer, compiled for n qubits; its slots are the layer's      */
+                            /* parameters (channels require MB_DENSITY)                        */
+  mb_observable observable; /* Hermitian for gradient requests                                 */
+  int kind;                 /* MB_PURE or MB_DENSITY                                           */
+  int repeats;              /* layers, >= 1                                                    */
+  const double* theta;      /* repeats * nslots(block) values, layer by layer; copied           */
+  size_t ntheta;
+  int gradient;             /* 0: <H>; 1: <H> and d Re<H> / d theta (adjoint method)           */
+  int reserved[5];
+} mb_request;
+
+typedef struct mb_result {
+  int status;               /* MB_OK or the request's error code                                */
+  int iterations;           /* scheduler iterations the request took part in                   */
+  double value[2];          /* <H> (re, im)                                                    */
+  double latency_ms;        /* submission to completion                                        */
+  double queue_ms;          /* submission to admission                                         */
+  char error[128];          /* message when status != MB_OK                                    */
+} mb_result;
+
+typedef struct mb_server_stats {
+  uint64_t submitted, completed, failed, iterations;
+  int active, pending;
+  size_t bytes_in_use, peak_bytes, budget_bytes;
+  double p50_ms, p99_ms;    /* latency percentiles of the completed requests                   */
+  double evals_per_s;       /* completed requests / (last completion - first submission)       */
+} mb_server_stats;
+
+typedef struct mb_server_s* mb_server;
+MB_API int mb_server_start(const mb_server_config* cfg, mb_server* out);
+/* Queues a request; returns at once with its ticket. */
+MB_API int mb_submit(mb_server s, const mb_request* req, uint64_t* ticket);
+/* MB_ENOTREADY while the request is queued or running; otherwise fills res (and, for
+ * gradient requests, grad with repeats*nslots doubles when ngrad is large enough), releases
+ * the ticket and returns MB_OK. */
+MB_API int mb_poll(mb_server s, uint64_t ticket, mb_result* res, double* grad, size_t ngrad);
+/* As mb_poll, waiting up to timeout_ms (< 0: no limit); MB_ETIMEOUT when it runs out. */
+MB_API int mb_wait(mb_server s, uint64_t ticket, int timeout_ms, mb_result* res, double* grad, size_t ngrad);
+MB_API int mb_server_stats_get(mb_server s, mb_server_stats* out);
+/* Clears the latency record and counters (between load levels of a sweep). */
+MB_API int mb_server_stats_reset(mb_server s);
+/* Finishes the admitted requests, fails the queued ones, joins the scheduler thread and
+ * releases the server's memory. Call before mb_shutdown. */
+MB_API int mb_server_stop(mb_server s);
 
 /* ---- allocation-free expectation -----------------------------------------------------
  * No counterpart in the reference: MOSSQuantum's CPU path never allocates device memory.

@@ -57,9 +57,31 @@ class MbTerm(ctypes.Structure):
                 ("ops", ctypes.c_void_p)]
 
 
+class MbServerConfig(ctypes.Structure):
+    _fields_ = [("hbm_budget_bytes", ctypes.c_size_t), ("max_active", ctypes.c_int), ("reserved", ctypes.c_int * 7)]
+
+
+class MbRequest(ctypes.Structure):
+    _fields_ = [("block", ctypes.c_void_p), ("observable", ctypes.c_void_p), ("kind", ctypes.c_int),
+                ("repeats", ctypes.c_int), ("theta", ctypes.c_void_p), ("ntheta", ctypes.c_size_t),
+                ("gradient", ctypes.c_int), ("reserved", ctypes.c_int * 5)]
+
+
+class MbResult(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("iterations", ctypes.c_int), ("value", ctypes.c_double * 2),
+                ("latency_ms", ctypes.c_double), ("queue_ms", ctypes.c_double), ("error", ctypes.c_char * 128)]
+
+
+class MbServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64), ("failed", ctypes.c_uint64),
+                ("iterations", ctypes.c_uint64), ("active", ctypes.c_int), ("pending", ctypes.c_int),
+                ("bytes_in_use", ctypes.c_size_t), ("peak_bytes", ctypes.c_size_t), ("budget_bytes", ctypes.c_size_t),
+                ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double), ("evals_per_s", ctypes.c_double)]
+
+
 class MbKernelStat(ctypes.Structure):
     _fields_ = [("name", ctypes.c_char * 48), ("launches", ctypes.c_uint64), ("total_ms", ctypes.c_double),
-                ("bytes", ctypes.c_double)]
+                ("bytes", ctypes.c_double), ("flops", ctypes.c_double)]
 
 
 _lib = None
@@ -119,6 +141,14 @@ def load():
         "mb_tuning_set": ([ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
         "mb_tuning_get": ([ctypes.c_int, ip, ip], ctypes.c_int),
         "mb_autotune": ([vp, vp, dp, sz, ctypes.c_int, ip, ip, dp], ctypes.c_int),
+        "mb_measure_fp64_peak": ([dp], ctypes.c_int),
+        "mb_server_start": ([ctypes.POINTER(MbServerConfig), ctypes.POINTER(vp)], ctypes.c_int),
+        "mb_submit": ([vp, ctypes.POINTER(MbRequest), ctypes.POINTER(ctypes.c_uint64)], ctypes.c_int),
+        "mb_poll": ([vp, ctypes.c_uint64, ctypes.POINTER(MbResult), dp, sz], ctypes.c_int),
+        "mb_wait": ([vp, ctypes.c_uint64, ctypes.c_int, ctypes.POINTER(MbResult), dp, sz], ctypes.c_int),
+        "mb_server_stats_get": ([vp, ctypes.POINTER(MbServerStats)], ctypes.c_int),
+        "mb_server_stats_reset": ([vp], ctypes.c_int),
+        "mb_server_stop": ([vp], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -188,12 +218,20 @@ def profile(enable: bool) -> None:
 
 
 def profile_report():
-    """{kernel name: (launches, total_ms, algorithmic bytes)} since profile(True)."""
+    """{kernel name: (launches, total_ms, algorithmic bytes, algorithmic FP64 flops)} since profile(True)."""
     cap = 64
     arr = (MbKernelStat * cap)()
     cnt = ctypes.c_int()
     check(lib().mb_profile_report(arr, cap, ctypes.byref(cnt)))
-    return {arr[i].name.decode(): (arr[i].launches, arr[i].total_ms, arr[i].bytes) for i in range(min(cnt.value, cap))}
+    return {arr[i].name.decode(): (arr[i].launches, arr[i].total_ms, arr[i].bytes, arr[i].flops)
+            for i in range(min(cnt.value, cap))}
+
+
+def measure_fp64_peak() -> float:
+    """FP64 TFLOP/s of a DFMA-only kernel on every SM (the FP64-pipe roofline denominator)."""
+    v = ctypes.c_double()
+    check(lib().mb_measure_fp64_peak(ctypes.byref(v)), "mb_measure_fp64_peak")
+    return v.value
 
 
 def synchronize() -> None:

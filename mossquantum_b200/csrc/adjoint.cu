@@ -57,6 +57,103 @@ static int gate_gradient(mb_circuit c, const COp& op, const double2* y, const do
   return launch_cross_dense(delta, y, elems, nsamples, p, D, 0, MAT_TRANSPOSE, ws(), 0, ro, g_ctx.stream);
 }
 
+// Reverse of one application of a unitary circuit c on one pure sample, as used by the serving
+// loop for every repetition of an ansatz block. On entry y is the state after c and delta the
+// adjoint of the state; on exit y is the state before c, delta = c' delta, and d_grad[slot] has
+// been incremented by Re<y|D|delta> per active parameter (back_propagate, circuit.jl:136-144).
+// try_fused: use the specialised dual-state passes when the circuit allows them.
+int reverse_pure_single(mb_circuit c, int n, double2* y, double2* delta, double* d_grad, bool try_fused,
+                        bool* used_fused) {
+  if (used_fused) *used_fused = false;
+  if (try_fused && n >= 9 && !c->has_channel && !c->ops.empty()) {
+    Schedule* S = nullptr;
+    if (adjoint_prepare(c, n, 0, int(c->ops.size()), &S) == MB_OK) {
+      if (used_fused) *used_fused = true;
+      return run_adjoint_schedule(c, S, y, delta, d_grad);
+    }
+  }
+  for (int i = int(c->ops.size()) - 1; i >= 0; --i) {
+    const COp& op = c->ops[i];
+    int rc;
+    if ((rc = plain_op(c, op, delta, n, 0, 1, 0, true))) return rc;
+    if ((rc = plain_op(c, op, y, n, 0, 1, 0, true))) return rc;
+    if (op.gen_off >= 0 && (rc = gate_gradient(c, op, y, delta, n, 0, 1, d_grad + op.slot, nullptr))) return rc;
+  }
+  return MB_OK;
+}
+
+// Segment length of the two-level recomputation in reverse_dm_single and the number of
+// scratch states it needs: one working state, the checkpoints of segments 1.., and the
+// channel inputs of the longest segment.
+void dm_reverse_plan(mb_circuit c, int* seg_len, int* nscratch) {
+  const int k = int(c->ops.size());
+  const int m = std::max(1, int(std::ceil(std::sqrt(double(std::max(k, 1))))));
+  const int nseg = std::max(1, (k + m - 1) / m);
+  int maxch = 0;
+  for (int s = 0; s < nseg; ++s) {
+    int ch = 0;
+    for (int i = s * m; i < std::min(k, (s + 1) * m); ++i) ch += c->ops[i].kind == MB_OP_CHANNEL;
+    maxch = std::max(maxch, ch);
+  }
+  *seg_len = m;
+  *nscratch = 1 + (nseg - 1) + maxch;
+}
+
+// Forward application of instructions [lo, hi) of c on one density matrix (fused passes when
+// available, plain otherwise).
+static int forward_range_dm(mb_circuit c, int n, int lo, int hi, double2* z) {
+  if (lo >= hi) return MB_OK;
+  Schedule* S = nullptr;
+  if (2 * n >= 8 && get_schedule_ex(c, n, 1, 0, lo, hi, 1, &S) == MB_OK) return run_schedule(c, S, z, 1, 0);
+  for (int i = lo; i < hi; ++i)
+    if (int rc = plain_op(c, c->ops[i], z, n, 1, 1, 0, false)) return rc;
+  return MB_OK;
+}
+
+// Reverse of one application of circuit c (gates and channels) on one density matrix, for the
+// serving loop. ckpt is the state before c (kept by the caller); delta enters as the adjoint
+// after c and leaves as the adjoint before c; d_grad[slot] += Re(<delta, D'y> + <delta, yD>)
+// per active parameter (_density_gate_gradient!, circuit.jl:155-172). Channel inputs come
+// from a two-level recomputation: checkpoints every seg_len instructions, then the inputs of
+// one segment at a time, so scratch holds dm_reverse_plan's nscratch states.
+int reverse_dm_single(mb_circuit c, int n, const double2* ckpt, double2* delta, double* d_grad,
+                      double2* const* scratch) {
+  const int k = int(c->ops.size());
+  int m = 1, nscratch = 1;
+  dm_reverse_plan(c, &m, &nscratch);
+  const int nseg = std::max(1, (k + m - 1) / m);
+  const size_t sbytes = sizeof(double2) * (size_t(1) << (2 * n));
+  cudaStream_t st = g_ctx.stream;
+  double2* z = scratch[0];
+  int rc;
+  MB_CHECK_CUDA(cudaMemcpyAsync(z, ckpt, sbytes, cudaMemcpyDeviceToDevice, st));
+  for (int s = 1; s < nseg; ++s) {
+    if ((rc = forward_range_dm(c, n, (s - 1) * m, s * m, z))) return rc;
+    MB_CHECK_CUDA(cudaMemcpyAsync(scratch[s], z, sbytes, cudaMemcpyDeviceToDevice, st));
+  }
+  double2* const* chin = scratch + nseg;
+  for (int s = nseg - 1; s >= 0; --s) {
+    const int lo = s * m, hi = std::min(k, (s + 1) * m);
+    MB_CHECK_CUDA(cudaMemcpyAsync(z, s == 0 ? ckpt : scratch[s], sbytes, cudaMemcpyDeviceToDevice, st));
+    int nch = 0;
+    for (int i = lo; i < hi; ++i) {
+      if (c->ops[i].kind == MB_OP_CHANNEL) MB_CHECK_CUDA(cudaMemcpyAsync(chin[nch++], z, sbytes, cudaMemcpyDeviceToDevice, st));
+      if ((rc = plain_op(c, c->ops[i], z, n, 1, 1, 0, false))) return rc;
+    }
+    for (int i = hi - 1; i >= lo; --i) {
+      const COp& op = c->ops[i];
+      if ((rc = plain_op(c, op, delta, n, 1, 1, 0, true))) return rc;
+      if (op.kind == MB_OP_CHANNEL) {
+        MB_CHECK_CUDA(cudaMemcpyAsync(z, chin[--nch], sbytes, cudaMemcpyDeviceToDevice, st));
+        continue;
+      }
+      if ((rc = plain_op(c, op, z, n, 1, 1, 0, true))) return rc;
+      if (op.gen_off >= 0 && (rc = gate_gradient(c, op, z, delta, n, 1, 1, d_grad + op.slot, nullptr))) return rc;
+    }
+  }
+  return MB_OK;
+}
+
 }  // namespace mb
 
 extern "C" int mb_adjoint(mb_circuit c, mb_observable o, mb_state init, const double* theta, size_t ntheta,

@@ -181,6 +181,10 @@ extern "C" int mb_init(int device, size_t hbm_budget_bytes) {
 extern "C" int mb_shutdown(void) {
   std::lock_guard<std::recursive_mutex> lk(g_mu);
   if (!g_ctx.init) return MB_OK;
+  if (servers_running()) {
+    set_error("stop every server (mb_server_stop) before mb_shutdown");
+    return MB_EINVAL;
+  }
   cudaStreamSynchronize(g_ctx.stream);
   dev_free(g_ctx.partials);
   dev_free(g_ctx.counters);
@@ -361,6 +365,7 @@ extern "C" int mb_circuit_create(const mb_op* ops, size_t nops, int n, mb_circui
     return MB_EINVAL;
   }
   std::unique_ptr<mb_circuit_s> c(new mb_circuit_s());
+  c->uid = next_circuit_uid();
   c->n = n;
   int64_t off = 0;
   std::vector<double2> table;
@@ -545,16 +550,66 @@ extern "C" int mb_circuit_create(const mb_op* ops, size_t nops, int n, mb_circui
   return MB_OK;
 }
 
-extern "C" int mb_circuit_free(mb_circuit c) {
-  std::lock_guard<std::recursive_mutex> lk(g_mu);
-  if (!c) return MB_OK;
+namespace mb {
+
+uint64_t next_circuit_uid() {
+  static uint64_t next = 0;
+  return ++next;
+}
+
+// Device buffers, pinned staging and schedules of a circuit, then the handle itself.
+void circuit_release(mb_circuit c) {
+  if (!c) return;
   if (g_ctx.init) {
     dev_free(c->d_table);
     dev_free(c->d_binds);
     dev_free(c->d_theta);
     release_schedules(c);
   }
+  if (c->h_theta) cudaFreeHost(c->h_theta);
   delete c;
+}
+
+// Private copy of a compiled circuit: the same instructions and fixed matrices with its own
+// matrix table, parameter buffer and schedules, so the serving loop can bind per-request
+// parameters without touching the caller's handle.
+int circuit_clone(mb_circuit src, mb_circuit* out) {
+  mb_circuit c = new mb_circuit_s();
+  c->uid = next_circuit_uid();
+  c->n = src->n;
+  c->ops = src->ops;
+  c->nslots = src->nslots;
+  c->has_channel = src->has_channel;
+  c->fixed_table = src->fixed_table;
+  c->table_elems = src->table_elems;
+  c->binds = src->binds;
+  c->table_rows = 1;
+  int rc = dev_alloc((void**)&c->d_table, sizeof(double2) * c->table_elems);
+  if (!rc && !c->binds.empty()) rc = dev_alloc((void**)&c->d_binds, sizeof(BindRec) * c->binds.size());
+  if (rc) {
+    circuit_release(c);
+    return rc;
+  }
+  cudaError_t e = cudaMemcpyAsync(c->d_table, c->fixed_table.data(), sizeof(double2) * c->table_elems,
+                                  cudaMemcpyHostToDevice, g_ctx.stream);
+  if (e == cudaSuccess && !c->binds.empty())
+    e = cudaMemcpyAsync(c->d_binds, c->binds.data(), sizeof(BindRec) * c->binds.size(), cudaMemcpyHostToDevice,
+                        g_ctx.stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g_ctx.stream);
+  if (e != cudaSuccess) {
+    set_error("circuit copy failed: %s", cudaGetErrorString(e));
+    circuit_release(c);
+    return MB_EDEVICE;
+  }
+  *out = c;
+  return MB_OK;
+}
+
+}  // namespace mb
+
+extern "C" int mb_circuit_free(mb_circuit c) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  circuit_release(c);
   return MB_OK;
 }
 

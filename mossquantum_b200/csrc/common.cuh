@@ -94,7 +94,7 @@ uint64_t& launch_counter();
 struct ProfScope {
   int slot;
   cudaStream_t st;
-  ProfScope(const char* name, double bytes, cudaStream_t stream);
+  ProfScope(const char* name, double bytes, cudaStream_t stream, double flops = 0);
   ~ProfScope();
 };
 

@@ -204,6 +204,27 @@ struct Schedule {
 
 namespace {
 
+// Algorithmic FP64 flops per amplitude of one micro-op: 8*2^k for a dense k-qubit complex
+// gate (2^k complex multiply-adds), scaled by the fraction of amplitudes a controlled or
+// diagonal op touches; swaps and sign flips count zero.
+static double mop_flops(const MOp& m) {
+  switch (m.type) {
+    case MOP_U1: return 16.0;
+    case MOP_CTRL: return 16.0 / double(1 << m.nsel);
+    case MOP_U2: return 32.0;
+    case MOP_DIAG: return 6.0 * __builtin_popcount(m.active) / double(1 << m.nsel);
+    case MOP_CPHASE: return m.r1 ? 0.0 : 6.0 / double(1 << m.nsel);
+    case MOP_GRAD: return 8.0 * double(1 << m.nsel) + 8.0;
+    default: return 0.0;
+  }
+}
+
+static double pass_flops_per_amp(const Pass& p, bool dual) {
+  double f = 0;
+  for (const MOp& m : p.mops) f += (dual && m.type != MOP_GRAD) ? 2.0 * mop_flops(m) : mop_flops(m);
+  return f;
+}
+
 static bool is_one(double2 x) { return x.x == 1.0 && x.y == 0.0; }
 static bool is_zero(double2 x) { return x.x == 0.0 && x.y == 0.0; }
 
@@ -995,14 +1016,16 @@ int run_schedule(mb_circuit c, Schedule* S, double2* v, int nsamples, int64_t ms
       const int per_sm = std::max(1, int((227 * 1024) / (shm + 256)));
       const int64_t grid = std::min<int64_t>(a.ntiles, int64_t(g_ctx.sm_count) * std::min(per_sm, 4));
       if (S->jit == 1 && p.jit_fn) {
-        ProfScope ps("k_tile_pass_jit", 32.0 * double(elems) * nsamples, st);
+        ProfScope ps("k_tile_pass_jit", 32.0 * double(elems) * nsamples, st,
+                     pass_flops_per_amp(p, false) * double(elems) * nsamples);
         rc = jit_launch_tile((CUfunction)p.jit_fn, &map, c->d_table, mstride, a.tiles_per_sample, a.ntiles, a.err,
                              threads, shm, int(grid), st);
         ++launch_counter();
         if (rc) return rc;
         continue;
       }
-      ProfScope ps("k_tile_pass", 32.0 * double(elems) * nsamples, st);
+      ProfScope ps("k_tile_pass", 32.0 * double(elems) * nsamples, st,
+                   pass_flops_per_amp(p, false) * double(elems) * nsamples);
       const bool u2 = p.has_u2;
       auto launch = [&](auto kern) {
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm));
@@ -1026,13 +1049,15 @@ int run_schedule(mb_circuit c, Schedule* S, double2* v, int nsamples, int64_t ms
       const int block = 128;
       const int grid = grid_for(work, block, int64_t(g_ctx.sm_count) * 16);
       if (S->jit == 1 && p.jit_fn) {
-        ProfScope ps("k_reg_pass_jit", 32.0 * double(elems) * nsamples, st);
+        ProfScope ps("k_reg_pass_jit", 32.0 * double(elems) * nsamples, st,
+                     pass_flops_per_amp(p, false) * double(elems) * nsamples);
         rc = jit_launch_reg((CUfunction)p.jit_fn, v, c->d_table, mstride, a.groups, nsamples, grid, st);
         ++launch_counter();
         if (rc) return rc;
         continue;
       }
-      ProfScope ps("k_reg_pass", 32.0 * double(elems) * nsamples, st);
+      ProfScope ps("k_reg_pass", 32.0 * double(elems) * nsamples, st,
+                   pass_flops_per_amp(p, false) * double(elems) * nsamples);
       if (p.t == 5) p.has_u2 ? k_reg_pass<5, true><<<grid, block, 0, st>>>(v, a)
                              : k_reg_pass<5, false><<<grid, block, 0, st>>>(v, a);
       else p.has_u2 ? k_reg_pass<4, true><<<grid, block, 0, st>>>(v, a) : k_reg_pass<4, false><<<grid, block, 0, st>>>(v, a);
@@ -1083,7 +1108,7 @@ int run_adjoint_schedule(mb_circuit c, Schedule* S, double2* y, double2* d, doub
     const int per_sm = std::max(1, int((227 * 1024) / (shm + 256)));
     const int64_t ntiles = int64_t(1) << (N - p.t);
     const int grid = int(std::min<int64_t>(ntiles, int64_t(g_ctx.sm_count) * std::min(per_sm, 4)));
-    ProfScope ps("k_adjoint_pass_jit", 64.0 * double(elems), st);
+    ProfScope ps("k_adjoint_pass_jit", 64.0 * double(elems), st, pass_flops_per_amp(p, true) * double(elems));
     rc = jit_launch_adjoint((CUfunction)p.jit_fn, &my, &md, c->d_table, 0, ntiles, ntiles, g_ctx.flags + 2, gpart, gcount,
                             d_grad, S->d_gslots + p.grad_off, threads, shm, grid, st);
     ++launch_counter();

@@ -41,6 +41,7 @@ struct mb_state_s {
 };
 
 struct mb_circuit_s {
+  uint64_t uid = 0;                   // process-unique id (never reused, unlike the address)
   int n = 0;
   std::vector<mb::COp> ops;
   int nslots = 0;
@@ -112,6 +113,10 @@ int bind_launch(mb_circuit c, int rows);
 int check_not_capturing(const char* what);
 int plain_op(mb_circuit c, const COp& op, double2* v, int n, int is_dm, int nsamples, int64_t mrow_stride,
              bool dagger);
+int circuit_clone(mb_circuit src, mb_circuit* out);
+void circuit_release(mb_circuit c);
+uint64_t next_circuit_uid();
+int servers_running();  // serve.cu
 int apply_plain(mb_circuit c, mb_state s, int64_t mrow_stride);
 int validate_apply(mb_circuit c, mb_state s);
 int validate_observable(mb_observable o, mb_state s);
@@ -125,6 +130,13 @@ int run_schedule(mb_circuit c, Schedule* S, double2* v, int nsamples, int64_t ms
 int run_adjoint_schedule(mb_circuit c, Schedule* S, double2* y, double2* d, double* d_grad);
 int adjoint_prepare(mb_circuit c, int n, int lo, int hi, Schedule** out);
 void release_schedules(mb_circuit c);
+
+// adjoint.cu: single-sample reverse sweeps of one circuit application (serving loop)
+int reverse_pure_single(mb_circuit c, int n, double2* y, double2* delta, double* d_grad, bool try_fused,
+                        bool* used_fused);
+void dm_reverse_plan(mb_circuit c, int* seg_len, int* nscratch);
+int reverse_dm_single(mb_circuit c, int n, const double2* ckpt, double2* delta, double* d_grad,
+                      double2* const* scratch);
 
 // pauli.cu
 int pauli_compile(mb_observable o, const mb_term* terms, size_t nterms);

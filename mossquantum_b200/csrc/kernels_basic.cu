@@ -495,7 +495,7 @@ int launch_dense(double2* v, int64_t elems, int nsamples, const Pos& pos, const 
   if (nsamples <= 0 || elems == 0) return MB_OK;
   dim3 g = sample_grid(elems >> pos.k, nsamples);
   {
-    ProfScope ps("k_dense", 32.0 * elems * nsamples, st);
+    ProfScope ps("k_dense", 32.0 * elems * nsamples, st, 8.0 * (1 << pos.k) * elems * nsamples);
     MB_DISPATCH_K(pos.k, (k_dense<KK><<<g, kBlock, 0, st>>>(v, elems, pos, mats, mstride, mode)));
   }
   MB_LAUNCHED();

@@ -90,3 +90,40 @@ def xxz(n, J=1.0, Jzz=0.5):
         terms += [QubitsTerm([i, i + 1], ["X", "X"], J), QubitsTerm([i, i + 1], ["Y", "Y"], J),
                   QubitsTerm([i, i + 1], ["Z", "Z"], Jzz)]
     return QubitsOperator(terms)
+
+
+def unrolled(block_for, theta):
+    """The full circuit of a layered request: block_for(angles of one layer) per row of theta."""
+    c = QCircuit()
+    for row in np.asarray(theta):
+        c.push(block_for(row))
+    return c
+
+
+def hea_layer(n, noise=None):
+    """One hardware-efficient layer with active parameters (3n angles, zeros)."""
+    return hea_circuit(n, 1, noise=noise)
+
+
+def hea_layer_bound(n, row, noise=None):
+    """One hardware-efficient layer with its 3n angles bound (row ordered as hea_layer's
+    active parameters: RX, RY, RZ per qubit)."""
+    return hea_circuit(n, 1, np.asarray(row, dtype=np.float64).reshape(1, n, 3), noise=noise)
+
+
+SERVING_NOISE = (0.01, 0.02)
+
+
+def serving_requests(count, rng, pure_n=(8, 26), dm_n=(6, 12), layers=(4, 32), pure_frac=0.7, grad_frac=0.5):
+    """Request mix of the serving benchmark: (kind, n, repeats, observable name, gradient,
+    theta of shape (repeats, 3n)) per request, drawn from rng."""
+    out = []
+    for _ in range(count):
+        pure = rng.random() < pure_frac
+        n = int(rng.integers(pure_n[0], pure_n[1] + 1)) if pure else int(rng.integers(dm_n[0], dm_n[1] + 1))
+        L = int(rng.integers(layers[0], layers[1] + 1))
+        obs = "tfim" if rng.random() < 0.5 else "xxz"
+        grad = bool(rng.random() < grad_frac)
+        theta = rng.uniform(0.0, 2 * np.pi, size=(L, 3 * n))
+        out.append(("pure" if pure else "density", n, L, obs, grad, theta))
+    return out
