@@ -34,7 +34,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--variant", default="fused", choices=["fused", "plain"])
+    ap.add_argument("--variant", default="fused", choices=["fused", "plain", "block", "tensor"],
+                    help="fused: tiled passes (K1/K2); plain: one K0 sweep per gate; block: gates fused on the "
+                         "host into dense <=5-qubit blocks, one K0 sweep each; tensor: the same blocks on the "
+                         "FP64 tensor cores (K5)")
     ap.add_argument("--qubits", type=int, default=28)
     ap.add_argument("--layers", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -392,19 +395,16 @@ def serve_workload(args):
     srv = Server(budget_bytes=budget)
     # warm-up: every class once alone and in a batch (schedules, specialised kernels)
     t0 = time.perf_counter()
-    warm = []
-    for n in range(8, 27):
-        for g in (False, True):
-            th = np.zeros((2, 3 * n))
-            warm += [srv.submit(block("pure", n), n, observable("tfim", n), th, gradient=g) for _ in range(2)]
-    for n in range(6, 13):
-        for g in (False, True):
-            th = np.zeros((2, 3 * n))
-            warm += [srv.submit(block("density", n), n, observable("xxz", n), th, kind="density", gradient=g)
-                     for _ in range(2)]
-    for t in warm:
-        srv.wait(t)
-    log(f"serve warm-up {time.perf_counter() - t0:.1f} s")
+    classes = [("pure", n) for n in range(8, 27)] + [("density", n) for n in range(6, 13)]
+    # one request per class alone, then three together (both shapes of every specialised kernel)
+    for wave in ((("tfim", True),), (("tfim", True), ("xxz", False), ("tfim", False))):
+        warm = []
+        for k, n in classes:
+            for o, g in wave:
+                warm.append(srv.submit(block(k, n), n, observable(o, n), np.zeros((2, 3 * n)), kind=k, gradient=g))
+        for t in warm:
+            srv.wait(t)
+        log(f"serve warm-up wave done after {time.perf_counter() - t0:.1f} s")
     levels = []
     l0 = N.launch_count()
     all_reqs = []
@@ -513,13 +513,16 @@ def main():
     mq.init(local)
     n, depth = args.qubits, args.layers
     circuit = build_workload(mq, W, n, depth, (rank,))
+    if args.variant in ("block", "tensor"):
+        circuit = mq.fuse_gates(circuit, max_qubits=5)   # host fusion at bind time, outside the timed region
     state = mq.StateVector(n)
-    plain = args.variant == "plain"
+    plain = args.variant != "fused"
+    tensor = args.variant == "tensor"
     stream = torch.cuda.ExternalStream(N.stream_handle(), device=local)
 
     def step():
         state.set_zero()
-        mq.apply_(circuit, state, plain=plain)
+        mq.apply_(circuit, state, plain=plain, tensor=tensor)
 
     for _ in range(args.warmup):
         step()
@@ -557,7 +560,9 @@ def main():
 
         def e2e_step(c):
             state.set_zero()
-            mq.apply_(c, state, plain=plain)
+            if args.variant in ("block", "tensor"):
+                c = mq.fuse_gates(c, max_qubits=5)
+            mq.apply_(c, state, plain=plain, tensor=tensor)
             return mq.probabilities(state, readout)
 
         e2e_step(circuits[0])

@@ -107,6 +107,8 @@ typedef struct mb_observable_s* mb_observable;
 #define MB_APPLY_FUSED 0       /* tiled / fused kernels (default)                          */
 #define MB_APPLY_PLAIN 1       /* one plain kernel launch per gate (the per-call drop-in)  */
 #define MB_APPLY_PER_SAMPLE 2  /* batch states: theta holds B rows of nslots values         */
+#define MB_APPLY_TENSOR 8      /* with MB_APPLY_PLAIN: dense 4-5 qubit gates and 2-qubit     */
+                               /* channels on the FP64 tensor cores (K5) instead of K0       */
 
 /* ---- context: replaces the CPUBackend singleton (src/api/backend_protocols.jl:10-70) --- */
 MB_API int mb_init(int device, size_t hbm_budget_bytes);      /* budget 0 = 90% of free HBM    */

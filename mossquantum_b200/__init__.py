@@ -16,6 +16,7 @@ from .gates import (CCPHASEGate, CNOTGate, CONTROLCONTROLGate, CONTROLGate, CPHA
 from .objectives import (AdjointGradient, B200AdjointGradient, BatchExpectationObjective, ExpectationObjective,
                          UnsupportedGradient, differentiable_value, evaluate, evaluate_batch, supports_gradient,
                          value_and_gradient, value_and_pullback)
+from .fusion import fuse_gates
 from .operators import QubitsOperator, QubitsTerm
 from .states import (BatchDensityMatrix, BatchStateVector, DensityMatrix, HostConversionError, StateVector)
 

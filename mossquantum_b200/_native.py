@@ -30,7 +30,7 @@ MB_OP_GATE, MB_OP_CHANNEL = 0, 1
 FAMILIES = {"MATRIX": 0, "RX": 1, "RY": 2, "RZ": 3, "PHASE": 4, "CRX": 5, "CRY": 6, "CRZ": 7,
             "CPHASE": 8, "CCPHASE": 9}
 MB_OPF_ADJOINT = 1
-MB_APPLY_FUSED, MB_APPLY_PLAIN, MB_APPLY_PER_SAMPLE, MB_APPLY_DEVICE_THETA = 0, 1, 2, 4
+MB_APPLY_FUSED, MB_APPLY_PLAIN, MB_APPLY_PER_SAMPLE, MB_APPLY_DEVICE_THETA, MB_APPLY_TENSOR = 0, 1, 2, 4, 8
 
 
 class BackendError(RuntimeError):

@@ -79,12 +79,13 @@ def _as_circuit(operation):
     return cached
 
 
-def apply_(operation, state, theta=None, plain=False):
+def apply_(operation, state, theta=None, plain=False, tensor=False):
     """apply!(operation, state): execute a gate, channel or circuit on the device.
 
     theta: optional active-parameter values overriding the circuit's own (shape (P,), or
     (B, P) per-sample values on a batch state). plain=True runs one plain kernel launch per
-    gate (the per-call baseline) instead of the fused schedule.
+    gate (the per-call baseline) instead of the fused schedule; tensor=True (with plain) runs
+    dense 4-5 qubit gates and 2-qubit channels on the FP64 tensor cores.
     """
     if not isinstance(state, _DeviceState):
         raise TypeError("apply_ needs a B200 state")
@@ -98,6 +99,8 @@ def apply_(operation, state, theta=None, plain=False):
     values = circuit.active_parameters() if theta is None else theta
     values = np.asarray(values, dtype=np.float64)
     flags = N.MB_APPLY_PLAIN if plain else N.MB_APPLY_FUSED
+    if plain and tensor:
+        flags |= N.MB_APPLY_TENSOR
     if values.ndim == 2:
         if not state.is_batch or values.shape[0] != state.batch:
             raise ValueError("per-sample parameters need one row per batch sample")

@@ -78,6 +78,16 @@ int check_init() {
 
 ReduceWs ws() { return ReduceWs{g_ctx.partials, g_ctx.counters, g_ctx.partials_cap, g_ctx.ncounters}; }
 
+int launch_dense_block(double2* v, int64_t elems, int nsamples, const Pos& pos, const double2* m, int64_t mstride,
+                       int mode, bool allow_tensor, cudaStream_t st) {
+  static const bool disabled = getenv("MB_DMMA") && atoi(getenv("MB_DMMA")) == 0;
+  if (allow_tensor && !disabled && mstride == 0 && (pos.k == 4 || pos.k == 5)) {
+    const int rc = launch_dmma(v, elems, nsamples, pos, m, mode, st);
+    if (rc != MB_EUNSUPPORTED) return rc;
+  }
+  return launch_dense(v, elems, nsamples, pos, m, mstride, mode, st);
+}
+
 // ---------------------------------------------------------------------------------------------
 // Small host helpers
 // ---------------------------------------------------------------------------------------------
@@ -704,7 +714,7 @@ int plain_op(mb_circuit c, const COp& op, double2* v, int n, int is_dm, int nsam
       p.p[j] = op.pos[j];
       p.p[j + op.k] = op.pos[j] + n;
     }
-    return launch_dense(v, elems, nsamples, p, m, 0, dagger ? MAT_ADJOINT : MAT_PLAIN, st);
+    return launch_dense_block(v, elems, nsamples, p, m, 0, dagger ? MAT_ADJOINT : MAT_PLAIN, g_ctx.tensor_plain, st);
   }
   if (op.k == 0) {
     // Zero-qubit gate: a global scalar; on a density matrix |s|^2 (U rho U').
@@ -757,7 +767,7 @@ int plain_op(mb_circuit c, const COp& op, double2* v, int n, int is_dm, int nsam
       const int* sg = (mode == MAT_ADJOINT || mode == MAT_TRANSPOSE) ? op.sigma_inv : op.sigma;
       rc = launch_monomial(v, elems, nsamples, p, m, ms, mode, sg, d, st);
     } else {
-      rc = launch_dense(v, elems, nsamples, p, m, ms, mode, st);
+      rc = launch_dense_block(v, elems, nsamples, p, m, ms, mode, g_ctx.tensor_plain, st);
     }
     if (rc) return rc;
   }
@@ -811,7 +821,12 @@ extern "C" int mb_apply(mb_circuit c, mb_state s, const double* theta, size_t nt
     if (int rc = bind_circuit(c, theta, ntheta, rows)) return rc;
   }
   const int64_t stride = per_sample ? c->table_elems : 0;
-  if (flags & MB_APPLY_PLAIN) return apply_plain(c, s, stride);
+  if (flags & MB_APPLY_PLAIN) {
+    g_ctx.tensor_plain = (flags & MB_APPLY_TENSOR) != 0;
+    const int rc = apply_plain(c, s, stride);
+    g_ctx.tensor_plain = false;
+    return rc;
+  }
   return apply_fused(c, s, stride);
 }
 

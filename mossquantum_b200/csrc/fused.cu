@@ -830,7 +830,7 @@ static int plain_fop_launch(mb_circuit c, const FOp& f, double2* v, int64_t elem
   if (f.nb == 0) return MB_EUNSUPPORTED;
   if (f.cls == CLS_DIAG) return launch_diag(v, elems, nsamples, p, m, ms, f.mode, f.pactive, st);
   if (f.cls == CLS_MONO) return launch_monomial(v, elems, nsamples, p, m, ms, f.mode, f.sigma, f.d, st);
-  return launch_dense(v, elems, nsamples, p, m, ms, f.mode, st);
+  return launch_dense_block(v, elems, nsamples, p, m, ms, f.mode, true, st);
 }
 
 // Tile bits and register bits of the fused schedule. MB_TILE_BITS / MB_REG_BITS override

@@ -96,7 +96,12 @@ struct Ctx {
   double2* results = nullptr;
   unsigned* flags = nullptr;
   bool capturing = false;           // the library stream is recording a CUDA graph
+  bool tensor_plain = false;        // per-gate path: dense 4-5 qubit ops on the tensor cores
 };
+
+// Dense 4-5 qubit operators through K5 when allowed (MB_DMMA=0 disables it), else K0.
+int launch_dense_block(double2* v, int64_t elems, int nsamples, const Pos& pos, const double2* m, int64_t mstride,
+                       int mode, bool allow_tensor, cudaStream_t st);
 
 extern Ctx g_ctx;
 extern std::recursive_mutex g_mu;

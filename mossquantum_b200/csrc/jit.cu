@@ -106,6 +106,7 @@ __device__ __forceinline__ double2 cfma(double2 a, double2 b, double2 c) {
 __device__ __forceinline__ double2 ld(const double2* p) { return __ldg(p); }
 __device__ __forceinline__ double2 ldc(const double2* p) { double2 x = __ldg(p); return make_double2(x.x, -x.y); }
 __device__ __forceinline__ double2 neg(double2 a) { return make_double2(-a.x, -a.y); }
+__device__ __forceinline__ double2 cj(double2 a) { return make_double2(a.x, -a.y); }
 __device__ __forceinline__ u32 swz(u32 i) { return i ^ ((i >> 3) & 7u); }
 __device__ __forceinline__ u32 sa(const void* p) { return (u32)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ void mbar_init(u64* b) { asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(sa(b)) : "memory"); }
@@ -154,6 +155,7 @@ struct StageGen {
   bool lb64;           // pass-local index is a 64-bit global index (register sweep)
   std::vector<int> nm;
   std::string pre = "a";  // variable prefix
+  const std::map<int, int>* smap = nullptr;  // table offset -> slot of the pass's shared-memory copy
 
   // Selector classification: register bit k (>= 0), or -1 with a runtime expression.
   int regbit(int sel) const {
@@ -180,6 +182,13 @@ struct StageGen {
   }
   std::string v(int j) const { return pre + std::to_string(nm[j]); }
   std::string ldm(const MOp& m, int e) const {
+    if (!m.param && smap) {
+      auto it = smap->find(m.off[e]);
+      if (it != smap->end()) {
+        const std::string x = "smat[" + std::to_string(it->second) + "]";
+        return m.conj ? "cj(" + x + ")" : x;
+      }
+    }
     return std::string(m.conj ? "ldc" : "ld") + "(" + (m.param ? "tb" : "tab") + " + " + std::to_string(m.off[e]) + ")";
   }
 
@@ -344,15 +353,63 @@ CUfunction compile_kernel(const std::string& src, std::string* err) {
 
 bool jit_available() { return nvrtc().ok && drv().ok; }
 
+// Matrix elements of a pass that are the same for every sample (fixed gates and channels): the
+// kernel copies them from the table into shared memory once per CTA, so the gate loops read
+// them with uniform shared-memory loads instead of global loads. At most 2048 entries (32 KB).
+struct SharedMats {
+  std::map<int, int> slot;
+  std::vector<int> offs;
+};
+
+static SharedMats shared_mats(const Pass& p) {
+  SharedMats sm;
+  auto add = [&](int off) {
+    if (sm.slot.count(off)) return;
+    sm.slot[off] = int(sm.offs.size());
+    sm.offs.push_back(off);
+  };
+  for (const MOp& m : p.mops) {
+    if (m.param) continue;
+    switch (m.type) {
+      case MOP_U1: case MOP_CTRL: for (int e = 0; e < 4; ++e) add(m.off[e]); break;
+      case MOP_U2: for (int e = 0; e < 16; ++e) add(m.off[e]); break;
+      case MOP_DIAG: for (int e = 0; e < (1 << m.nsel); ++e) if ((m.active >> e) & 1) add(m.off[e]); break;
+      case MOP_CPHASE: if (!m.r1) add(m.off[0]); break;
+      default: break;
+    }
+  }
+  if (sm.offs.size() > 2048) sm = SharedMats();
+  return sm;
+}
+
+// File-scope table of the offsets and the in-kernel copy (run before the kernel's first barrier).
+static std::string shared_mats_decl(const SharedMats& sm) {
+  if (sm.offs.empty()) return "";
+  std::ostringstream o;
+  o << "__constant__ int k_moffs[" << sm.offs.size() << "] = {";
+  for (size_t i = 0; i < sm.offs.size(); ++i) o << (i ? "," : "") << sm.offs[i];
+  o << "};\n";
+  return o.str();
+}
+static std::string shared_mats_fill(const SharedMats& sm) {
+  if (sm.offs.empty()) return "";
+  std::ostringstream o;
+  o << "  __shared__ double2 smat[" << sm.offs.size() << "];\n  for (u32 i = threadIdx.x; i < " << sm.offs.size()
+    << "u; i += blockDim.x) smat[i] = __ldg(tab + k_moffs[i]);\n";
+  return o.str();
+}
+
 std::string jit_tile_source(const Pass& p, int R, int N) {
   std::ostringstream o;
   const int A = 1 << R;
   const int threads = 1 << (p.t - R);
   const TmaGeom& g = p.geom;
-  o << kPrelude;
+  const SharedMats smats = shared_mats(p);
+  o << kPrelude << shared_mats_decl(smats);
   o << "extern \"C\" __global__ void __launch_bounds__(" << threads << ", 1) mbk(const __grid_constant__ TMap tmap, "
     << "const double2* __restrict__ tab, long long tstride, long long tps, long long ntiles, u32* err) {\n";
   o << "  extern __shared__ unsigned char smem_raw[];\n  __shared__ __align__(8) u64 bar[2];\n  __shared__ int s_abort;\n";
+  o << shared_mats_fill(smats);
   o << "  double2* buf0 = (double2*)(((unsigned long long)smem_raw + 1023ull) & ~1023ull);\n";
   o << "  double2* bufs[2] = {buf0, buf0 + " << (1 << p.t) << "};\n";
   o << "  const u32 tx = threadIdx.x;\n";
@@ -421,6 +478,7 @@ std::string jit_tile_source(const Pass& p, int R, int N) {
     o << ";\n";
     for (int j = 0; j < A; ++j) o << "      a" << j << " = tl[swz(lb | " << reg_off_const(j, R, sd.reg) << ")];\n";
     StageGen sg{R, sd.reg, o, false, std::vector<int>(A)};
+    sg.smap = &smats.slot;
     for (int j = 0; j < A; ++j) sg.nm[j] = j;
     for (int q = 0; q < sd.nops; ++q) sg.emit(p.mops[sd.op0 + q]);
     for (int j = 0; j < A; ++j) o << "      tl[swz(lb | " << reg_off_const(j, R, sd.reg) << ")] = " << sg.v(j) << ";\n";
@@ -481,12 +539,14 @@ std::string jit_adjoint_source(const Pass& p, int R, int N) {
   const int nw = std::max(1, threads / 32);
   const int ngrad = int(p.grad_slots.size());
   const TmaGeom& g = p.geom;
-  o << kPrelude;
+  const SharedMats smats = shared_mats(p);
+  o << kPrelude << shared_mats_decl(smats);
   o << "extern \"C\" __global__ void __launch_bounds__(" << threads << ", 1) mbk(const __grid_constant__ TMap tmy, "
     << "const __grid_constant__ TMap tmd, const double2* __restrict__ tab, long long tstride, long long tps, "
     << "long long ntiles, u32* err, double* gpart, u32* gcount, double* gout, const int* __restrict__ gslot) {\n";
   o << "  extern __shared__ unsigned char smem_raw[];\n  __shared__ __align__(8) u64 bar[2];\n  __shared__ int s_abort;\n"
     << "  __shared__ bool lastcta;\n";
+  o << shared_mats_fill(smats);
   const unsigned T = 1u << p.t;
   o << "  double2* base0 = (double2*)(((unsigned long long)smem_raw + 1023ull) & ~1023ull);\n";
   o << "  double2* ybuf[2] = {base0, base0 + " << T << "};\n  double2* dbuf[2] = {base0 + " << 2 * T << ", base0 + "
@@ -555,6 +615,7 @@ std::string jit_adjoint_source(const Pass& p, int R, int N) {
         << reg_off_const(j, R, sd.reg) << ")];\n";
     StageGen gy{R, sd.reg, o, false, std::vector<int>(A), "y"};
     StageGen gd{R, sd.reg, o, false, std::vector<int>(A), "d"};
+    gy.smap = gd.smap = &smats.slot;
     for (int j = 0; j < A; ++j) gy.nm[j] = gd.nm[j] = j;
     for (int q = 0; q < sd.nops; ++q) {
       const MOp& m = p.mops[sd.op0 + q];
@@ -606,9 +667,11 @@ int jit_launch_adjoint(CUfunction fn, const CUtensorMap* my, const CUtensorMap* 
 std::string jit_reg_source(const Pass& p, int N) {
   std::ostringstream o;
   const int R = p.t, A = 1 << R;
-  o << kPrelude;
+  const SharedMats smats = shared_mats(p);
+  o << kPrelude << shared_mats_decl(smats);
   o << "extern \"C\" __global__ void __launch_bounds__(128) mbk(double2* __restrict__ v, const double2* __restrict__ tab, "
     << "long long tstride, long long groups, int nsamples) {\n";
+  if (!smats.offs.empty()) o << shared_mats_fill(smats) << "  __syncthreads();\n";
   o << "  const long long total = groups * nsamples;\n";
   o << "  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < total; g += (long long)gridDim.x * blockDim.x) {\n";
   o << "    const int b = (int)(g / groups);\n    u64 lb = (u64)(g - (long long)b * groups);\n";
@@ -623,6 +686,7 @@ std::string jit_reg_source(const Pass& p, int N) {
   for (int k = 0; k < R; ++k) reg[k] = p.bits[k];
   for (int j = 0; j < A; ++j) o << "    double2 a" << j << " = vs[lb | " << reg_off_const(j, R, reg) << "];\n";
   StageGen sg{R, reg, o, true, std::vector<int>(A)};
+  sg.smap = &smats.slot;
   for (int j = 0; j < A; ++j) sg.nm[j] = j;
   for (const MOp& m : p.mops) sg.emit(m);
   for (int j = 0; j < A; ++j) o << "    vs[lb | " << reg_off_const(j, R, reg) << "] = " << sg.v(j) << ";\n";

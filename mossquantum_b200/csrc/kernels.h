@@ -35,6 +35,11 @@ int launch_diag(double2* v, int64_t elems, int nsamples, const Pos& pos, const d
 int launch_monomial(double2* v, int64_t elems, int nsamples, const Pos& pos, const double2* mats,
                     int64_t mstride, int mode, const int* sigma_host, int d, cudaStream_t st);
 
+// Dense 4- or 5-qubit operator on the FP64 tensor cores (K5, dmma.cu); positions ascending,
+// one matrix shared by all samples. MB_EUNSUPPORTED when the shape does not fit.
+int launch_dmma(double2* v, int64_t elems, int nsamples, const Pos& pos, const double2* m, int mode,
+                cudaStream_t st);
+
 // ---- state utilities ---------------------------------------------------------------------
 int launch_set_basis(double2* v, int64_t elems, int nsamples, int64_t index, cudaStream_t st);
 int launch_to_density(const double2* psi, double2* rho, int n, int nsamples, cudaStream_t st);

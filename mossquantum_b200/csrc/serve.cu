@@ -134,7 +134,7 @@ int make_class(mb_server S, mb_circuit block, bool dm, Class** out) {
   c->dm = dm;
   c->n = block->n;
   c->elems = dm ? (int64_t(1) << (2 * block->n)) : (int64_t(1) << block->n);
-  c->sbytes = round256(sizeof(double2) * size_t(c->elems));
+  c->sbytes = sizeof(double2) * size_t(c->elems);  // samples back to back, as the batch kernels index them
   int rc = circuit_clone(block, &c->priv);
   if (rc) return rc;
   if (dm) {
@@ -303,10 +303,10 @@ void admit(mb_server S) {
 
 int ensure_theta(Class* c, size_t count) {
   if (count <= c->theta_cap) return MB_OK;
+  const size_t cap = std::max<size_t>(count, 2 * c->theta_cap);
   dev_free(c->d_theta);
   c->d_theta = nullptr;
   c->theta_cap = 0;
-  const size_t cap = std::max<size_t>(count, 2 * c->theta_cap);
   int rc = dev_alloc((void**)&c->d_theta, sizeof(double) * cap);
   if (!rc) c->theta_cap = cap;
   return rc;
