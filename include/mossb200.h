@@ -209,6 +209,20 @@ MB_API int mb_observable_apply(mb_observable o, mb_state in, mb_state out);
  * of the output index), normalised; out holds 2^nq doubles per sample. */
 MB_API int mb_probabilities(mb_state s, const int* qubits, int nq, double* out);
 
+/* ---- measurement and post-selection (src/execution/measurement.jl:4-201,
+ *      src/execution/post_selection.jl:3-112) -------------------------------------------
+ * w receives 2 doubles per sample: the unnormalised weights of outcome 0 and 1 of `qubit`
+ * (sum of |psi_i|^2, or Re rho_ii, over the indices whose bit is 0 / 1); the host normalises
+ * them and draws outcomes with its own random stream (discrete_sample, sampling.jl:3-18). */
+MB_API int mb_qubit_weights(mb_state s, int qubit, double* w);
+/* Collapses sample b onto outcomes[b] and divides by sqrt(probs[b]) (_collapse_batch_column!,
+ * measurement.jl); with auto_reset the kept amplitudes move to the qubit's 0 branch. Density
+ * matrices get the operator on the row and column bits. Every sample is validated first. */
+MB_API int mb_collapse(mb_state s, int qubit, const int* outcomes, const double* probs, int auto_reset);
+/* dst (pure, n-1 qubits, same batch) = scales[b] * the outcomes[b] slice of src
+ * (_qubit_slice, measurement.jl; post_select without keep, post_selection.jl). */
+MB_API int mb_remove_qubit(mb_state src, int qubit, const int* outcomes, const double* scales, mb_state dst);
+
 /* ---- adjoint gradients (src/differentiation/objectives.jl:183-296) --------------------
  * value = sum_b w_b Re<H>_b after applying the circuit to a copy of `init`; grad[slot] =
  * d value / d theta[slot] (slots, not independent parameters: the host accumulates a

@@ -17,6 +17,8 @@ from .objectives import (AdjointGradient, B200AdjointGradient, BatchExpectationO
                          UnsupportedGradient, differentiable_value, evaluate, evaluate_batch, supports_gradient,
                          value_and_gradient, value_and_pullback)
 from .fusion import fuse_gates
+from .measurement import (MeasurementRecord, QMeasure, QSelect, discrete_sample, measure, measure_, post_select,
+                          post_select_)
 from .operators import QubitsOperator, QubitsTerm
 from .states import (BatchDensityMatrix, BatchStateVector, DensityMatrix, HostConversionError, StateVector)
 

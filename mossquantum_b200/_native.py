@@ -142,6 +142,9 @@ def load():
         "mb_tuning_get": ([ctypes.c_int, ip, ip], ctypes.c_int),
         "mb_autotune": ([vp, vp, dp, sz, ctypes.c_int, ip, ip, dp], ctypes.c_int),
         "mb_measure_fp64_peak": ([dp], ctypes.c_int),
+        "mb_qubit_weights": ([vp, ctypes.c_int, dp], ctypes.c_int),
+        "mb_collapse": ([vp, ctypes.c_int, ip, dp, ctypes.c_int], ctypes.c_int),
+        "mb_remove_qubit": ([vp, ctypes.c_int, ip, dp, vp], ctypes.c_int),
         "mb_server_start": ([ctypes.POINTER(MbServerConfig), ctypes.POINTER(vp)], ctypes.c_int),
         "mb_submit": ([vp, ctypes.POINTER(MbRequest), ctypes.POINTER(ctypes.c_uint64)], ctypes.c_int),
         "mb_poll": ([vp, ctypes.c_uint64, ctypes.POINTER(MbResult), dp, sz], ctypes.c_int),

@@ -206,13 +206,36 @@ def counts(rng, state, shots, qubits=None):
 
 
 class SimulationResult:
+    """Final state and the measurement records in execution order (one list per sample for
+    batches), as SimulationResult / BatchSimulationResult (simulation.jl:21-40)."""
+
     def __init__(self, state, records):
         self.state = state
         self.records = records
+        self.measurements = records
 
 
 def simulate(circuit, state, rng=None):
-    """simulate(circuit, state): bulk record-free execution for gate/channel circuits
-    (the simulate_circuit! hook, simulation.jl:174-175); the input is not modified."""
-    out = apply_(circuit, state.copy())
-    return SimulationResult(out, [])
+    """simulate(circuit, state; rng): executes a copy of the state (simulation.jl:174-231).
+    Runs of gates and channels execute as fused device passes; QMeasure / QSelect run on the
+    device with outcomes drawn from rng in instruction order, then sample order."""
+    from .measurement import QMeasure, QSelect, run_instruction
+    rng = np.random.default_rng() if rng is None else rng
+    out = state.copy()
+    records = [[] for _ in range(out.batch)] if out.is_batch else []
+    run = []
+
+    def flush(st):
+        if run:
+            st = apply_(QCircuit(list(run)), st)
+            run.clear()
+        return st
+
+    for it in _as_circuit(circuit).flat():
+        if isinstance(it, (QMeasure, QSelect)):
+            out = flush(out)
+            out = run_instruction(it, out, rng, records)
+        else:
+            run.append(it)
+    out = flush(out)
+    return SimulationResult(out, records)

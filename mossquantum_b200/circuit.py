@@ -27,7 +27,8 @@ class QCircuit(Instruction):
         self._compiled = {}
 
     def push(self, item):
-        if not isinstance(item, (Gate, QuantumMap, QCircuit)):
+        from .measurement import QMeasure, QSelect
+        if not isinstance(item, (Gate, QuantumMap, QCircuit, QMeasure, QSelect)):
             raise TypeError(f"unsupported instruction {type(item).__name__}")
         self.items.append(item)
         self._invalidate()
@@ -72,6 +73,10 @@ class QCircuit(Instruction):
 
     def adjoint(self):
         return QCircuit([it.adjoint() for it in reversed(self.flat())])
+
+    def has_measurement(self):
+        from .measurement import QMeasure, QSelect
+        return any(isinstance(it, (QMeasure, QSelect)) for it in self.flat())
 
     def has_channel(self):
         return any(isinstance(it, QuantumMap) for it in self.flat())
