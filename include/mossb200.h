@@ -223,6 +223,19 @@ MB_API int mb_collapse(mb_state s, int qubit, const int* outcomes, const double*
  * (_qubit_slice, measurement.jl; post_select without keep, post_selection.jl). */
 MB_API int mb_remove_qubit(mb_state src, int qubit, const int* outcomes, const double* scales, mb_state dst);
 
+/* ---- partial trace, inner products, fidelities ------------------------------------------
+ * partial_tr (observables/partial_trace.jl:11-97): out = Tr_sites(in) per sample; sites are
+ * k distinct zero-based qubits, 0 < k < n; the remaining qubits keep their order as the low
+ * bits of out, a DensityMatrix (BatchDensityMatrix for batch inputs) of n - k qubits. A pure
+ * input gives V V' (partial_tr(::StateVector), partial_trace.jl:58-71). */
+MB_API int mb_partial_trace(mb_state in, const int* sites, int k, mb_state out);
+/* <x|y> per sample (dot(x, y), conjugating x) for pure states of equal shape; 2 doubles each. */
+MB_API int mb_inner(mb_state x, mb_state y, double* out);
+/* <y|rho|y> per sample: fidelity(::DensityMatrix, ::StateVector) (density_matrix.jl:129). */
+MB_API int mb_sandwich(mb_state rho, mb_state y, double* out);
+/* Copies sample `index` of a batch state into a single state of the same kind and size. */
+MB_API int mb_state_extract(mb_state src, int index, mb_state dst);
+
 /* ---- adjoint gradients (src/differentiation/objectives.jl:183-296) --------------------
  * value = sum_b w_b Re<H>_b after applying the circuit to a copy of `init`; grad[slot] =
  * d value / d theta[slot] (slots, not independent parameters: the host accumulates a

@@ -20,6 +20,7 @@ from .fusion import fuse_gates
 from .measurement import (MeasurementRecord, QMeasure, QSelect, discrete_sample, measure, measure_, post_select,
                           post_select_)
 from .operators import QubitsOperator, QubitsTerm
+from .reduced import fidelity, inner, partial_tr, trace
 from .states import (BatchDensityMatrix, BatchStateVector, DensityMatrix, HostConversionError, StateVector)
 
 __all__ = [k for k in dir() if not k.startswith("_")]

@@ -143,6 +143,10 @@ def load():
         "mb_autotune": ([vp, vp, dp, sz, ctypes.c_int, ip, ip, dp], ctypes.c_int),
         "mb_measure_fp64_peak": ([dp], ctypes.c_int),
         "mb_qubit_weights": ([vp, ctypes.c_int, dp], ctypes.c_int),
+        "mb_partial_trace": ([vp, ip, ctypes.c_int, vp], ctypes.c_int),
+        "mb_inner": ([vp, vp, dp], ctypes.c_int),
+        "mb_sandwich": ([vp, vp, dp], ctypes.c_int),
+        "mb_state_extract": ([vp, ctypes.c_int, vp], ctypes.c_int),
         "mb_collapse": ([vp, ctypes.c_int, ip, dp, ctypes.c_int], ctypes.c_int),
         "mb_remove_qubit": ([vp, ctypes.c_int, ip, dp, vp], ctypes.c_int),
         "mb_server_start": ([ctypes.POINTER(MbServerConfig), ctypes.POINTER(vp)], ctypes.c_int),
