@@ -13,6 +13,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cstdio>
 #include <cstring>
 #include <functional>
@@ -323,7 +324,25 @@ CUfunction compile_kernel(const std::string& src, std::string* err) {
     return nullptr;
   }
   const char* opts[] = {"--gpu-architecture=sm_100a", "-std=c++17", "--fmad=true", "-default-device"};
+  const auto t0 = std::chrono::steady_clock::now();
   const int rc = n.compile(prog, 4, opts);
+  if (const char* dir = getenv("MB_JIT_DUMP")) {
+    // Development aid: every compiled source and its compile time.
+    const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    const size_t h = std::hash<std::string>()(src);
+    char path[512];
+    snprintf(path, sizeof(path), "%s/mbk_%016zx.cu", dir, h);
+    if (FILE* f = fopen(path, "w")) {
+      fwrite(src.data(), 1, src.size(), f);
+      fclose(f);
+    }
+    snprintf(path, sizeof(path), "%s/compile_times.txt", dir);
+    std::lock_guard<std::mutex> lk(g_jit_mu);
+    if (FILE* f = fopen(path, "a")) {
+      fprintf(f, "mbk_%016zx %.3f s %zu bytes rc=%d\n", h, sec, src.size(), rc);
+      fclose(f);
+    }
+  }
   if (rc != 0) {
     size_t ls = 0;
     n.log_size(prog, &ls);
@@ -694,9 +713,10 @@ std::string jit_reg_source(const Pass& p, int N) {
   return o.str();
 }
 
-int jit_prepare(std::vector<std::string>& sources, std::vector<CUfunction>& out, std::string* err) {
+int jit_prepare(std::vector<std::string>& sources, std::vector<CUfunction>& out, std::string* err, double budget_s) {
   out.assign(sources.size(), nullptr);
   std::vector<std::string> errs(sources.size());
+  std::vector<char> skipped(sources.size(), 0);
   std::vector<std::thread> pool;
   const size_t nthreads = std::max<size_t>(1, std::min<size_t>(sources.size(), std::thread::hardware_concurrency()));
   // Compilation runs on worker threads; modules load on the worker threads too, which is
@@ -704,15 +724,27 @@ int jit_prepare(std::vector<std::string>& sources, std::vector<CUfunction>& out,
   int dev = 0;
   cudaGetDevice(&dev);
   std::atomic<size_t> next{0};
+  const auto t0 = std::chrono::steady_clock::now();
+  auto elapsed = [&] { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); };
   for (size_t w = 0; w < nthreads; ++w)
     pool.emplace_back([&] {
       cudaSetDevice(dev);
       cudaFree(nullptr);
-      for (size_t i = next++; i < sources.size(); i = next++) out[i] = compile_kernel(sources[i], &errs[i]);
+      for (size_t i = next++; i < sources.size(); i = next++) {
+        // Past the budget only kernels already in the cache are taken; the rest run interpreted.
+        if (budget_s > 0 && elapsed() > budget_s) {
+          std::lock_guard<std::mutex> lk(g_jit_mu);
+          auto it = g_cache.find(sources[i]);
+          if (it != g_cache.end()) out[i] = it->second;
+          else skipped[i] = 1;
+          continue;
+        }
+        out[i] = compile_kernel(sources[i], &errs[i]);
+      }
     });
   for (auto& t : pool) t.join();
   for (size_t i = 0; i < sources.size(); ++i)
-    if (!out[i]) {
+    if (!out[i] && !skipped[i]) {
       *err = errs[i];
       return MB_EUNSUPPORTED;
     }

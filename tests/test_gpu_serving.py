@@ -79,11 +79,13 @@ def test_serving_admission_budget(mq):
     from mossquantum_b200 import workloads as W
     from mossquantum_b200.serving import Server
     small = W.hea_layer(8)
-    big = W.hea_layer(14)
+    big = W.hea_layer(15)
     rng = W.rng_for(4, 8)
-    with Server(budget_bytes=1 << 20) as srv:   # 1 MiB: an 8-qubit state is 4 KiB, 14 qubits 256 KiB (+ gradients)
+    # 1 MiB budget: an 8-qubit state is 4 KiB; a 15-qubit gradient request needs its 512 KiB
+    # state plus y and delta (another 1 MiB), more than the whole budget
+    with Server(budget_bytes=1 << 20) as srv:
         t_ok = [srv.submit(small, 8, W.tfim(8), rng.uniform(0, 6, (3, 24))) for _ in range(4)]
-        t_big = srv.submit(big, 14, W.tfim(14), rng.uniform(0, 6, (30, 42)), gradient=True)
+        t_big = srv.submit(big, 15, W.tfim(15), rng.uniform(0, 6, (30, 45)), gradient=True)
         for t in t_ok:
             assert np.isfinite(srv.wait(t, timeout_s=120).value.real)
         with pytest.raises(Exception, match="budget"):
