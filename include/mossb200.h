@@ -235,6 +235,10 @@ MB_API int mb_inner(mb_state x, mb_state y, double* out);
 MB_API int mb_sandwich(mb_state rho, mb_state y, double* out);
 /* Copies sample `index` of a batch state into a single state of the same kind and size. */
 MB_API int mb_state_extract(mb_state src, int index, mb_state dst);
+/* Copies a single state into every sample of a batch state of the same kind and size. */
+MB_API int mb_state_broadcast(mb_state src, mb_state dst);
+/* dst (batch of copies * B samples) = `copies` back-to-back copies of the batch src. */
+MB_API int mb_state_tile(mb_state src, int copies, mb_state dst);
 
 /* ---- adjoint gradients (src/differentiation/objectives.jl:183-296) --------------------
  * value = sum_b w_b Re<H>_b after applying the circuit to a copy of `init`; grad[slot] =

@@ -21,6 +21,8 @@ from .measurement import (MeasurementRecord, QMeasure, QSelect, discrete_sample,
                           post_select_)
 from .operators import QubitsOperator, QubitsTerm
 from .reduced import fidelity, inner, partial_tr, trace
+from .sampled import (FiniteDifference, GradientEstimate, ParameterShift, SPSAGradient, estimate_gradient,
+                      parameter_shift_rule)
 from .states import (BatchDensityMatrix, BatchStateVector, DensityMatrix, HostConversionError, StateVector)
 
 __all__ = [k for k in dir() if not k.startswith("_")]

@@ -147,6 +147,8 @@ def load():
         "mb_inner": ([vp, vp, dp], ctypes.c_int),
         "mb_sandwich": ([vp, vp, dp], ctypes.c_int),
         "mb_state_extract": ([vp, ctypes.c_int, vp], ctypes.c_int),
+        "mb_state_broadcast": ([vp, vp], ctypes.c_int),
+        "mb_state_tile": ([vp, ctypes.c_int, vp], ctypes.c_int),
         "mb_collapse": ([vp, ctypes.c_int, ip, dp, ctypes.c_int], ctypes.c_int),
         "mb_remove_qubit": ([vp, ctypes.c_int, ip, dp, vp], ctypes.c_int),
         "mb_server_start": ([ctypes.POINTER(MbServerConfig), ctypes.POINTER(vp)], ctypes.c_int),

@@ -226,3 +226,37 @@ extern "C" int mb_state_extract(mb_state src, int index, mb_state dst) {
   MB_CHECK_CUDA(cudaStreamSynchronize(g_ctx.stream));
   return MB_OK;
 }
+
+extern "C" int mb_state_broadcast(mb_state src, mb_state dst) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (int rc = check_init()) return rc;
+  if (!src || !dst) return MB_EINVAL;
+  const bool ok = ((src->kind == MB_PURE && dst->kind == MB_BATCH_PURE) ||
+                   (src->kind == MB_DENSITY && dst->kind == MB_BATCH_DENSITY)) && dst->n == src->n;
+  if (!ok) {
+    set_error("broadcast needs a single source and a batch destination of the same kind and size");
+    return MB_EINVAL;
+  }
+  for (int b = 0; b < dst->batch; ++b)
+    MB_CHECK_CUDA(cudaMemcpyAsync(dst->d + int64_t(b) * dst->elems, src->d, sizeof(double2) * src->elems,
+                                  cudaMemcpyDeviceToDevice, g_ctx.stream));
+  MB_CHECK_CUDA(cudaStreamSynchronize(g_ctx.stream));
+  return MB_OK;
+}
+
+extern "C" int mb_state_tile(mb_state src, int copies, mb_state dst) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (int rc = check_init()) return rc;
+  if (!src || !dst || copies < 0) return MB_EINVAL;
+  if (src->kind != dst->kind || src->kind < MB_BATCH_PURE || dst->n != src->n ||
+      int64_t(dst->batch) != int64_t(src->batch) * copies) {
+    set_error("tile needs batch states of one kind and size, the destination holding `copies` copies of the source");
+    return MB_EINVAL;
+  }
+  const size_t bytes = sizeof(double2) * size_t(src->elems) * src->batch;
+  for (int c = 0; c < copies; ++c)
+    MB_CHECK_CUDA(cudaMemcpyAsync(reinterpret_cast<char*>(dst->d) + bytes * c, src->d, bytes, cudaMemcpyDeviceToDevice,
+                                  g_ctx.stream));
+  MB_CHECK_CUDA(cudaStreamSynchronize(g_ctx.stream));
+  return MB_OK;
+}

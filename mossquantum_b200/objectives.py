@@ -110,6 +110,9 @@ def evaluate_batch(objective, values):
 
 
 def supports_gradient(method, objective) -> bool:
+    from .sampled import SAMPLED_METHODS, supports_sampled
+    if isinstance(method, SAMPLED_METHODS):
+        return supports_sampled(method, objective)
     if not isinstance(method, AdjointGradient) or not isinstance(objective, ExpectationObjective):
         return False
     try:
@@ -119,8 +122,14 @@ def supports_gradient(method, objective) -> bool:
     return compiled.gradient_ok and objective.observable.is_hermitian()
 
 
-def value_and_gradient(method, objective, values):
-    """(value, gradient) with one gradient entry per independent parameter."""
+def value_and_gradient(method, objective, values, rng=None):
+    """(value, gradient) with one gradient entry per independent parameter. Adjoint gradients
+    run as one device reverse sweep; ParameterShift / FiniteDifference / SPSAGradient evaluate
+    their shifted parameter vectors as one batch on the device."""
+    from .sampled import SAMPLED_METHODS, estimate_gradient
+    if isinstance(method, SAMPLED_METHODS):
+        est = estimate_gradient(method, objective, values, rng=rng)
+        return est.value, est.gradient
     if not supports_gradient(method, objective):
         raise UnsupportedGradient(f"{method!r} does not support this objective")
     slots = objective._slots(values)
