@@ -68,6 +68,9 @@ extern "C" {
 #define MB_FAM_CRZ 7         /* CRzGate                                                      */
 #define MB_FAM_CPHASE 8      /* CPHASEGate CONTROL(PHASE(θ))                                 */
 #define MB_FAM_CCPHASE 9     /* CCPHASEGate CONTROLCONTROL(PHASE(θ)), pos = (c1, c2, target) */
+#define MB_FAM_SELECT 10     /* one of nkraus operators in data (1-3 positions), chosen by the */
+                             /* integer value of its parameter: the branch of a Kraus trajectory */
+                             /* (execution/noisy_execution.jl:40-120); not differentiable        */
 
 #define MB_OPF_ADJOINT 1     /* AdjointQuantumGate wrapper (gates/quantum_gate.jl:32-45)     */
 
@@ -222,6 +225,8 @@ MB_API int mb_collapse(mb_state s, int qubit, const int* outcomes, const double*
 /* dst (pure, n-1 qubits, same batch) = scales[b] * the outcomes[b] slice of src
  * (_qubit_slice, measurement.jl; post_select without keep, post_selection.jl). */
 MB_API int mb_remove_qubit(mb_state src, int qubit, const int* outcomes, const double* scales, mb_state dst);
+/* Multiplies sample b by scales[b] (renormalising trajectories, normalize!). */
+MB_API int mb_scale_samples(mb_state s, const double* scales);
 
 /* ---- partial trace, inner products, fidelities ------------------------------------------
  * partial_tr (observables/partial_trace.jl:11-97): out = Tr_sites(in) per sample; sites are

@@ -23,6 +23,7 @@ from .operators import QubitsOperator, QubitsTerm
 from .reduced import fidelity, inner, partial_tr, trace
 from .sampled import (FiniteDifference, GradientEstimate, ParameterShift, SPSAGradient, estimate_gradient,
                       parameter_shift_rule)
+from .trajectories import CountsResult, DensityMatrixEvolution, KrausTrajectory, execute, run_trajectories
 from .states import (BatchDensityMatrix, BatchStateVector, DensityMatrix, HostConversionError, StateVector)
 
 __all__ = [k for k in dir() if not k.startswith("_")]

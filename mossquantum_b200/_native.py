@@ -28,7 +28,7 @@ MB_ENOTREADY = -8
 MB_PURE, MB_DENSITY, MB_BATCH_PURE, MB_BATCH_DENSITY = 0, 1, 2, 3
 MB_OP_GATE, MB_OP_CHANNEL = 0, 1
 FAMILIES = {"MATRIX": 0, "RX": 1, "RY": 2, "RZ": 3, "PHASE": 4, "CRX": 5, "CRY": 6, "CRZ": 7,
-            "CPHASE": 8, "CCPHASE": 9}
+            "CPHASE": 8, "CCPHASE": 9, "SELECT": 10}
 MB_OPF_ADJOINT = 1
 MB_APPLY_FUSED, MB_APPLY_PLAIN, MB_APPLY_PER_SAMPLE, MB_APPLY_DEVICE_THETA, MB_APPLY_TENSOR = 0, 1, 2, 4, 8
 
@@ -151,6 +151,7 @@ def load():
         "mb_state_tile": ([vp, ctypes.c_int, vp], ctypes.c_int),
         "mb_collapse": ([vp, ctypes.c_int, ip, dp, ctypes.c_int], ctypes.c_int),
         "mb_remove_qubit": ([vp, ctypes.c_int, ip, dp, vp], ctypes.c_int),
+        "mb_scale_samples": ([vp, dp], ctypes.c_int),
         "mb_server_start": ([ctypes.POINTER(MbServerConfig), ctypes.POINTER(vp)], ctypes.c_int),
         "mb_submit": ([vp, ctypes.POINTER(MbRequest), ctypes.POINTER(ctypes.c_uint64)], ctypes.c_int),
         "mb_poll": ([vp, ctypes.c_uint64, ctypes.POINTER(MbResult), dp, sz], ctypes.c_int),

@@ -153,6 +153,8 @@ class QCircuit(Instruction):
                 extra = it.mat().tobytes()
             if isinstance(it, QuantumMap):
                 extra = b"".join(k.tobytes() for k in it.kraus)
+            if hasattr(it, "signature_data"):
+                extra = it.signature_data()
             sig.append((type(it).__name__, getattr(it, "parent", None).__class__.__name__, it.positions,
                         tuple(act or ()), frozen, extra))
         return hash(tuple(sig))

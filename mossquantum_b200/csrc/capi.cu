@@ -118,6 +118,7 @@ static int family_arity(int fam) {
     case MB_FAM_RX: case MB_FAM_RY: case MB_FAM_RZ: case MB_FAM_PHASE: return 1;
     case MB_FAM_CRX: case MB_FAM_CRY: case MB_FAM_CRZ: case MB_FAM_CPHASE: return 2;
     case MB_FAM_CCPHASE: return 3;
+    case MB_FAM_SELECT: return 0;  // 1..3 positions, checked separately
     default: return -1;
   }
 }
@@ -490,6 +491,41 @@ extern "C" int mb_circuit_create(const mb_op* ops, size_t nops, int n, mb_circui
       }
       for (auto& x : M) table.push_back(d2(x));
       off += int64_t(d) * d;
+    } else if (o.family == MB_FAM_SELECT) {
+      // Operator j of nkraus, chosen per parameter row by k_bind; stored ordered after the
+      // slot the bound matrix occupies.
+      if (o.nq < 1 || o.nq > 3 || o.nkraus < 1 || !o.data || !finite_mat(o.data, size_t(o.nkraus) * d * d * 2)) {
+        set_error("instruction %zu: a selection needs 1-3 positions and finite operators", i);
+        return MB_EINVAL;
+      }
+      if (o.slot < 0 && !std::isfinite(o.value)) {
+        set_error("instruction %zu: parameter must be finite", i);
+        return MB_EINVAL;
+      }
+      op.parametric = true;
+      op.cls = CLS_DENSE;
+      BindRec br{};
+      br.family = o.family;
+      br.flags = 0;
+      br.slot = o.slot;
+      br.k = o.nq;
+      br.value = o.value;
+      br.mat_off = int(off);
+      br.gen_off = -1;
+      br.nopt = o.nkraus;
+      for (int a = 0; a < d; ++a) br.perm[a] = perm[a];
+      table.resize(table.size() + size_t(d) * d, cz());
+      for (int kk = 0; kk < o.nkraus; ++kk) {
+        const double* K = o.data + size_t(kk) * d * d * 2;
+        for (int bp = 0; bp < d; ++bp)
+          for (int ap = 0; ap < d; ++ap) {
+            const int a = perm[ap], b = perm[bp];
+            table.push_back(make_double2(K[2 * (a + b * d)], K[2 * (a + b * d) + 1]));
+          }
+      }
+      off += int64_t(d) * d * (1 + o.nkraus);
+      if (o.slot >= 0) max_slot = std::max(max_slot, o.slot);
+      c->binds.push_back(br);
     } else {
       int ar = family_arity(o.family);
       if (ar < 0 || ar != o.nq) {

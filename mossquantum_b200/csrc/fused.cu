@@ -962,10 +962,13 @@ static void prepare_jit(Schedule* S) {
   if ((!want_jit(S->N) && !S->adjoint) || !jit_available()) return;
   std::vector<std::string> src;
   std::vector<Pass*> who;
+  // One sample: every thread reads row 0 of the matrix table, so the parametric elements can be
+  // staged in shared memory with the fixed ones.
+  const bool single = S->nsamples == 1;
   for (Pass& p : S->passes) {
-    if (p.kind == PASS_TILE && S->adjoint) src.push_back(jit_adjoint_source(p, S->R, S->N));
-    else if (p.kind == PASS_TILE) src.push_back(jit_tile_source(p, S->R, S->N));
-    else if (p.kind == PASS_REG) src.push_back(jit_reg_source(p, S->N));
+    if (p.kind == PASS_TILE && S->adjoint) src.push_back(jit_adjoint_source(p, S->R, S->N, single));
+    else if (p.kind == PASS_TILE) src.push_back(jit_tile_source(p, S->R, S->N, single));
+    else if (p.kind == PASS_REG) src.push_back(jit_reg_source(p, S->N, single));
     else continue;
     who.push_back(&p);
   }

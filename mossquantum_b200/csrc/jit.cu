@@ -183,7 +183,7 @@ struct StageGen {
   }
   std::string v(int j) const { return pre + std::to_string(nm[j]); }
   std::string ldm(const MOp& m, int e) const {
-    if (!m.param && smap) {
+    if (smap) {
       auto it = smap->find(m.off[e]);
       if (it != smap->end()) {
         const std::string x = "smat[" + std::to_string(it->second) + "]";
@@ -380,7 +380,9 @@ struct SharedMats {
   std::vector<int> offs;
 };
 
-static SharedMats shared_mats(const Pass& p) {
+// with_params: also stage the per-sample (parametric) elements and derivative generators;
+// valid for single-sample schedules, where every thread reads sample 0's row.
+static SharedMats shared_mats(const Pass& p, bool with_params) {
   SharedMats sm;
   auto add = [&](int off) {
     if (sm.slot.count(off)) return;
@@ -388,12 +390,13 @@ static SharedMats shared_mats(const Pass& p) {
     sm.offs.push_back(off);
   };
   for (const MOp& m : p.mops) {
-    if (m.param) continue;
+    if (m.param && !with_params) continue;
     switch (m.type) {
       case MOP_U1: case MOP_CTRL: for (int e = 0; e < 4; ++e) add(m.off[e]); break;
       case MOP_U2: for (int e = 0; e < 16; ++e) add(m.off[e]); break;
       case MOP_DIAG: for (int e = 0; e < (1 << m.nsel); ++e) if ((m.active >> e) & 1) add(m.off[e]); break;
       case MOP_CPHASE: if (!m.r1) add(m.off[0]); break;
+      case MOP_GRAD: for (int e = 0; e < (m.nsel == 1 ? 4 : 16); ++e) add(m.off[e]); break;
       default: break;
     }
   }
@@ -418,12 +421,12 @@ static std::string shared_mats_fill(const SharedMats& sm) {
   return o.str();
 }
 
-std::string jit_tile_source(const Pass& p, int R, int N) {
+std::string jit_tile_source(const Pass& p, int R, int N, bool stage_params) {
   std::ostringstream o;
   const int A = 1 << R;
   const int threads = 1 << (p.t - R);
   const TmaGeom& g = p.geom;
-  const SharedMats smats = shared_mats(p);
+  const SharedMats smats = shared_mats(p, stage_params);
   o << kPrelude << shared_mats_decl(smats);
   o << "extern \"C\" __global__ void __launch_bounds__(" << threads << ", 1) mbk(const __grid_constant__ TMap tmap, "
     << "const double2* __restrict__ tab, long long tstride, long long tps, long long ntiles, u32* err) {\n";
@@ -520,7 +523,13 @@ std::string jit_tile_source(const Pass& p, int R, int N) {
 static void emit_grad(std::ostringstream& o, const MOp& m, const StageGen& gy, const StageGen& gd, int R, int nw) {
   const int A = 1 << R;
   const std::string tabn = m.param ? "tb" : "tab";
-  auto L = [&](int e) { return "ld(" + tabn + " + " + std::to_string(m.off[e]) + ")"; };
+  auto L = [&](int e) {
+    if (gy.smap) {
+      auto it = gy.smap->find(m.off[e]);
+      if (it != gy.smap->end()) return "smat[" + std::to_string(it->second) + "]";
+    }
+    return "ld(" + tabn + " + " + std::to_string(m.off[e]) + ")";
+  };
   o << "{ double gs = 0.0;\n";
   if (m.nsel == 1) {
     const int b = 1 << m.r0;
@@ -551,14 +560,14 @@ static void emit_grad(std::ostringstream& o, const MOp& m, const StageGen& gy, c
   o << "  if ((tx & 31u) == 0u) gw[" << m.active << " * " << nw << " + (tx >> 5)] += gs;\n}\n";
 }
 
-std::string jit_adjoint_source(const Pass& p, int R, int N) {
+std::string jit_adjoint_source(const Pass& p, int R, int N, bool stage_params) {
   std::ostringstream o;
   const int A = 1 << R;
   const int threads = 1 << (p.t - R);
   const int nw = std::max(1, threads / 32);
   const int ngrad = int(p.grad_slots.size());
   const TmaGeom& g = p.geom;
-  const SharedMats smats = shared_mats(p);
+  const SharedMats smats = shared_mats(p, stage_params);
   o << kPrelude << shared_mats_decl(smats);
   o << "extern \"C\" __global__ void __launch_bounds__(" << threads << ", 1) mbk(const __grid_constant__ TMap tmy, "
     << "const __grid_constant__ TMap tmd, const double2* __restrict__ tab, long long tstride, long long tps, "
@@ -683,10 +692,10 @@ int jit_launch_adjoint(CUfunction fn, const CUtensorMap* my, const CUtensorMap* 
   return MB_OK;
 }
 
-std::string jit_reg_source(const Pass& p, int N) {
+std::string jit_reg_source(const Pass& p, int N, bool stage_params) {
   std::ostringstream o;
   const int R = p.t, A = 1 << R;
-  const SharedMats smats = shared_mats(p);
+  const SharedMats smats = shared_mats(p, stage_params);
   o << kPrelude << shared_mats_decl(smats);
   o << "extern \"C\" __global__ void __launch_bounds__(128) mbk(double2* __restrict__ v, const double2* __restrict__ tab, "
     << "long long tstride, long long groups, int nsamples) {\n";

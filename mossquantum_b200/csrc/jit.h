@@ -9,8 +9,8 @@
 
 namespace mb {
 bool jit_available();
-std::string jit_tile_source(const Pass& p, int R, int N);
-std::string jit_reg_source(const Pass& p, int N);
+std::string jit_tile_source(const Pass& p, int R, int N, bool stage_params);
+std::string jit_reg_source(const Pass& p, int N, bool stage_params);
 // Compiles every source (in parallel, cached by text); fills out[i] or fails with err. With a
 // positive budget (seconds) sources not started within it are skipped (out[i] = nullptr) and
 // the call still succeeds; a source that fails to compile always fails the call.
@@ -18,7 +18,7 @@ int jit_prepare(std::vector<std::string>& sources, std::vector<CUfunction>& out,
                 double budget_s = 0);
 int jit_launch_tile(CUfunction fn, const CUtensorMap* map, const double2* tab, int64_t tstride, int64_t tps,
                     int64_t ntiles, unsigned* err, int threads, size_t shm, int grid, cudaStream_t st);
-std::string jit_adjoint_source(const Pass& p, int R, int N);
+std::string jit_adjoint_source(const Pass& p, int R, int N, bool stage_params);
 int jit_launch_adjoint(CUfunction fn, const CUtensorMap* my, const CUtensorMap* md, const double2* tab, int64_t tstride,
                        int64_t tps, int64_t ntiles, unsigned* err, double* gpart, unsigned* gcount, double* gout,
                        const int* gslot, int threads, size_t shm, int grid, cudaStream_t st);

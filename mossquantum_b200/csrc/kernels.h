@@ -79,6 +79,7 @@ struct BindRec {
   int mat_off;        // offset of the ordered matrix in one sample's matrix table (double2)
   int gen_off;        // offset of the ordered generator, or -1
   int perm[8];        // ordered local index a' -> own-order local index (k <= 3)
+  int nopt;           // MB_FAM_SELECT: number of stored operators (ordered, after the matrix)
 };
 int launch_bind(const BindRec* recs_dev, int nrecs, const double* theta_dev, int nslots, int ntheta_rows,
                 double2* table, int64_t table_stride, cudaStream_t st);

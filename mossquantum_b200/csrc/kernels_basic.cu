@@ -452,6 +452,15 @@ __global__ void k_bind(const BindRec* __restrict__ recs, int nrecs, const double
   const int row = int(idx / nrecs), q = int(idx % nrecs);
   const BindRec rc = recs[q];
   const double t = rc.slot >= 0 ? theta[int64_t(row) * nslots + rc.slot] : rc.value;
+  if (rc.family == MB_FAM_SELECT) {
+    // Copy stored operator j (ordered form, kept in row 0 after the matrix) into this row.
+    const int d2 = 1 << (2 * rc.k);
+    const int j = min(max(int(llrint(t)), 0), rc.nopt - 1);
+    double2* out = table + int64_t(row) * stride + rc.mat_off;
+    const double2* src = table + rc.mat_off + int64_t(d2) * (1 + j);
+    for (int e = 0; e < d2; ++e) out[e] = src[e];
+    return;
+  }
   double2 m[64], g[64];
   family_matrix(rc.family, t, m, g);
   const int d = 1 << rc.k;

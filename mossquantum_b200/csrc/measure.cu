@@ -152,3 +152,20 @@ extern "C" int mb_remove_qubit(mb_state src, int qubit, const int* outcomes, con
   dev_free(d_sc);
   return rc;
 }
+
+extern "C" int mb_scale_samples(mb_state s, const double* scales) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (int rc = check_init()) return rc;
+  if (int rc = check_not_capturing("mb_scale_samples")) return rc;
+  if (!s || (!scales && s->batch)) return MB_EINVAL;
+  for (int b = 0; b < s->batch; ++b)
+    if (!std::isfinite(scales[b])) {
+      set_error("scales must be finite");
+      return MB_EINVAL;
+    }
+  for (int b = 0; b < s->batch; ++b)
+    if (scales[b] != 1.0)
+      if (int rc = launch_scale(s->d + int64_t(b) * s->elems, s->elems, scales[b], g_ctx.stream)) return rc;
+  MB_CHECK_CUDA(cudaStreamSynchronize(g_ctx.stream));
+  return MB_OK;
+}
