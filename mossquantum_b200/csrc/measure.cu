@@ -29,6 +29,15 @@ __global__ void k_remove_qubit(const double2* __restrict__ src, double2* __restr
   }
 }
 
+__global__ void k_scale_samples(double2* __restrict__ v, int64_t elems, int nsamples, const double* __restrict__ sc) {
+  const int64_t total = elems * nsamples;
+  for (int64_t g = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; g < total; g += int64_t(gridDim.x) * blockDim.x) {
+    const double s = sc[g / elems];
+    const double2 x = v[g];
+    v[g] = make_double2(x.x * s, x.y * s);
+  }
+}
+
 int check_qubit(mb_state s, int qubit) {
   if (!s) return MB_EINVAL;
   if (qubit < 0 || qubit >= s->n) {
@@ -163,9 +172,18 @@ extern "C" int mb_scale_samples(mb_state s, const double* scales) {
       set_error("scales must be finite");
       return MB_EINVAL;
     }
-  for (int b = 0; b < s->batch; ++b)
-    if (scales[b] != 1.0)
-      if (int rc = launch_scale(s->d + int64_t(b) * s->elems, s->elems, scales[b], g_ctx.stream)) return rc;
-  MB_CHECK_CUDA(cudaStreamSynchronize(g_ctx.stream));
-  return MB_OK;
+  if (s->batch == 0) return MB_OK;
+  double* d = nullptr;
+  int rc = dev_alloc((void**)&d, sizeof(double) * s->batch);
+  if (rc) return rc;
+  cudaStream_t st = g_ctx.stream;
+  cudaMemcpyAsync(d, scales, sizeof(double) * s->batch, cudaMemcpyHostToDevice, st);
+  k_scale_samples<<<grid_for(s->elems * s->batch, 256), 256, 0, st>>>(s->d, s->elems, s->batch, d);
+  ++launch_counter();
+  if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(st) != cudaSuccess) {
+    set_error("scaling samples failed");
+    rc = MB_EDEVICE;
+  }
+  dev_free(d);
+  return rc;
 }
