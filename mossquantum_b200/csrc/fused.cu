@@ -956,6 +956,16 @@ static bool want_jit(int N) {
   return N >= lo;
 }
 
+// CTAs per SM of a specialised tile pass: as many double-buffered tiles as shared memory holds
+// (the pass's matrix copy takes at most 32 KB more), capped at MB_TILE_CTAS (default 4). The
+// kernel's launch bounds ask the compiler to fit that many CTAs in the register file.
+static int tile_ctas(int t) {
+  const size_t shm = (size_t(32) << t) + 1024 + 32 * 1024;
+  int cap = 4;
+  if (const char* e = getenv("MB_TILE_CTAS")) cap = std::max(1, std::min(8, atoi(e)));
+  return std::max(1, std::min(cap, int((227 * 1024) / (shm + 256))));
+}
+
 static void prepare_jit(Schedule* S) {
   if (S->jit != 0) return;
   S->jit = -1;
@@ -966,8 +976,9 @@ static void prepare_jit(Schedule* S) {
   // staged in shared memory with the fixed ones.
   const bool single = S->nsamples == 1;
   for (Pass& p : S->passes) {
+    if (p.kind == PASS_TILE && !S->adjoint) p.ctas = tile_ctas(p.t);
     if (p.kind == PASS_TILE && S->adjoint) src.push_back(jit_adjoint_source(p, S->R, S->N, single));
-    else if (p.kind == PASS_TILE) src.push_back(jit_tile_source(p, S->R, S->N, single));
+    else if (p.kind == PASS_TILE) src.push_back(jit_tile_source(p, S->R, S->N, single, p.ctas));
     else if (p.kind == PASS_REG) src.push_back(jit_reg_source(p, S->N, single));
     else continue;
     who.push_back(&p);
@@ -975,16 +986,31 @@ static void prepare_jit(Schedule* S) {
   std::vector<CUfunction> fns;
   std::string err;
   // Passes whose kernels do not compile within the budget (MB_JIT_BUDGET_S seconds per
-  // schedule, default 30) run on the interpreter kernels, which exist for R = 4 and 5; the
-  // adjoint and R = 3 schedules need every specialised kernel.
+  // schedule, default 30), and passes whose generated source exceeds MB_JIT_MAX_SOURCE_KB
+  // (default 256 KB; NVRTC time grows faster than the source, about 17 s at 240 KB), run on the
+  // interpreter kernels, which exist for R = 4 and 5; the adjoint and R = 3 schedules need
+  // every specialised kernel.
   double budget = 30.0;
   if (const char* e = getenv("MB_JIT_BUDGET_S")) budget = atof(e);
+  size_t max_src = size_t(256) << 10;
+  if (const char* e = getenv("MB_JIT_MAX_SOURCE_KB")) max_src = size_t(std::max(1, atoi(e))) << 10;
   const bool partial_ok = !S->adjoint && (S->R == 4 || S->R == 5);
-  if (jit_prepare(src, fns, &err, partial_ok ? budget : 0.0) != MB_OK) {
+  std::vector<std::string> small;
+  std::vector<Pass*> small_who;
+  for (size_t i = 0; i < src.size(); ++i) {
+    if (src[i].size() <= max_src) {
+      small.push_back(std::move(src[i]));
+      small_who.push_back(who[i]);
+    } else if (!partial_ok) {
+      if (getenv("MB_JIT_VERBOSE")) fprintf(stderr, "mossb200: JIT disabled: a pass source has %zu bytes\n", src[i].size());
+      return;
+    }
+  }
+  if (jit_prepare(small, fns, &err, partial_ok ? budget : 0.0) != MB_OK) {
     if (getenv("MB_JIT_VERBOSE")) fprintf(stderr, "mossb200: JIT disabled for this schedule: %s\n", err.c_str());
     return;
   }
-  for (size_t i = 0; i < who.size(); ++i) who[i]->jit_fn = fns[i];
+  for (size_t i = 0; i < small_who.size(); ++i) small_who[i]->jit_fn = fns[i];
   S->jit = 1;
 }
 
@@ -1023,7 +1049,8 @@ int run_schedule(mb_circuit c, Schedule* S, double2* v, int nsamples, int64_t ms
       const int threads = 1 << (p.t - S->R);
       const size_t shm = (size_t(32) << p.t) + 1024;  // two tile buffers + alignment slack
       const int per_sm = std::max(1, int((227 * 1024) / (shm + 256)));
-      const int64_t grid = std::min<int64_t>(a.ntiles, int64_t(g_ctx.sm_count) * std::min(per_sm, 4));
+      int64_t grid = std::min<int64_t>(a.ntiles, int64_t(g_ctx.sm_count) * std::min(per_sm, 4));
+      if (S->jit == 1 && p.jit_fn && p.ctas > 0) grid = std::min<int64_t>(a.ntiles, int64_t(g_ctx.sm_count) * p.ctas);
       if (S->jit == 1 && p.jit_fn) {
         ProfScope ps("k_tile_pass_jit", 32.0 * double(elems) * nsamples, st,
                      pass_flops_per_amp(p, false) * double(elems) * nsamples);

@@ -60,6 +60,7 @@ struct Pass {
   int plain_fop = -1;           // PASS_PLAIN: index into the schedule's fused ops
   bool has_u2 = false;          // holds a 4x4 micro-op (selects the kernel variant)
   void* jit_fn = nullptr;       // specialised kernel (CUfunction) when the JIT is in use
+  int ctas = 0;                 // specialised tile kernels: CTAs per SM they were compiled for
   std::vector<int> grad_slots;  // adjoint passes: parameter slot of each gradient accumulator
   int grad_off = 0;             // offset of grad_slots in the schedule's device slot array
   TmaGeom geom{};

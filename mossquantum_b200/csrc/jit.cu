@@ -421,14 +421,15 @@ static std::string shared_mats_fill(const SharedMats& sm) {
   return o.str();
 }
 
-std::string jit_tile_source(const Pass& p, int R, int N, bool stage_params) {
+std::string jit_tile_source(const Pass& p, int R, int N, bool stage_params, int ctas) {
   std::ostringstream o;
   const int A = 1 << R;
   const int threads = 1 << (p.t - R);
   const TmaGeom& g = p.geom;
   const SharedMats smats = shared_mats(p, stage_params);
   o << kPrelude << shared_mats_decl(smats);
-  o << "extern \"C\" __global__ void __launch_bounds__(" << threads << ", 1) mbk(const __grid_constant__ TMap tmap, "
+  o << "extern \"C\" __global__ void __launch_bounds__(" << threads << ", " << std::max(1, ctas)
+    << ") mbk(const __grid_constant__ TMap tmap, "
     << "const double2* __restrict__ tab, long long tstride, long long tps, long long ntiles, u32* err) {\n";
   o << "  extern __shared__ unsigned char smem_raw[];\n  __shared__ __align__(8) u64 bar[2];\n  __shared__ int s_abort;\n";
   o << shared_mats_fill(smats);

@@ -9,7 +9,8 @@
 
 namespace mb {
 bool jit_available();
-std::string jit_tile_source(const Pass& p, int R, int N, bool stage_params);
+// ctas: CTAs per SM the kernel is compiled for (its launch bounds; the launch uses the same).
+std::string jit_tile_source(const Pass& p, int R, int N, bool stage_params, int ctas = 1);
 std::string jit_reg_source(const Pass& p, int N, bool stage_params);
 // Compiles every source (in parallel, cached by text); fills out[i] or fails with err. With a
 // positive budget (seconds) sources not started within it are skipped (out[i] = nullptr) and
