@@ -989,12 +989,13 @@ static void prepare_jit(Schedule* S) {
   // schedule, default 30), and passes whose generated source exceeds MB_JIT_MAX_SOURCE_KB
   // (default 256 KB; NVRTC time grows faster than the source, about 17 s at 240 KB), run on the
   // interpreter kernels, which exist for R = 4 and 5; the adjoint and R = 3 schedules need
-  // every specialised kernel.
+  // every specialised kernel (their size limit is four times larger).
   double budget = 30.0;
   if (const char* e = getenv("MB_JIT_BUDGET_S")) budget = atof(e);
   size_t max_src = size_t(256) << 10;
   if (const char* e = getenv("MB_JIT_MAX_SOURCE_KB")) max_src = size_t(std::max(1, atoi(e))) << 10;
   const bool partial_ok = !S->adjoint && (S->R == 4 || S->R == 5);
+  if (!partial_ok) max_src *= 4;  // no interpreter to fall back on: only refuse the extreme ones
   std::vector<std::string> small;
   std::vector<Pass*> small_who;
   for (size_t i = 0; i < src.size(); ++i) {
