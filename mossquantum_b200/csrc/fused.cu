@@ -957,10 +957,11 @@ static bool want_jit(int N) {
 }
 
 // CTAs per SM of a specialised tile pass: as many double-buffered tiles as shared memory holds
-// (the pass's matrix copy takes at most 32 KB more), capped at MB_TILE_CTAS (default 4). The
-// kernel's launch bounds ask the compiler to fit that many CTAs in the register file.
+// (allowing 4 KB for the pass's matrix copy; a larger copy only lowers the resident count),
+// capped at MB_TILE_CTAS (default 4). The kernel's launch bounds ask the compiler to fit that
+// many CTAs in the register file.
 static int tile_ctas(int t) {
-  const size_t shm = (size_t(32) << t) + 1024 + 32 * 1024;
+  const size_t shm = (size_t(32) << t) + 1024 + 4 * 1024;
   int cap = 4;
   if (const char* e = getenv("MB_TILE_CTAS")) cap = std::max(1, std::min(8, atoi(e)));
   return std::max(1, std::min(cap, int((227 * 1024) / (shm + 256))));
