@@ -223,9 +223,9 @@ def batch_workload(args):
     dm_groups = {10: (W.hea_circuit(10, depth, noise=(0.01, 0.02)), 64)}
     t0 = time.perf_counter()
     log("building the pure-state plan")
-    plan = BatchPlan(groups, W.xxz)
+    plan = BatchPlan(groups, W.xxz, autotune=True)
     log(f"pure plan ready after {time.perf_counter() - t0:.1f} s; building the density plan")
-    plan_dm = BatchPlan(dm_groups, W.xxz, kind="density")
+    plan_dm = BatchPlan(dm_groups, W.xxz, kind="density", autotune=True)
     prep_s = time.perf_counter() - t0
     log(f"plans ready after {prep_s:.1f} s")
     def thetas(gr, seed):
@@ -278,7 +278,8 @@ def batch_workload(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "complex128 (f64)",
             "data": "synthetic (seeded)",
             "config": {"workload": "512 pure (n=10..22, HEA depth 8) + 64 density (n=10, noisy) <XXZ>",
-                       "sizes": counts, "plan_build_s": prep_s},
+                       "sizes": counts, "plan_build_s": prep_s,
+                       "autotuned": {str(k): list(v) for k, v in {**plan.tuned, **plan_dm.tuned}.items()}},
             "plain_per_call": {"value": evals / plain_total, "unit": "evals/s", "seconds_per_batch": plain_total,
                                "sample": f"{nsub} pure samples + 2 density samples timed, weighted by the size mix"},
             "speedup_vs_plain": plain_total / (ms_step / 1e3),

@@ -25,8 +25,9 @@ class BatchPlan:
     """groups: {n: (template circuit for n qubits, samples B_n)}; observable_for(n) gives the
     observable evaluated on every sample of size n. kind: "pure" or "density"."""
 
-    def __init__(self, groups, observable_for, kind="pure"):
+    def __init__(self, groups, observable_for, kind="pure", autotune=False, autotune_max_bits=17):
         self.kind = kind
+        self.tuned = {}
         self.groups = []
         total = 0
         for n in sorted(groups):
@@ -44,6 +45,16 @@ class BatchPlan:
         N.check(N.lib().mb_buffer_alloc(16 * max(1, total), ctypes.byref(buf)), "mb_buffer_alloc")
         self.results = buf
         self.graph = None
+        if autotune:
+            # Tile and register widths per register size, timed on each group's own batch;
+            # sizes above autotune_max_bits keep the defaults (their candidates would each
+            # need specialised kernels compiled first).
+            from .autotune import autotune as tune
+            for g in self.groups:
+                bits = 2 * g["n"] if kind == "density" else g["n"]
+                if 8 <= bits <= autotune_max_bits:
+                    th = np.zeros((g["B"], g["circuit"].nparameters()))
+                    self.tuned[bits] = tune(g["circuit"], g["state"], th)
         # Eager warm-up with zero parameters: builds schedules, kernels and reduction plans.
         self._stage({g["n"]: np.zeros((g["B"], g["circuit"].nparameters())) for g in self.groups})
         self._record_body()
