@@ -842,8 +842,26 @@ struct Tuning {
 std::mutex g_tune_mu;
 std::map<int, std::pair<int, int>> g_tuning;  // register bits -> (tile bits, register bits)
 
+// Specialised kernels are used from MB_JIT_MIN_BITS register bits on (default 18); MB_JIT=0
+// disables them. Small states keep the interpreter kernels (no compile latency).
+static bool want_jit(int N) {
+  const char* e = getenv("MB_JIT");
+  if (e && atoi(e) == 0) return false;
+  int lo = 18;
+  if (const char* m = getenv("MB_JIT_MIN_BITS")) lo = atoi(m);
+  return N >= lo;
+}
+
+// Defaults: sizes run by the specialised kernels use 2^11-amplitude tiles with 8 amplitudes per
+// thread and two CTAs per SM (the fastest point of a sweep over tile bits 10-12, register bits
+// 3-4 and 1-6 CTAs per SM on the 28-qubit U3 circuit); the interpreter kernels use 2^12 tiles
+// with 16 amplitudes per thread. mb_tuning_set / the autotuner override both per register size.
 static Tuning tuning_for(int N) {
   Tuning tu;
+  if (want_jit(N) && jit_available()) {
+    tu.t = 11;
+    tu.R = 3;
+  }
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tuning.find(N);
@@ -860,11 +878,16 @@ static Tuning tuning_for(int N) {
 
 }  // namespace
 
+static void prepare_jit(Schedule* S);
+
 int get_schedule_ex(mb_circuit c, int n, int dm, int adjoint, int lo, int hi, int nsamples, Schedule** out) {
   const int N = dm ? 2 * n : n;
   if (hi < 0) hi = int(c->ops.size());
   Tuning tu = tuning_for(N);
-  if (adjoint) tu.t = std::min(tu.t, 11);  // y and delta tiles, double-buffered
+  if (adjoint) {
+    tu.t = std::min(tu.t, 11);  // y and delta tiles, double-buffered
+    if (!getenv("MB_REG_BITS")) tu.R = 4;
+  }
   for (Schedule* s : c->scheds)
     if (s->N == N && s->dm == dm && !s->dagger && s->t == tu.t && s->R == tu.R && s->nsamples == nsamples &&
         s->lo == lo && s->hi == hi && s->adjoint == adjoint) {
@@ -936,6 +959,22 @@ int get_schedule_ex(mb_circuit c, int n, int dm, int adjoint, int lo, int hi, in
     MB_CHECK_CUDA(cudaMemcpyAsync(S->d_gslots, gs.data(), sizeof(int) * gs.size(), cudaMemcpyHostToDevice, g_ctx.stream));
   }
   MB_CHECK_CUDA(cudaStreamSynchronize(g_ctx.stream));
+  if (!adjoint && S->R == 3) {
+    // Register width 3 exists only as specialised kernels: if they cannot all be built (source
+    // limits, compile budget), use width 4 for this register size from now on.
+    prepare_jit(S.get());
+    if (S->jit != 1) {
+      if (getenv("MB_JIT_VERBOSE")) fprintf(stderr, "mossb200: %d-bit schedules fall back to register width 4\n", N);
+      {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tuning[N] = {S->t, 4};
+      }
+      dev_free(S->d_stages);
+      dev_free(S->d_mops);
+      dev_free(S->d_gslots);
+      return get_schedule_ex(c, n, dm, adjoint, lo, hi, nsamples, out);
+    }
+  }
   *out = S.get();
   c->scheds.push_back(S.release());
   return MB_OK;
@@ -946,23 +985,14 @@ int get_schedule(mb_circuit c, int n, int dm, bool dagger, int nsamples, Schedul
   return get_schedule_ex(c, n, dm, 0, 0, -1, nsamples, out);
 }
 
-// Specialised kernels are used from MB_JIT_MIN_BITS register bits on (default 18); MB_JIT=0
-// disables them. Small states keep the interpreter kernels (no compile latency).
-static bool want_jit(int N) {
-  const char* e = getenv("MB_JIT");
-  if (e && atoi(e) == 0) return false;
-  int lo = 18;
-  if (const char* m = getenv("MB_JIT_MIN_BITS")) lo = atoi(m);
-  return N >= lo;
-}
 
 // CTAs per SM of a specialised tile pass: as many double-buffered tiles as shared memory holds
 // (allowing 4 KB for the pass's matrix copy; a larger copy only lowers the resident count),
-// capped at MB_TILE_CTAS (default 4). The kernel's launch bounds ask the compiler to fit that
+// capped at MB_TILE_CTAS (default 2). The kernel's launch bounds ask the compiler to fit that
 // many CTAs in the register file.
 static int tile_ctas(int t) {
   const size_t shm = (size_t(32) << t) + 1024 + 4 * 1024;
-  int cap = 4;
+  int cap = 2;
   if (const char* e = getenv("MB_TILE_CTAS")) cap = std::max(1, std::min(8, atoi(e)));
   return std::max(1, std::min(cap, int((227 * 1024) / (shm + 256))));
 }
@@ -988,15 +1018,16 @@ static void prepare_jit(Schedule* S) {
   std::string err;
   // Passes whose kernels do not compile within the budget (MB_JIT_BUDGET_S seconds per
   // schedule, default 30), and passes whose generated source exceeds MB_JIT_MAX_SOURCE_KB
-  // (default 256 KB; NVRTC time grows faster than the source, about 17 s at 240 KB), run on the
+  // (default 128 KB; NVRTC time grows faster than the source: 3 s at 97 KB, 17 s at 238 KB), run on the
   // interpreter kernels, which exist for R = 4 and 5; the adjoint and R = 3 schedules need
-  // every specialised kernel (their size limit is four times larger).
+  // every specialised kernel (an R = 3 schedule that cannot have them is rebuilt with R = 4;
+  // the adjoint's size limit is four times larger).
   double budget = 30.0;
   if (const char* e = getenv("MB_JIT_BUDGET_S")) budget = atof(e);
-  size_t max_src = size_t(256) << 10;
+  size_t max_src = size_t(128) << 10;
   if (const char* e = getenv("MB_JIT_MAX_SOURCE_KB")) max_src = size_t(std::max(1, atoi(e))) << 10;
   const bool partial_ok = !S->adjoint && (S->R == 4 || S->R == 5);
-  if (!partial_ok) max_src *= 4;  // no interpreter to fall back on: only refuse the extreme ones
+  if (S->adjoint) max_src *= 4;  // no interpreter to fall back on: only refuse the extreme ones
   std::vector<std::string> small;
   std::vector<Pass*> small_who;
   for (size_t i = 0; i < src.size(); ++i) {

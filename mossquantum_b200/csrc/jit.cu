@@ -326,6 +326,10 @@ CUfunction compile_kernel(const std::string& src, std::string* err) {
   const char* opts[] = {"--gpu-architecture=sm_100a", "-std=c++17", "--fmad=true", "-default-device"};
   const auto t0 = std::chrono::steady_clock::now();
   const int rc = n.compile(prog, 4, opts);
+  if (getenv("MB_JIT_VERBOSE")) {
+    const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    fprintf(stderr, "mossb200: compiled a %zu-byte pass in %.2f s\n", src.size(), sec);
+  }
   if (const char* dir = getenv("MB_JIT_DUMP")) {
     // Development aid: every compiled source and its compile time.
     const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
