@@ -11,6 +11,10 @@
 // ascending order, onto the k target bits and the 6 lowest group bits, so a warp's 32
 // consecutive e are 32 consecutive amplitudes (512 contiguous bytes) for any target set.
 // Only the FP64 tensor pipe does arithmetic: 8 * 2^k flop per amplitude.
+// Shared-memory layout of X (and Y): row r of 2D rows, column g of 64, at
+// r * 72 + (g ^ ((r >> 2) & 7)). The stride (8 mod 16 doubles) spreads the four rows of a
+// B fragment over both bank halves; the XOR, constant within each fragment's rows, spreads a
+// staging access whose 32 lanes hold 32 rows of one column over all banks.
 #include <algorithm>
 
 #include "kernels.h"
@@ -39,12 +43,14 @@ __device__ __forceinline__ void dmma_m8n8k4(double& d0, double& d1, double a, do
                : "d"(a), "d"(b));
 }
 
+constexpr int kXS = kGT + 8;
+__device__ __forceinline__ int xsw(int r, int g) { return r * kXS + (g ^ ((r >> 2) & 7)); }
+
 template <int K>
 __global__ void __launch_bounds__(kDThreads) k_dmma_block(double2* __restrict__ v, const DmmaArgs a,
                                                           const double2* __restrict__ m, int mode) {
   constexpr int D = 1 << K, M2 = 2 * D;
   constexpr int AS = M2 + 4;            // padded row strides (doubles): conflict-free fragments
-  constexpr int XS = kGT + 8;
   constexpr int MT = M2 / 8;            // 8-row output tiles
   constexpr int WPM = 8 / MT;           // warps per output tile
   constexpr int NT = (kGT / 8) / WPM;   // 8-column output tiles per warp
@@ -70,18 +76,19 @@ __global__ void __launch_bounds__(kDThreads) k_dmma_block(double2* __restrict__ 
       else t_g |= 1 << a.egrp[j];
     }
   int64_t i_addr[PER];
-  int i_a[PER], i_g[PER];
+  int i_re[PER], i_im[PER];   // swizzled shared-memory slots of the element's real / imaginary part
 #pragma unroll
   for (int i = 0; i < PER; ++i) {
     i_addr[i] = t_addr;
-    i_a[i] = t_a;
-    i_g[i] = t_g;
+    int ia = t_a, ig = t_g;
     for (int j = 8; j < a.ebits; ++j)
       if ((i >> (j - 8)) & 1) {
         i_addr[i] |= int64_t(1) << a.eaddr[j];
-        if (a.etgt[j] >= 0) i_a[i] |= 1 << a.etgt[j];
-        else i_g[i] |= 1 << a.egrp[j];
+        if (a.etgt[j] >= 0) ia |= 1 << a.etgt[j];
+        else ig |= 1 << a.egrp[j];
       }
+    i_re[i] = xsw(ia, ig);
+    i_im[i] = xsw(D + ia, ig);
   }
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -101,8 +108,8 @@ __global__ void __launch_bounds__(kDThreads) k_dmma_block(double2* __restrict__ 
     for (int i = 0; i < PER; ++i) x[i] = v[base | i_addr[i]];
 #pragma unroll
     for (int i = 0; i < PER; ++i) {
-      Xs[i_a[i] * XS + i_g[i]] = x[i].x;
-      Xs[(D + i_a[i]) * XS + i_g[i]] = x[i].y;
+      Xs[i_re[i]] = x[i].x;
+      Xs[i_im[i]] = x[i].y;
     }
     __syncthreads();
     double acc[NT][2];
@@ -110,19 +117,22 @@ __global__ void __launch_bounds__(kDThreads) k_dmma_block(double2* __restrict__ 
     for (int j = 0; j < NT; ++j) acc[j][0] = acc[j][1] = 0.0;
 #pragma unroll
     for (int ks = 0; ks < M2 / 4; ++ks) {
-      const double* xr = Xs + (ks * 4 + (lane & 3)) * XS + nt0 * 8 + (lane >> 2);
+      // rows ks*4 .. ks*4+3 share the swizzle (ks & 7)
+      const double* xr = Xs + (ks * 4 + (lane & 3)) * kXS;
+      const int c0 = nt0 * 8 + (lane >> 2);
 #pragma unroll
-      for (int j = 0; j < NT; ++j) dmma_m8n8k4(acc[j][0], acc[j][1], afr[ks], xr[j * 8]);
+      for (int j = 0; j < NT; ++j) dmma_m8n8k4(acc[j][0], acc[j][1], afr[ks], xr[(c0 + j * 8) ^ (ks & 7)]);
     }
     __syncthreads();
 #pragma unroll
-    for (int j = 0; j < NT; ++j)
-      *reinterpret_cast<double2*>(Xs + (mt * 8 + (lane >> 2)) * XS + (nt0 + j) * 8 + (lane & 3) * 2) =
-          make_double2(acc[j][0], acc[j][1]);
+    for (int j = 0; j < NT; ++j) {
+      const int r = mt * 8 + (lane >> 2), c = (nt0 + j) * 8 + (lane & 3) * 2;
+      Xs[xsw(r, c)] = acc[j][0];
+      Xs[xsw(r, c + 1)] = acc[j][1];
+    }
     __syncthreads();
 #pragma unroll
-    for (int i = 0; i < PER; ++i)
-      v[base | i_addr[i]] = make_double2(Xs[i_a[i] * XS + i_g[i]], Xs[(D + i_a[i]) * XS + i_g[i]]);
+    for (int i = 0; i < PER; ++i) v[base | i_addr[i]] = make_double2(Xs[i_re[i]], Xs[i_im[i]]);
     __syncthreads();
   }
 }
