@@ -959,9 +959,10 @@ int get_schedule_ex(mb_circuit c, int n, int dm, int adjoint, int lo, int hi, in
     MB_CHECK_CUDA(cudaMemcpyAsync(S->d_gslots, gs.data(), sizeof(int) * gs.size(), cudaMemcpyHostToDevice, g_ctx.stream));
   }
   MB_CHECK_CUDA(cudaStreamSynchronize(g_ctx.stream));
-  if (!adjoint && S->R == 3) {
+  if (!adjoint && S->R == 3 && !getenv("MB_REG_BITS")) {
     // Register width 3 exists only as specialised kernels: if they cannot all be built (source
-    // limits, compile budget), use width 4 for this register size from now on.
+    // limits, compile budget), use width 4 for this register size from now on. (A width forced
+    // through MB_REG_BITS is kept; run_schedule then reports the missing kernels.)
     prepare_jit(S.get());
     if (S->jit != 1) {
       if (getenv("MB_JIT_VERBOSE")) fprintf(stderr, "mossb200: %d-bit schedules fall back to register width 4\n", N);
