@@ -886,7 +886,8 @@ int get_schedule_ex(mb_circuit c, int n, int dm, int adjoint, int lo, int hi, in
   Tuning tu = tuning_for(N);
   if (adjoint) {
     tu.t = std::min(tu.t, 11);  // y and delta tiles, double-buffered
-    if (!getenv("MB_REG_BITS")) tu.R = 4;
+    tu.R = 4;                   // register width of the dual-state passes (MB_ADJOINT_REG_BITS: 3..4)
+    if (const char* e = getenv("MB_ADJOINT_REG_BITS")) tu.R = std::max(3, std::min(4, atoi(e)));
   }
   for (Schedule* s : c->scheds)
     if (s->N == N && s->dm == dm && !s->dagger && s->t == tu.t && s->R == tu.R && s->nsamples == nsamples &&
