@@ -540,15 +540,13 @@ def main():
         end.record(stream)
         end.synchronize()
     launches = N.launch_count() - l0
-    ms = start.elapsed_time(end)
+    from mossquantum_b200 import replicas
+    ms = replicas.max_over_ranks(start.elapsed_time(end), device=f"cuda:{local}")   # slowest replica
     if world > 1:
-        t = torch.tensor([ms], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
         dist.barrier()
     ms_step = ms / args.steps
     bytes_step = plain_bytes(n, depth)
-    value = world * bytes_step / (ms_step / 1e3) / 1e9
+    value = replicas.aggregate_rate(bytes_step, world, ms_step / 1e3) / 1e9
 
     roofline = dominant_roofline(N, step, f"n{n}")
 
