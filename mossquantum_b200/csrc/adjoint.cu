@@ -99,12 +99,10 @@ void dm_reverse_plan(mb_circuit c, int* seg_len, int* nscratch) {
   *nscratch = 1 + (nseg - 1) + maxch;
 }
 
-// Forward application of instructions [lo, hi) of c on one density matrix (fused passes when
-// available, plain otherwise).
+// Forward application of instructions [lo, hi) of c on one density matrix with the plain
+// kernels: the segments are about sqrt(k) instructions long, and a fused schedule (with its
+// specialised kernels) per distinct segment would cost more to build than it saves.
 static int forward_range_dm(mb_circuit c, int n, int lo, int hi, double2* z) {
-  if (lo >= hi) return MB_OK;
-  Schedule* S = nullptr;
-  if (2 * n >= 8 && get_schedule_ex(c, n, 1, 0, lo, hi, 1, &S) == MB_OK) return run_schedule(c, S, z, 1, 0);
   for (int i = lo; i < hi; ++i)
     if (int rc = plain_op(c, c->ops[i], z, n, 1, 1, 0, false)) return rc;
   return MB_OK;

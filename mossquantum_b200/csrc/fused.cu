@@ -196,6 +196,7 @@ struct Schedule {
   int max_grad = 0;     // most gradient accumulators in one pass
   int jit = 0;  // 0 not tried, 1 specialised kernels ready, -1 interpreter kernels
   bool dagger = false;
+  bool unschedulable = false;  // an adjoint op that no pass can hold
   std::vector<FOp> fops;
   std::vector<Pass> passes;
   StageDesc* d_stages = nullptr;
@@ -736,6 +737,22 @@ static void build_schedule(Schedule& S, int nsamples, bool allow_reg = true) {
         }
         const int rlo = std::max(5, std::min(h0, N - R));
         if (allow_reg && N - 5 >= R) cands.push_back({PASS_REG, window(rlo, R, N)});
+        if (S.dm) {
+          // Paired windows for density matrices: row bits [a, a+w1) and the matching column
+          // bits [b, b+w2) (b = a + n), so a channel's supermatrix on (q, q+n) and both halves
+          // of a gate fit one tile even when n exceeds a single window.
+          const int nq = N / 2, w1 = (t - 3) / 2, w2 = t - 3 - w1, q0 = h0 % nq;
+          if (nq - w1 >= 3) {
+            for (int a : {q0, q0 - w1 / 2}) {
+              a = std::max(3, std::min(a, nq - w1));
+              int b = std::max(nq, std::min((q0 < 3 ? 0 : a) + nq, N - w2));
+              std::vector<int> bb = {0, 1, 2};
+              for (int q : window(a, w1, N)) bb.push_back(q);
+              for (int q : window(b, w2, N)) bb.push_back(q);
+              cands.push_back({PASS_TILE, bb});
+            }
+          }
+        }
       }
     }
     double best = -1;
@@ -754,6 +771,21 @@ static void build_schedule(Schedule& S, int nsamples, bool allow_reg = true) {
         best_taken = tk;
         bg = g;
       }
+    }
+    if (bi < 0 || best_taken.empty()) {
+      // No candidate holds the first op (its bits lie farther apart than any window): run it
+      // by itself with the plain kernel, which always makes progress. The adjoint has no
+      // plain form of its gradient ops, so its schedule is refused instead.
+      if (S.adjoint) {
+        S.unschedulable = true;
+        return;
+      }
+      Pass p;
+      p.kind = PASS_PLAIN;
+      p.plain_fop = rem[0];
+      S.passes.push_back(p);
+      rem.erase(rem.begin());
+      continue;
     }
     Pass p;
     p.kind = cands[bi].kind;
@@ -917,6 +949,10 @@ int get_schedule_ex(mb_circuit c, int n, int dm, int adjoint, int lo, int hi, in
     build_fops(c, n, dm, false, S->fops, lo, hi);
   }
   build_schedule(*S, nsamples, !adjoint);
+  if (S->unschedulable) {
+    set_error("the fused adjoint cannot place an instruction whose qubits are farther apart than a tile");
+    return MB_EUNSUPPORTED;
+  }
   // Every register op must name register bits inside the stage width.
   for (const Pass& p : S->passes) {
     const int R = p.kind == PASS_REG ? p.t : S->R;
