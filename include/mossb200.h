@@ -166,6 +166,12 @@ MB_API int mb_circuit_free(mb_circuit c);
 MB_API int mb_circuit_nslots(mb_circuit c, int* nslots);
 /* Number of fused passes the fused schedule uses on an n-qubit pure state. */
 MB_API int mb_circuit_passes(mb_circuit c, int* npasses);
+/* Host-only schedule of an instruction list (needs no device and no mb_init): the number of
+ * passes (tile, register and plain) the fused scheduler makes for an n-qubit pure state
+ * (dm = 0) or density matrix (dm = 1) with the given tile and register bits, and whether every
+ * fused operation landed in exactly one pass. For tests and capacity planning. */
+MB_API int mb_schedule_info(const mb_op* ops, size_t nops, int n, int dm, int tile_bits, int reg_bits, int nsamples,
+                            int* npasses, int* ntile, int* nreg, int* nplain, int* complete);
 /* apply!(circuit, state) (execution/gates.jl:21-36, batch_gates.jl, channels.jl).
  * theta: host array of nslots values (or B*nslots with MB_APPLY_PER_SAMPLE).
  * A circuit with channels requires a density kind (pure states must be promoted first,

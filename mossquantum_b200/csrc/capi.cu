@@ -366,17 +366,12 @@ extern "C" int mb_state_to_density(mb_state src, mb_state dst) {
 // =============================================================================================
 // Circuits
 // =============================================================================================
-extern "C" int mb_circuit_create(const mb_op* ops, size_t nops, int n, mb_circuit* out) {
-  std::lock_guard<std::recursive_mutex> lk(g_mu);
-  if (int rc = check_init()) return rc;
-  if (int rc = check_not_capturing("mb_circuit_create")) return rc;
-  if (!out || (!ops && nops)) return MB_EINVAL;
-  if (n < 0 || n > 32) {
-    set_error("register size %d out of range", n);
-    return MB_EINVAL;
-  }
-  std::unique_ptr<mb_circuit_s> c(new mb_circuit_s());
-  c->uid = next_circuit_uid();
+namespace mb {
+
+// Host half of mb_circuit_create: ordered instructions, the matrix table of one parameter row
+// (fixed matrices, channel supermatrices, room for bound parametric matrices and generators)
+// and the bind records. Touches no device memory.
+int circuit_compile_host(const mb_op* ops, size_t nops, int n, mb_circuit c) {
   c->n = n;
   int64_t off = 0;
   std::vector<double2> table;
@@ -581,17 +576,41 @@ extern "C" int mb_circuit_create(const mb_op* ops, size_t nops, int n, mb_circui
   c->table_elems = std::max<int64_t>(off, 1);
   c->fixed_table = table;
   c->fixed_table.resize(c->table_elems, cz());
-  int rc;
-  if ((rc = dev_alloc((void**)&c->d_table, sizeof(double2) * c->table_elems))) return rc;
-  c->table_rows = 1;
-  MB_CHECK_CUDA(cudaMemcpyAsync(c->d_table, c->fixed_table.data(), sizeof(double2) * c->table_elems,
-                                cudaMemcpyHostToDevice, g_ctx.stream));
-  if (!c->binds.empty()) {
-    if ((rc = dev_alloc((void**)&c->d_binds, sizeof(BindRec) * c->binds.size()))) return rc;
-    MB_CHECK_CUDA(cudaMemcpyAsync(c->d_binds, c->binds.data(), sizeof(BindRec) * c->binds.size(),
-                                  cudaMemcpyHostToDevice, g_ctx.stream));
+  return MB_OK;
+}
+
+}  // namespace mb
+
+extern "C" int mb_circuit_create(const mb_op* ops, size_t nops, int n, mb_circuit* out) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (int rc = check_init()) return rc;
+  if (int rc = check_not_capturing("mb_circuit_create")) return rc;
+  if (!out || (!ops && nops)) return MB_EINVAL;
+  if (n < 0 || n > 32) {
+    set_error("register size %d out of range", n);
+    return MB_EINVAL;
   }
-  MB_CHECK_CUDA(cudaStreamSynchronize(g_ctx.stream));
+  std::unique_ptr<mb_circuit_s> c(new mb_circuit_s());
+  c->uid = next_circuit_uid();
+  if (int rc = circuit_compile_host(ops, nops, n, c.get())) return rc;
+  int rc = dev_alloc((void**)&c->d_table, sizeof(double2) * c->table_elems);
+  if (!rc && !c->binds.empty()) rc = dev_alloc((void**)&c->d_binds, sizeof(BindRec) * c->binds.size());
+  if (rc) {
+    circuit_release(c.release());
+    return rc;
+  }
+  c->table_rows = 1;
+  cudaError_t e = cudaMemcpyAsync(c->d_table, c->fixed_table.data(), sizeof(double2) * c->table_elems,
+                                  cudaMemcpyHostToDevice, g_ctx.stream);
+  if (e == cudaSuccess && !c->binds.empty())
+    e = cudaMemcpyAsync(c->d_binds, c->binds.data(), sizeof(BindRec) * c->binds.size(), cudaMemcpyHostToDevice,
+                        g_ctx.stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g_ctx.stream);
+  if (e != cudaSuccess) {
+    set_error("circuit upload failed: %s", cudaGetErrorString(e));
+    circuit_release(c.release());
+    return MB_EDEVICE;
+  }
   *out = c.release();
   return MB_OK;
 }

@@ -1297,3 +1297,40 @@ extern "C" int mb_tuning_get(int nbits, int* tile_bits, int* reg_bits) {
   *reg_bits = tu.R;
   return MB_OK;
 }
+
+// Host-only view of the fused schedule (no device, no mb_init): builds the circuit's
+// instructions and the pass schedule for the given shape and reports its passes. `complete` is
+// 1 when every fused op landed in exactly one pass.
+extern "C" int mb_schedule_info(const mb_op* ops, size_t nops, int n, int dm, int tile_bits, int reg_bits,
+                                int nsamples, int* npasses, int* ntile, int* nreg, int* nplain, int* complete) {
+  if ((!ops && nops) || !npasses || !ntile || !nreg || !nplain || !complete) return MB_EINVAL;
+  const int N = dm ? 2 * n : n;
+  if (n < 1 || N > 40 || tile_bits < 8 || tile_bits > 12 || reg_bits < 3 || reg_bits > 5 || nsamples < 1) {
+    mb::set_error("schedule info: n, tile bits (8..12) or register bits (3..5) out of range");
+    return MB_EINVAL;
+  }
+  mb_circuit_s c;
+  if (int rc = mb::circuit_compile_host(ops, nops, n, &c)) return rc;
+  mb::Schedule S;
+  S.N = N;
+  S.dm = dm ? 1 : 0;
+  S.t = std::min(tile_bits, N);
+  S.R = reg_bits;
+  S.nsamples = nsamples;
+  mb::build_fops(&c, n, S.dm, false, S.fops);
+  mb::build_schedule(S, nsamples);
+  int t = 0, r = 0, p = 0;
+  size_t covered = 0;
+  for (const mb::Pass& ps : S.passes) {
+    if (ps.kind == mb::PASS_TILE) ++t;
+    else if (ps.kind == mb::PASS_REG) ++r;
+    else ++p;
+    covered += ps.kind == mb::PASS_PLAIN ? 1 : ps.mops.size();
+  }
+  *npasses = int(S.passes.size());
+  *ntile = t;
+  *nreg = r;
+  *nplain = p;
+  *complete = covered == S.fops.size() ? 1 : 0;
+  return MB_OK;
+}

@@ -119,6 +119,7 @@ int check_not_capturing(const char* what);
 int plain_op(mb_circuit c, const COp& op, double2* v, int n, int is_dm, int nsamples, int64_t mrow_stride,
              bool dagger);
 int circuit_clone(mb_circuit src, mb_circuit* out);
+int circuit_compile_host(const mb_op* ops, size_t nops, int n, mb_circuit c);
 void circuit_release(mb_circuit c);
 uint64_t next_circuit_uid();
 int servers_running();  // serve.cu
