@@ -74,3 +74,25 @@ def test_noisy_hea(mq, O):
     assert np.max(np.abs(s.to_numpy().ravel(order="F") - ref)) <= TOL
     H = W.xxz(n)
     assert abs(mq.expectation(H, s) - O.expect(ref, n, H.specs(), dm=True)) <= 1e-11
+
+
+@pytest.mark.parametrize("n,jit", [(7, False), (8, False), (9, True)])
+def test_noisy_hea_wider_than_a_tile(mq, O, n, jit, monkeypatch):
+    """Density matrices of 2n > tile bits: channels on (q, q+n) and both halves of every gate
+    fit paired row/column windows; checked against the oracle (1e-12), single and batched."""
+    from mossquantum_b200 import workloads as W
+    if jit:
+        monkeypatch.setenv("MB_JIT_MIN_BITS", "18")
+    c = W.hea_circuit(n, 1, W.hea_angles(n, 1, W.rng_for(2, n)), noise=(0.01, 0.02))
+    s = mq.apply_(c, mq.DensityMatrix(n))
+    ref = O.apply(c.specs(), O.zero_state(n, True), n, True)
+    assert np.max(np.abs(s.to_numpy().ravel(order="F") - ref)) <= TOL
+    if n == 7:
+        B = 2
+        ca = W.hea_circuit(n, 1, noise=(0.01, 0.02))
+        thetas = np.random.default_rng(n).uniform(0, 2 * np.pi, size=(B, ca.nparameters()))
+        sb = mq.apply_(ca, mq.BatchDensityMatrix(n, B), theta=thetas)
+        out = sb.to_numpy()
+        for b in range(B):
+            rb = O.apply(ca.copy().reset_parameters(thetas[b]).specs(), O.zero_state(n, True), n, True)
+            assert np.max(np.abs(out[:, :, b].ravel(order="F") - rb)) <= TOL
