@@ -145,6 +145,9 @@ extern "C" int mb_autotune(mb_circuit c, mb_state s, const double* theta, size_t
       rc = MB_OK;  // a width this circuit cannot use (e.g. no specialised kernels): skip it
       continue;
     }
+    int et = 0, er = 0;
+    mb_tuning_get(N, &et, &er);
+    if (et != cd[0] || er != cd[1]) continue;  // the library fell back to another width: not this candidate
     cudaEventRecord(a, g_ctx.stream);
     for (int k = 0; k < 2 && !rc; ++k) rc = mb_apply(c, s, theta, ntheta, flags & ~MB_APPLY_PLAIN);
     cudaEventRecord(b, g_ctx.stream);
