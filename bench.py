@@ -203,7 +203,7 @@ def reference_arm(args):
 
 
 def batch_workload(args):
-    """Config 2: 512 pure states with n uniform in 10..22 running the hardware-efficient
+    """Uneven batch: 512 pure states with n uniform in 10..22 running the hardware-efficient
     ansatz (depth 8) with per-sample angles, plus 64 ten-qubit density matrices with
     depolarizing (p=0.01) and amplitude damping (gamma=0.02) after every gate; output <XXZ>
     per sample. One step = one evaluation of the whole batch through a BatchPlan (one CUDA
@@ -296,7 +296,7 @@ def log(msg):
 
 
 def grad_workload(args):
-    """Config 3: adjoint gradient of the TFIM loss of a 24-qubit depth-16 hardware-efficient
+    """Gradients: adjoint gradient of the TFIM loss of a 24-qubit depth-16 hardware-efficient
     ansatz (1152 independent angles) with forward checkpoints every 4 layers, and the
     shared-parameter gradient of 64 ten-qubit density matrices with depolarizing noise
     (p = 0.005) after every gate. One step = one value_and_gradient of each; the plain
@@ -367,7 +367,7 @@ def grad_workload(args):
 
 
 def serve_workload(args):
-    """Config 4: Poisson arrivals at each swept rate; 70% pure requests (8..26 qubits), 30%
+    """Serving: Poisson arrivals at each swept rate; 70% pure requests (8..26 qubits), 30%
     density-matrix requests (6..12 qubits, depolarizing p=0.01 and amplitude damping
     gamma=0.02 after every gate); 4..32 hardware-efficient layers with random angles; TFIM
     or XXZ; expectation or adjoint gradient (50/50). Requests go through the continuous-

@@ -98,7 +98,7 @@ def test_config0_shape_at_n14(mq, O):
 
 
 def test_config0_full_size(mq, O):
-    """Config 0 exactly: 20 qubits, 10 layers, 600 angles, TFIM output."""
+    """The 20-qubit hardware-efficient workload exactly: 20 qubits, 10 layers, 600 angles, TFIM output."""
     from mossquantum_b200 import workloads as W
     n, depth = 20, 10
     c = W.hea_circuit(n, depth, W.hea_angles(n, depth, W.rng_for(0)))

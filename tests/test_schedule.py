@@ -2,8 +2,8 @@
 
 Every circuit must schedule in bounded time with every fused operation in exactly one pass:
 density-matrix channels on qubits farther apart than a tile window (paired row/column
-windows), 2-qubit gates between distant qubits (a plain pass), the config-1 and config-2
-circuits, across tile and register widths.
+windows), 2-qubit gates between distant qubits (a plain pass), the 28-qubit U3 circuit and
+the uneven-batch circuits, across tile and register widths.
 """
 import ctypes
 import time
