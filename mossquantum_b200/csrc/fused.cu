@@ -34,7 +34,6 @@ namespace mb {
 namespace {
 
 typedef std::complex<double> cd;
-constexpr int kThreadsMax = 256;
 
 // ---------------------------------------------------------------------------------------------
 // Kernels
