@@ -109,3 +109,29 @@ def test_fused_ansatz_blocks_on_tensor_cores(mq, O):
     for kw in ({"plain": True, "tensor": True}, {"plain": True}, {}):
         s = mq.apply_(f, mq.StateVector(n), **kw)
         assert np.max(np.abs(s.to_numpy() - ref)) <= 1e-12, kw
+
+
+@pytest.mark.parametrize("k", [4, 5])
+def test_high_qubit_gates_match_operator_products(mq, O, k):
+    """test/unit/high_qubit_gates.jl:1-46 on the device: the k-body gate
+    from_external(positions, kron(m1..mk)) through K5 equals the operator product
+    QubitsTerm(positions[j] => m_j) applied by the observable kernels (1e-12)."""
+    rng = np.random.default_rng(60 + k)
+    n = 12
+    for order in [(2, 9, 4, 12, 7)[:k], (12, 7, 2, 9, 4)[:k], (9, 2, 12, 4, 7)[:k]]:
+        ms = [random_unitary(2, rng) for _ in range(k)]
+        ext = ms[0]
+        for x in ms[1:]:
+            ext = np.kron(ext, x)
+        gate = mq.QCircuit([mq.QuantumGate(tuple(order), O.from_external(ext))])
+        term = mq.QubitsOperator([mq.QubitsTerm(list(order), ms)])
+        psi = random_state(n, rng)
+        ref = O.apply_observable(psi, n, term.specs())
+        for kw in ({"plain": True, "tensor": True}, {}, {"plain": True}):
+            s = mq.StateVector(n)
+            s.upload(psi)
+            mq.apply_(gate, s, **kw)
+            assert np.max(np.abs(s.to_numpy() - ref)) <= 1e-12, (order, kw)
+        s = mq.StateVector(n)
+        s.upload(psi)
+        assert np.max(np.abs(mq.apply_observable(term, s).to_numpy() - ref)) <= 1e-12

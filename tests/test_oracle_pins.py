@@ -146,3 +146,28 @@ def test_expectation_matches_dense_embedding():
 def test_probabilities_reject_unnormalised():
     with pytest.raises(ValueError):
         O.probabilities(np.array([1.0, 1.0], dtype=complex), 1)
+
+
+@pytest.mark.parametrize("k", [4, 5])
+def test_high_qubit_gates_match_operator_products(k):
+    """test/unit/high_qubit_gates.jl:1-46: a k-body gate from_external(positions, kron(m1..mk))
+    applied to a state equals the product QubitsTerm(positions[j] => m_j) applied as an
+    operator, for the reference's permuted position orders."""
+    import mossquantum_b200 as mq
+    rng = np.random.default_rng(40 + k)
+    L = 7
+    i, j, kk, l, m = 2, 5, 3, 7, 1
+    orders = {4: [(i, j, kk, l), (i, j, l, kk), (j, i, kk, l), (j, i, l, kk), (l, kk, j, i), (kk, i, l, j)],
+              5: [(i, j, kk, l, m), (i, j, l, m, kk), (j, i, m, kk, l), (j, m, i, l, kk), (l, kk, j, m, i),
+                  (m, kk, i, l, j)]}[k]
+    for order in orders:
+        ms = [random_unitary(2, rng) for _ in range(k)]
+        ext = ms[0]
+        for x in ms[1:]:
+            ext = np.kron(ext, x)          # kron(m1, ..., mk): m1 is the most significant factor
+        gate = mq.QuantumGate(tuple(order), O.from_external(ext))
+        term = mq.QubitsOperator([mq.QubitsTerm(list(order), ms)])
+        psi = random_state(L, rng)
+        a = O.apply(mq.QCircuit([gate]).specs(), psi, L)
+        b = O.apply_observable(psi, L, term.specs())
+        assert np.max(np.abs(a - b)) <= 1e-12, order
