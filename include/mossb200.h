@@ -337,8 +337,10 @@ MB_API int mb_server_stop(mb_server s);
  * call returns after the result has reached `out`.
  * Limits: k <= 3, nsamples <= 32 (the reduction scratch is a fixed 82,560-byte array in the
  * library, held on every GPU that loads it until exit). The first call on each device looks
- * up that array's device address, so make it before any stream capture. All calls share the
- * array: calls that overlap on the GPU race and must be serialised by the caller. */
+ * up that array's device address, so make it before any stream capture; the address is kept
+ * for the life of the process, so do not call this after resetting the device
+ * (cudaDeviceReset). All calls share the array: calls that overlap on the GPU race and must be
+ * serialised by the caller. */
 MB_API int mb_expect_local_noalloc(const double* state_dev, int n, int nsamples, int k, const int* positions,
                                    const double* matrix, double* out, void* stream);
 

@@ -11,7 +11,9 @@
 // The array holds 82,560 bytes and lives on every GPU that loads this library until the process
 // exits. All calls share it, and each call keeps its contents until the next call: two
 // calls that overlap on the GPU (different streams or threads) race on it and must be
-// serialised by the caller.
+// serialised by the caller. The array's device address is looked up on the first call on each
+// device and kept for the life of the process, so the entry point must not be used after the
+// caller resets that device (cudaDeviceReset), which invalidates the address.
 #include <cmath>
 #include <mutex>
 

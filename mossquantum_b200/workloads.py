@@ -55,6 +55,22 @@ def hea_circuit(n, depth, angles=None, active=True, noise=None):
     return c
 
 
+def cpu_scan_circuit(angles_by_layer):
+    """The reference's CPU-scheduling benchmark circuit (cpu_thread_scan.jl:4-18): on 1-based
+    layer l and qubit q a fixed (RX, RY, RZ)[mod1(l + q, 3)] with angle angles_by_layer[l][q],
+    then CNOT(q, q + 1) for q = 1..n-1."""
+    angles = np.asarray(angles_by_layer, dtype=np.float64)
+    depth, n = angles.shape
+    rot = (RxGate, RyGate, RzGate)
+    c = QCircuit()
+    for layer in range(1, depth + 1):
+        for q in range(1, n + 1):
+            c.push(rot[(layer + q - 1) % 3](q, float(angles[layer - 1, q - 1])))
+        for q in range(1, n):
+            c.push(CNOTGate(q, q + 1))
+    return c
+
+
 def u3_params(n, depth, rng):
     u = rng.uniform(0.0, 1.0, size=(depth, n))
     theta = np.arccos(1 - 2 * u)

@@ -26,6 +26,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <condition_variable>
 #include <cstdint>
 #include <cstring>
 #include <functional>
@@ -50,6 +51,87 @@ constexpr int64_t kPhaseMinWork = 32768;
 
 int g_threads = 1;
 
+// Persistent worker pool behind parallel_run / parallel_sum: the reference schedules its
+// ranges as tasks on Julia's resident thread pool, so threads are started once here too
+// rather than once per gate. The calling thread runs task 0 itself.
+class Pool {
+ public:
+  ~Pool() { resize(0); }
+  // Runs f(p) for p = 0..tasks-1 and returns when all have finished.
+  void run(int64_t tasks, const std::function<void(int64_t)>& f) {
+    if (tasks <= 1) {
+      if (tasks == 1) f(0);
+      return;
+    }
+    std::lock_guard<std::mutex> serial(run_mu_);
+    if (int64_t(workers_.size()) < tasks - 1) resize(int(tasks - 1));
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      job_ = &f;
+      tasks_ = tasks;
+      next_.store(1);
+      pending_ = tasks - 1;
+      ++gen_;
+    }
+    cv_.notify_all();
+    f(0);
+    std::unique_lock<std::mutex> lk(mu_);
+    done_cv_.wait(lk, [&] { return pending_ == 0; });
+    job_ = nullptr;
+  }
+
+ private:
+  void resize(int n) {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      stop_ = true;
+      ++gen_;
+    }
+    cv_.notify_all();
+    for (auto& t : workers_) t.join();
+    workers_.clear();
+    stop_ = false;
+    for (int i = 0; i < n; ++i) workers_.emplace_back([this] { loop(); });
+  }
+  void loop() {
+    uint64_t seen;
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      seen = gen_;
+    }
+    for (;;) {
+      const std::function<void(int64_t)>* job;
+      int64_t tasks;
+      {
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_.wait(lk, [&] { return gen_ != seen; });
+        seen = gen_;
+        if (stop_) return;
+        job = job_;
+        tasks = tasks_;
+      }
+      for (int64_t p = next_.fetch_add(1); p < tasks; p = next_.fetch_add(1)) {
+        (*job)(p);
+        std::lock_guard<std::mutex> lk(mu_);
+        if (--pending_ == 0) done_cv_.notify_one();
+      }
+    }
+  }
+  std::vector<std::thread> workers_;
+  std::mutex mu_, run_mu_;
+  std::condition_variable cv_, done_cv_;
+  const std::function<void(int64_t)>* job_ = nullptr;
+  int64_t tasks_ = 0, pending_ = 0;
+  std::atomic<int64_t> next_{0};
+  uint64_t gen_ = 0;
+  bool stop_ = false;
+};
+
+Pool& pool() {
+  static Pool p;
+  return p;
+}
+
 // parallel_run (src/utils/parallel_for.jl:9-45): contiguous zero-based inclusive ranges
 // [total*p/tasks, total*(p+1)/tasks - 1], tasks = max(1, min(threads, total / min_work)).
 void parallel_run(int64_t total, int64_t min_work, const std::function<void(int64_t, int64_t)>& f) {
@@ -58,26 +140,22 @@ void parallel_run(int64_t total, int64_t min_work, const std::function<void(int6
     if (total > 0) f(0, total - 1);
     return;
   }
-  std::vector<std::thread> pool;
-  pool.reserve(tasks);
-  for (int64_t p = 0; p < tasks; ++p) {
-    int64_t ist = total * p / tasks, ifn = total * (p + 1) / tasks - 1;
-    pool.emplace_back([=, &f] { if (ifn >= ist) f(ist, ifn); });
-  }
-  for (auto& t : pool) t.join();
+  pool().run(tasks, [&](int64_t p) {
+    const int64_t ist = total * p / tasks, ifn = total * (p + 1) / tasks - 1;
+    if (ifn >= ist) f(ist, ifn);
+  });
 }
 
 // parallel_sum (src/utils/parallel_for.jl:47-80): partitions into n_threads ranges when
 // total >= MIN_SIZE and sums the partial results.
 cplx parallel_sum(int64_t total, const std::function<cplx(int64_t, int64_t)>& f) {
   if (total >= kMinSize && g_threads > 1) {
-    std::vector<cplx> part(g_threads, cplx{0, 0});
-    std::vector<std::thread> pool;
-    for (int p = 0; p < g_threads; ++p) {
-      int64_t ist = total * p / g_threads, ifn = total * (p + 1) / g_threads - 1;
-      pool.emplace_back([=, &f, &part] { part[p] = ifn >= ist ? f(ist, ifn) : cplx{0, 0}; });
-    }
-    for (auto& t : pool) t.join();
+    const int tasks = g_threads;
+    std::vector<cplx> part(tasks, cplx{0, 0});
+    pool().run(tasks, [&](int64_t p) {
+      const int64_t ist = total * p / tasks, ifn = total * (p + 1) / tasks - 1;
+      part[p] = ifn >= ist ? f(ist, ifn) : cplx{0, 0};
+    });
     cplx r{0, 0};
     for (auto& v : part) r = cadd(r, v);
     return r;
@@ -94,12 +172,42 @@ static inline int64_t insert_zeros(int64_t i, int k, const int* pos) {
   return i;
 }
 
+// Small k with the block size known at compile time; the arithmetic (and its order) is the
+// generic loop's, so results are identical.
+template <int K>
+void apply_dense_k(cplx* v, int64_t len, const int* pos, const cplx* m) {
+  constexpr int d = 1 << K;
+  int64_t off[d];
+  for (int a = 0; a < d; ++a) {
+    int64_t o = 0;
+    for (int j = 0; j < K; ++j)
+      if ((a >> j) & 1) o |= int64_t(1) << pos[j];
+    off[a] = o;
+  }
+  parallel_run(len >> K, kDenseGateMinWork, [&](int64_t ist, int64_t ifn) {
+    cplx in[d], out[d];
+    for (int64_t b = ist; b <= ifn; ++b) {
+      const int64_t base = insert_zeros(b, K, pos);
+      for (int a = 0; a < d; ++a) in[a] = v[base + off[a]];
+      for (int r = 0; r < d; ++r) {
+        cplx acc = cmul(m[r], in[0]);
+        for (int c = 1; c < d; ++c) acc = cadd(acc, cmul(m[r + c * d], in[c]));
+        out[r] = acc;
+      }
+      for (int a = 0; a < d; ++a) v[base + off[a]] = out[a];
+    }
+  });
+}
+
 // Generic k-qubit sweep (k <= 10 so channels on up to 5 qubits fit): for every block of
 // 2^k amplitudes sharing the other bits, v_local <- M v_local, local bit j = bit pos[j].
 // Restates _apply_gate_2_impl! (serial_short_range.jl:2-71) and the 4/5-body kernels
 // (threaded_long_range.jl:3-132); the sum over j runs in ascending order like the
 // StaticArrays product M * v.
 void apply_dense(cplx* v, int64_t len, int k, const int* pos, const cplx* m) {
+  if (k == 1) return apply_dense_k<1>(v, len, pos, m);
+  if (k == 2) return apply_dense_k<2>(v, len, pos, m);
+  if (k == 3) return apply_dense_k<3>(v, len, pos, m);
   const int d = 1 << k;
   std::vector<int64_t> off(d);
   for (int a = 0; a < d; ++a) {

@@ -43,6 +43,31 @@ def build() -> str:
     return _LIB_PATH
 
 
+def _cpu_tag() -> str:
+    """Identifies this host's CPU (model and flags), so a -march=native build is only ever run
+    on the kind of CPU it was built for."""
+    import hashlib
+    try:
+        with open("/proc/cpuinfo") as f:
+            lines = f.read().splitlines()
+    except OSError:
+        lines = []
+    model = next((ln for ln in lines if ln.startswith("model name")), "")
+    flags = next((ln for ln in lines if ln.startswith("flags")), "")
+    return hashlib.sha1((model + flags).encode()).hexdigest()[:12]
+
+
+def use_fast() -> str:
+    """Switch this module to the host-native build (-O3 -march=native, FMA contraction), used
+    only to time the CPU baseline; parity checks use the portable build."""
+    global _lib, _LIB_PATH
+    sub = os.path.join("_build", "native-" + _cpu_tag())
+    subprocess.run(["make", "-s", "-C", _HERE, "fast", f"FAST_DIR={sub}"], check=True)
+    _LIB_PATH = os.path.join(_HERE, sub, "liboracle_fast.so")
+    _lib = None
+    return _LIB_PATH
+
+
 class OrOp(ctypes.Structure):
     _fields_ = [("kind", ctypes.c_int32), ("nq", ctypes.c_int32), ("pos", ctypes.c_int32 * 5),
                 ("nparams", ctypes.c_int32), ("mat", ctypes.c_void_p), ("gens", ctypes.c_void_p)]

@@ -3,7 +3,8 @@
 Restates the reference's known answers (test/unit/measurements.jl:1-54: a measured qubit
 measures the same outcome again with probability 1, post-selection of a Bell pair) and checks
 every collapse against a numpy restatement of measurement.jl / post_selection.jl applied to
-the same state with the same seeded generator (1e-12 max-abs on states, identical records).
+the same state with the same seeded generator (1e-12 max-abs on states, identical records);
+the outcome draw is restated here too (sampling.jl:3-18).
 """
 import numpy as np
 import pytest
@@ -16,6 +17,22 @@ def rand_state(n, rng):
     return v / np.linalg.norm(v)
 
 
+def ref_discrete_sample(rng, weights):
+    """Inverse-CDF draw (sampling.jl:3-18), restated here so the check does not use the
+    product's sampler: the first index whose running sum exceeds u * total, else the last
+    index with positive weight."""
+    w = np.asarray(weights, dtype=float)
+    threshold = rng.random() * float(np.sum(w))
+    cumulative, last_positive = 0.0, 0
+    for i, x in enumerate(w):
+        if x > 0:
+            last_positive = i
+        cumulative += x
+        if threshold < cumulative:
+            return i
+    return last_positive
+
+
 def ref_measure(psi, n, pos, auto_reset, rng, mq):
     """measure! on a host vector (measurement.jl:4-18, 151-172)."""
     bit = 1 << (pos - 1)
@@ -23,7 +40,7 @@ def ref_measure(psi, n, pos, auto_reset, rng, mq):
     p0 = np.sum(np.abs(psi[(idx & bit) == 0]) ** 2)
     l = np.array([p0, 1 - p0])
     l = np.maximum(l, 0) / np.sum(np.maximum(l, 0))
-    i = mq.discrete_sample(rng, l)
+    i = ref_discrete_sample(rng, l)
     p = l[i]
     out = np.zeros_like(psi)
     sel = ((idx & bit) != 0) == bool(i)
@@ -72,7 +89,7 @@ def test_batch_and_density_measurement(mq):
     for b in range(B):
         p0 = np.sum(np.abs(psis[b][(idx & bit) == 0]) ** 2)
         dist = np.array([p0, 1 - p0])
-        i = mq.discrete_sample(r, dist / dist.sum())
+        i = ref_discrete_sample(r, dist / dist.sum())
         assert outcomes[b] == i
         ref = np.where(((idx & bit) != 0) == bool(i), psis[b], 0) / np.sqrt(dist[i])
         assert np.max(np.abs(out[:, b] - ref)) <= 1e-12

@@ -16,26 +16,44 @@ def noisy_circuit(mq, W, n, layers):
     return c
 
 
+def discrete_sample(rng, weights):
+    """Inverse-CDF draw (sampling.jl:3-18), restated for the replay."""
+    w = np.asarray(weights, dtype=float)
+    threshold = rng.random() * float(np.sum(w))
+    cumulative, last_positive = 0.0, 0
+    for i, x in enumerate(w):
+        if x > 0:
+            last_positive = i
+        cumulative += x
+        if threshold < cumulative:
+            return i
+    return last_positive
+
+
 def replay(mq, O, circ, n, seed):
-    """One trajectory on the host: mixtures draw p_j and apply K_j/sqrt(p_j); other channels
-    draw ||K_j psi||^2 and apply K_j; normalised at the end."""
-    from mossquantum_b200.trajectories import _compile_channel
+    """One trajectory on the host, from the oracle's own Kraus matrices: a channel whose
+    operators all satisfy K_j'K_j = p_j I (a mixture) draws p_j and applies K_j/sqrt(p_j);
+    any other channel draws with weights ||K_j psi||^2 and applies K_j
+    (noisy_execution.jl:1-334); the state is normalised at the end."""
     gen = np.random.default_rng(int(seed))
     psi = O.zero_state(n)
-    for it in circ.flat():
-        if isinstance(it, mq.QuantumMap):
-            ch = _compile_channel(it)
-            pos0 = [p - 1 for p in ch.positions]
-            if ch.mixture:
-                j = mq.discrete_sample(gen, ch.weights)
-                psi = O.apply_matrix(psi, pos0, ch.options[j])
-            else:
-                cands = [O.apply_matrix(psi, pos0, k) for k in ch.kraus]
-                w = np.array([np.vdot(c, c).real for c in cands])
-                j = mq.discrete_sample(gen, w)
-                psi = cands[j]
+    for spec in circ.specs():
+        if spec[0] != "channel":
+            psi = O.apply([spec], psi, n)
+            continue
+        _, name, positions, params, _, data = spec
+        assert len(positions) == 1
+        ks = O.kraus_matrices(name, params, data, 1)
+        pos0 = [positions[0] - 1]
+        p = [np.trace(k.conj().T @ k).real / 2 for k in ks]
+        if all(np.allclose(k.conj().T @ k, pk * np.eye(2), atol=1e-14) for k, pk in zip(ks, p)):
+            keep = [j for j, pk in enumerate(p) if pk > 0]
+            j = keep[discrete_sample(gen, [p[i] for i in keep])]
+            psi = O.apply_matrix(psi, pos0, ks[j] / np.sqrt(p[j]))
         else:
-            psi = O.apply(mq.QCircuit([it]).specs(), psi, n)
+            cands = [O.apply_matrix(psi, pos0, k) for k in ks]
+            j = discrete_sample(gen, [np.vdot(c, c).real for c in cands])
+            psi = cands[j]
     return psi / np.linalg.norm(psi)
 
 
