@@ -43,10 +43,12 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
-    ap.add_argument("--workload", default="scale", choices=["scale", "batch", "grad", "serve"],
+    ap.add_argument("--case", default="all", help="kernel workload: one of " + ", ".join(KERNEL_CASES) + " or all")
+    ap.add_argument("--workload", default="scale", choices=["scale", "batch", "grad", "serve", "kernel"],
                     help="scale: 28-qubit U3+CZ circuit (headline); batch: uneven batch of 512 pure + 64 density "
                          "states; grad: adjoint gradients (24 qubits, 1152 angles; 64 noisy density matrices); "
-                         "serve: Poisson request stream through the continuous-batching server")
+                         "serve: Poisson request stream through the continuous-batching server; kernel: one small "
+                         "case per kernel family, each launch timed with CUDA events (the ncu capture command)")
     ap.add_argument("--plain-samples", type=int, default=48)
     ap.add_argument("--rates", default="4,8,16", help="serve: arrival rates (requests/s) to sweep")
     ap.add_argument("--requests", type=int, default=96, help="serve: requests per rate")
@@ -162,18 +164,58 @@ def build_workload(mq, W, n, depth, seed_stream):
     return W.u3_brickwork(n, depth, params)
 
 
-def cpu_baseline_run(n, layers_sample, threads, W, mq_circuit=None):
-    """Times the oracle (restated reference CPU method) on a bounded sample: `layers_sample`
-    layers of the same circuit family at the same qubit count, on `threads` host threads."""
+def timing_oracle():
+    """The oracle built for this host (-O3 -march=native, FMA contraction; the checker build is
+    portable and contraction-free), loaded only for the timed CPU baseline."""
     from oracle import oracle as O
+    O.use_fast()
+    return O
+
+
+def cpu_baseline_run(n, layers_sample, threads, W, repeats=3):
+    """Times the oracle (restated reference CPU method) on a bounded sample: `layers_sample`
+    layers of the same circuit family at the same qubit count, on `threads` host threads.
+    One untimed run, then the median of `repeats` runs. Returns (GB/s, seconds per run)."""
+    O = timing_oracle()
     O.set_threads(threads)
     circ = W.u3_brickwork(n, layers_sample, W.u3_params(n, layers_sample, W.rng_for(1, 99)))
     specs = circ.specs()
     state = O.zero_state(n)
-    t0 = time.perf_counter()
     O.apply(specs, state, n)
-    dt = time.perf_counter() - t0
+    times = []
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        O.apply(specs, state, n)
+        times.append(time.perf_counter() - t0)
+    dt = statistics.median(times)
     return plain_bytes(n, layers_sample) / dt / 1e9, dt
+
+
+# The reference's own median for its recorded 20-qubit depth-20 circuit (780 gates) with 16
+# Julia threads (docs/performance/cpu-scheduling-2026-11-17/summary.csv:94).
+REFERENCE_N20_D20_16T_S = 0.23005131
+
+
+def cpu_anchor(threads):
+    """The oracle on the reference's recorded 20-qubit, depth-20 benchmark circuit (exact
+    angles, tests/golden/cpu_scan_circuits.json): median of 5 runs after one untimed run,
+    reported beside the reference's own Julia time for the same circuit."""
+    from mossquantum_b200 import workloads as W
+    O = timing_oracle()
+    O.set_threads(threads)
+    with open(os.path.join(ROOT, "tests", "golden", "cpu_scan_circuits.json")) as f:
+        case = json.load(f)["cases"]["n20-d20"]
+    specs = W.cpu_scan_circuit(case["angles_by_layer"]).specs()
+    state = O.zero_state(20)
+    O.apply(specs, state, 20)
+    times = []
+    for _ in range(5):
+        t0 = time.perf_counter()
+        O.apply(specs, state, 20)
+        times.append(time.perf_counter() - t0)
+    return {"circuit": "reference n20-d20 (cpu_thread_scan.jl:4-18, recorded angles)", "threads": threads,
+            "oracle_median_s": statistics.median(times), "reference_julia_16_threads_median_s": REFERENCE_N20_D20_16T_S,
+            "note": "different hardware; context for the CPU baseline, not a pass/fail"}
 
 
 def reference_arm(args):
@@ -186,17 +228,19 @@ def reference_arm(args):
     sample_layers = 1
     vals = []
     for i in range(args.warmup + args.steps):
-        v, dt = cpu_baseline_run(n, sample_layers, threads, W)
+        v, dt = cpu_baseline_run(n, sample_layers, threads, W, repeats=1)
         if i >= args.warmup:
             vals.append(v)
     value = statistics.median(vals)
-    sample = f"{sample_layers} of {args.layers} layers at n={n} per step ({n} U3 + CZ brickwork)"
+    sample = (f"{sample_layers} of {args.layers} layers at n={n} per step ({n} U3 + CZ brickwork), "
+              f"host-native oracle build")
     line = {"metric": "gate-kernel HBM GB/s (effective, plain per-gate bytes)", "value": value, "unit": "GB/s",
             "impl": "reference", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "complex128 (f64)",
             "data": "synthetic (seeded)",
             "config": {"workload": f"u3_cz_brickwork n={n} layers={args.layers}", "qubits": n, "layers": args.layers},
-            "cpu_baseline": {"value": value, "unit": "GB/s", "cores": threads, "kind": "port", "sample": sample},
+            "cpu_baseline": {"value": value, "unit": "GB/s", "cores": threads, "kind": "port", "sample": sample,
+                             "anchor": cpu_anchor(threads)},
             "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -288,6 +332,103 @@ def batch_workload(args):
                 "d2h_bytes_per_step": 16 * evals},
             "gpu_launches": N.launch_count() - l0, "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
+    return 0
+
+
+def _random_unitary(d, rng):
+    z = rng.normal(size=(d, d)) + 1j * rng.normal(size=(d, d))
+    q, r = np.linalg.qr(z)
+    return q * (np.diag(r) / np.abs(np.diag(r)))
+
+
+def _case_setup(name, mq, W):
+    """(description, step) of one kernel case: a small workload (1 GiB states, or two 256 MiB
+    states for the adjoint) dominated by one kernel family."""
+    rng = np.random.default_rng(7)
+    if name in ("dense1_low", "dense1_high"):
+        n = 26
+        q = 2 if name == "dense1_low" else 26
+        c = mq.QCircuit([mq.QuantumGate(q, _random_unitary(2, rng)) for _ in range(4)])
+        s = mq.StateVector(n)
+        return f"K0 plain sweep: 4 dense 1-qubit gates on qubit {q}, n={n}", lambda: mq.apply_(c, s, plain=True)
+    if name == "tile":
+        n = 26
+        c = W.u3_brickwork(n, 20, W.u3_params(n, 20, W.rng_for(1, 0)))
+        s = mq.StateVector(n)
+        return f"K1 tile passes: U3 + CZ brickwork, n={n}, 20 layers", lambda: (s.set_zero(), mq.apply_(c, s))
+    if name == "density":
+        n = 13
+        c = W.hea_circuit(n, 1, W.hea_angles(n, 1, W.rng_for(9)), active=False, noise=(0.01, 0.02))
+        s = mq.DensityMatrix(n)
+        return f"K3 density passes: noisy HEA layer on a {n}-qubit density matrix (26 bits)", \
+            lambda: (s.set_zero(), mq.apply_(c, s))
+    if name == "pauli":
+        n = 26
+        s = mq.StateVector(n)
+        mq.apply_(W.u3_brickwork(n, 1, W.u3_params(n, 1, W.rng_for(1, 3))), s)
+        H = W.tfim(n)
+        return f"K4 Pauli pass: TFIM expectation (51 strings), n={n}", lambda: mq.expectation(H, s)
+    if name == "adjoint":
+        n, depth = 24, 2
+        c = W.hea_circuit(n, depth, W.hea_angles(n, depth, W.rng_for(3)))
+        obj = mq.ExpectationObjective(c, W.tfim(n), mq.StateVector(n))
+        th = c.active_parameters()
+        return f"K6 adjoint dual-state passes: HEA n={n} depth {depth}", \
+            lambda: mq.value_and_gradient(mq.AdjointGradient(), obj, th)
+    if name == "marginal":
+        n = 26
+        s = mq.StateVector(n)
+        mq.apply_(W.u3_brickwork(n, 1, W.u3_params(n, 1, W.rng_for(1, 4))), s)
+        return f"K7 marginal: probabilities of 10 qubits, n={n}", lambda: mq.probabilities(s, list(range(1, 11)))
+    if name in ("dmma", "dense5"):
+        n = 26
+        gates = []
+        for layer in range(4):
+            for a in range(1 + (layer % 2) * 2, n - 3, 5):
+                gates.append(mq.QuantumGate(tuple(range(a, a + 5)), _random_unitary(32, rng)))
+        c = mq.QCircuit(gates)
+        s = mq.StateVector(n)
+        tensor = name == "dmma"
+        return (f"K5 {'FP64 tensor cores' if tensor else 'on K0 (CUDA cores)'}: {len(gates)} random dense 5-qubit "
+                f"gates in brickwork, n={n}"), lambda: mq.apply_(c, s, plain=True, tensor=tensor)
+    raise ValueError(f"unknown kernel case {name}")
+
+
+KERNEL_CASES = ("dense1_low", "dense1_high", "tile", "density", "pauli", "adjoint", "marginal", "dmma", "dense5")
+
+
+def kernel_workload(args):
+    """One JSON line per kernel case: the case's dominant kernel with its launches, average
+    launch time (CUDA events on the library stream) and algorithmic bytes and flops per
+    launch, against the measured HBM peak and the FP64 rate of a DFMA-only probe."""
+    import mossquantum_b200 as mq
+    from mossquantum_b200 import _native as N
+    from mossquantum_b200 import workloads as W
+    mq.init(0)
+    peak, peak_kind = load_peaks()
+    fp64 = N.measure_fp64_peak()
+    names = KERNEL_CASES if args.case == "all" else [c.strip() for c in args.case.split(",")]
+    for name in names:
+        desc, step = _case_setup(name, mq, W)
+        for _ in range(max(1, args.warmup)):
+            step()
+        N.synchronize()
+        N.profile(True)
+        for _ in range(max(1, args.steps)):
+            step()
+        N.synchronize()
+        rep = N.profile_report()
+        N.profile(False)
+        kern, (lc, tms, byts, flops) = max(rep.items(), key=lambda kv: kv[1][1])
+        sec = tms / 1e3 / lc
+        line = {"case": name, "what": desc, "kernel": kern, "launches": lc, "avg_launch_ms": tms / lc,
+                "share": tms / sum(v[1] for v in rep.values()),
+                "algorithmic_bytes_per_launch": byts / lc, "gbs": byts / lc / sec / 1e9,
+                "hbm_frac": byts / lc / sec / 1e9 / peak, "hbm_peak": peak, "hbm_peak_kind": peak_kind,
+                "algorithmic_flops_per_launch": flops / lc, "tflops": flops / lc / sec / 1e12,
+                "fp64_frac": (flops / lc / sec / 1e12 / fp64) if fp64 else None, "fp64_peak_tflops": fp64,
+                "others": {k: [v[0], v[1]] for k, v in rep.items() if k != kern}}
+        print(json.dumps(line), flush=True)
     return 0
 
 
@@ -500,6 +641,8 @@ def main():
         return grad_workload(args)
     if args.workload == "serve":
         return serve_workload(args)
+    if args.workload == "kernel":
+        return kernel_workload(args)
     import torch
     import torch.distributed as dist
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -576,9 +719,11 @@ def main():
     cpu = None
     if not args.no_cpu_baseline and rank == 0 and world == 1:
         threads = os.cpu_count() or 1
-        v, dt = cpu_baseline_run(n, 1, threads, W)
+        v, dt = cpu_baseline_run(n, 1, threads, W, repeats=3)
         cpu = {"value": v, "unit": "GB/s", "cores": threads, "kind": "port",
-               "sample": f"1 of {depth} layers at n={n} ({dt:.1f} s, oracle C++ restatement)"}
+               "sample": f"1 of {depth} layers at n={n}, median of 3 warm runs ({dt:.2f} s each; C++ restatement "
+                         f"of the reference CPU method, host-native build)",
+               "anchor": cpu_anchor(threads)}
 
     if rank == 0:
         line = {"metric": "gate-kernel HBM GB/s (effective, plain per-gate bytes)", "value": value, "unit": "GB/s",

@@ -305,6 +305,14 @@ std::string reg_off_const(int j, int R, const int* reg) {
   return std::to_string(c) + "ull";
 }
 
+// Entry point of a generated source: mbk_tile (tile pass), mbk_reg (strided sweep) or
+// mbk_adj (adjoint dual-state pass).
+const char* kernel_name(const std::string& src) {
+  if (src.find(" mbk_adj(") != std::string::npos) return "mbk_adj";
+  if (src.find(" mbk_reg(") != std::string::npos) return "mbk_reg";
+  return "mbk_tile";
+}
+
 // Compiles (or fetches) a kernel; returns nullptr on any failure.
 CUfunction compile_kernel(const std::string& src, std::string* err) {
   {
@@ -363,7 +371,7 @@ CUfunction compile_kernel(const std::string& src, std::string* err) {
   n.destroy(&prog);
   CUmodule mod;
   CUfunction fn;
-  if (d.load(&mod, cubin.data()) != CUDA_SUCCESS || d.getfn(&fn, mod, "mbk") != CUDA_SUCCESS) {
+  if (d.load(&mod, cubin.data()) != CUDA_SUCCESS || d.getfn(&fn, mod, kernel_name(src)) != CUDA_SUCCESS) {
     *err = "module load failed";
     return nullptr;
   }
@@ -433,7 +441,7 @@ std::string jit_tile_source(const Pass& p, int R, int N, bool stage_params, int 
   const SharedMats smats = shared_mats(p, stage_params);
   o << kPrelude << shared_mats_decl(smats);
   o << "extern \"C\" __global__ void __launch_bounds__(" << threads << ", " << std::max(1, ctas)
-    << ") mbk(const __grid_constant__ TMap tmap, "
+    << ") mbk_tile(const __grid_constant__ TMap tmap, "
     << "const double2* __restrict__ tab, long long tstride, long long tps, long long ntiles, u32* err) {\n";
   o << "  extern __shared__ unsigned char smem_raw[];\n  __shared__ __align__(8) u64 bar[2];\n  __shared__ int s_abort;\n";
   o << shared_mats_fill(smats);
@@ -574,7 +582,7 @@ std::string jit_adjoint_source(const Pass& p, int R, int N, bool stage_params) {
   const TmaGeom& g = p.geom;
   const SharedMats smats = shared_mats(p, stage_params);
   o << kPrelude << shared_mats_decl(smats);
-  o << "extern \"C\" __global__ void __launch_bounds__(" << threads << ", 1) mbk(const __grid_constant__ TMap tmy, "
+  o << "extern \"C\" __global__ void __launch_bounds__(" << threads << ", 1) mbk_adj(const __grid_constant__ TMap tmy, "
     << "const __grid_constant__ TMap tmd, const double2* __restrict__ tab, long long tstride, long long tps, "
     << "long long ntiles, u32* err, double* gpart, u32* gcount, double* gout, const int* __restrict__ gslot) {\n";
   o << "  extern __shared__ unsigned char smem_raw[];\n  __shared__ __align__(8) u64 bar[2];\n  __shared__ int s_abort;\n"
@@ -702,7 +710,7 @@ std::string jit_reg_source(const Pass& p, int N, bool stage_params) {
   const int R = p.t, A = 1 << R;
   const SharedMats smats = shared_mats(p, stage_params);
   o << kPrelude << shared_mats_decl(smats);
-  o << "extern \"C\" __global__ void __launch_bounds__(128) mbk(double2* __restrict__ v, const double2* __restrict__ tab, "
+  o << "extern \"C\" __global__ void __launch_bounds__(128) mbk_reg(double2* __restrict__ v, const double2* __restrict__ tab, "
     << "long long tstride, long long groups, int nsamples) {\n";
   if (!smats.offs.empty()) o << shared_mats_fill(smats) << "  __syncthreads();\n";
   o << "  const long long total = groups * nsamples;\n";

@@ -644,6 +644,8 @@ int launch_marginal(const double2* v, int n, int is_dm, int nsamples, const int*
     identity = identity && qubits[j] == j;
   }
   const int64_t dim = int64_t(1) << n;
+  // A pure state is read whole and a density matrix only on its diagonal: 16 B per entry read.
+  ProfScope ps(nq <= 12 && !identity ? "k_marginal_small" : "k_marginal_large", 16.0 * double(dim) * nsamples, st);
   if (nq <= 12 && !identity) {
     size_t shm = sizeof(double) << nq;
     k_marginal_small<<<sample_grid(dim, nsamples), kBlock, shm, st>>>(v, n, is_dm, ro, out, flags, tol);
