@@ -121,7 +121,7 @@ __global__ void __launch_bounds__(TileBounds<R>::threads, TileBounds<R>::blocks)
       double2 v[1 << R];
 #pragma unroll
       for (int j = 0; j < (1 << R); ++j) v[j] = tl[fk::swz(lbase | uint32_t(fk::reg_offset<R>(j, reg)))];
-      fk::run_mops<R, U2>(v, a.mops + sd.op0, sd.nops, lbase, reg, base, a.table, a.tstride, b);
+      fk::run_mops<R, U2>(v, a.mops + sd.op0, sd.nops, lbase, reg, base, a.table, a.xtab, a.tstride, b);
 #pragma unroll
       for (int j = 0; j < (1 << R); ++j) tl[fk::swz(lbase | uint32_t(fk::reg_offset<R>(j, reg)))] = v[j];
       __syncthreads();
@@ -152,7 +152,7 @@ __global__ void __launch_bounds__(128) k_reg_pass(double2* __restrict__ v, const
     double2 x[1 << R];
 #pragma unroll
     for (int j = 0; j < (1 << R); ++j) x[j] = vs[base | fk::reg_offset<R>(j, reg)];
-    fk::run_mops<R, U2>(x, a.mops, a.nops, base, reg, 0, a.table, a.tstride, b);
+    fk::run_mops<R, U2>(x, a.mops, a.nops, base, reg, 0, a.table, a.xtab, a.tstride, b);
 #pragma unroll
     for (int j = 0; j < (1 << R); ++j) vs[base | fk::reg_offset<R>(j, reg)] = x[j];
   }
@@ -185,9 +185,15 @@ struct FOp {
   uint32_t pactive = 0;
   int sigma[32];
   int d = 1;
+  // Phase bookkeeping of the forward schedules (merge_phases): a fixed single-qubit phase
+  // diag(1, ph) on bits[0] that may be merged with its neighbours, and a global factor.
+  bool merge = false;
+  cd ph = cd(1, 0), glob = cd(1, 0);
 };
 
 struct Schedule {
+  std::vector<double2> xtab;      // derived coefficients (kXtabFlag offsets)
+  double2* d_xtab = nullptr;
   int N = 0, dm = 0, t = 0, R = 0, nsamples = 1;
   int lo = 0, hi = -1;  // instruction range [lo, hi) of the circuit
   int adjoint = 0;      // reverse sweep with gradient accumulators
@@ -206,7 +212,8 @@ namespace {
 
 // Algorithmic FP64 flops per amplitude of one micro-op: 8*2^k for a dense k-qubit complex
 // gate (2^k complex multiply-adds), scaled by the fraction of amplitudes a controlled or
-// diagonal op touches; swaps and sign flips count zero.
+// diagonal op touches; 8 for a 2x2 with real (or real-diagonal, imaginary-off-diagonal)
+// entries, 6 for a rotation applied as three shears; swaps and sign flips count zero.
 static double mop_flops(const MOp& m) {
   switch (m.type) {
     case MOP_U1: return 16.0;
@@ -215,6 +222,8 @@ static double mop_flops(const MOp& m) {
     case MOP_DIAG: return 6.0 * __builtin_popcount(m.active) / double(1 << m.nsel);
     case MOP_CPHASE: return m.r1 ? 0.0 : 6.0 / double(1 << m.nsel);
     case MOP_GRAD: return 8.0 * double(1 << m.nsel) + 8.0;
+    case MOP_RROT: case MOP_IROT: return 8.0;  // four real multiply-adds per amplitude
+    case MOP_LIFT: return 6.0;                 // three fused multiply-adds per amplitude
     default: return 0.0;
   }
 }
@@ -287,7 +296,16 @@ static FOp gate_fop(mb_circuit c, const COp& op, int shift, int conj, bool dagge
       finalize_masks(f);
       return f;
     }
-    // A diagonal that is identity unless all bits but one are set is a controlled 2x2.
+    if (op.k <= 3) {
+      // One complex multiply per touched amplitude, no register target needed (RZ, CRZ, ...).
+      f.type = MOP_DIAG;
+      for (int a = 0; a < d; ++a) f.off[a] = off(a, a);
+      f.active = op.active;
+      f.conj = fconj;
+      finalize_masks(f);
+      return f;
+    }
+    // Larger diagonals that are identity unless all bits but one are set: controlled 2x2.
     for (int tj = 0; tj < op.k && op.k >= 1; ++tj) {
       const int tb = 1 << tj, cm = (d - 1) & ~tb;
       uint32_t ctl = 0;
@@ -348,6 +366,19 @@ static FOp gate_fop(mb_circuit c, const COp& op, int shift, int conj, bool dagge
       is_x = is_zero(M[f.off[0]]) && is_one(M[f.off[1]]) && is_one(M[f.off[2]]) && is_zero(M[f.off[3]]);
     }
     f.type = is_x ? MOP_CTRLX : (f.nctrl ? MOP_CTRL : MOP_U1);
+    if (f.type == MOP_U1) {
+      // Real (RY, H) and real-diagonal / imaginary-off-diagonal (RX) matrices take half the
+      // arithmetic of a complex 2x2; the structure holds for U, conj U, U' and U^T alike.
+      if (op.parametric) {
+        if (op.family == MB_FAM_RY) f.type = MOP_RROT;
+        else if (op.family == MB_FAM_RX) f.type = MOP_IROT;
+      } else {
+        const double2* M = c->fixed_table.data();
+        const double2 e00 = M[f.off[0]], e10 = M[f.off[1]], e01 = M[f.off[2]], e11 = M[f.off[3]];
+        if (e00.y == 0.0 && e10.y == 0.0 && e01.y == 0.0 && e11.y == 0.0) f.type = MOP_RROT;
+        else if (e00.y == 0.0 && e11.y == 0.0 && e01.x == 0.0 && e10.x == 0.0) f.type = MOP_IROT;
+      }
+    }
     if (f.nctrl > 4) f.type = F_UNFUSABLE;
     f.conj = fconj;
     finalize_masks(f);
@@ -374,10 +405,164 @@ static void mark_unfusable_masks(FOp& f) {
   f.nd = f.all;
 }
 
-static void build_fops(mb_circuit c, int n, int dm, bool dagger, std::vector<FOp>& out, int lo = 0, int hi = -1) {
+// A fixed 2x2 as E = g * diag(1, A) * R * diag(1, B), R = [[c, -s], [s, c]] with c = |e00| and
+// s = |e10|, so that R runs as three shears with t = s / (1 + c) <= 1. Returns false (the gate
+// stays a complex 2x2) unless E is unitary to 1e-14 and the factors, with R as the product of
+// its shears, reproduce E to 1e-14.
+static bool decompose_u2(const cd E[4], cd* g, cd* A, cd* B, double* mt, double* sn) {
+  const cd u00 = std::conj(E[0]) * E[0] + std::conj(E[1]) * E[1];
+  const cd u01 = std::conj(E[0]) * E[2] + std::conj(E[1]) * E[3];
+  const cd u11 = std::conj(E[2]) * E[2] + std::conj(E[3]) * E[3];
+  if (std::abs(u00 - 1.0) > 1e-14 || std::abs(u11 - 1.0) > 1e-14 || std::abs(u01) > 1e-14) return false;
+  const double c = std::abs(E[0]), s = std::abs(E[1]);
+  if (!(s > 0.0)) return false;
+  *g = c > 0.0 ? E[0] / c : cd(1, 0);
+  *A = E[1] / (*g * s);
+  *B = -E[2] / (*g * s);
+  const double t = s / (1.0 + c);
+  const double r00 = 1.0 - t * s, r01 = -2.0 * t + s * t * t, r10 = s, r11 = 1.0 - s * t;
+  const cd F[4] = {*g * r00, *g * *A * r10, *g * r01 * *B, *g * *A * r11 * *B};
+  for (int e = 0; e < 4; ++e)
+    if (std::abs(F[e] - E[e]) > 1e-14) return false;
+  *mt = -t;
+  *sn = s;
+  return true;
+}
+
+static int xtab_push(std::vector<double2>* xt, double2 v) {
+  xt->push_back(v);
+  return int(xt->size() - 1) | kXtabFlag;
+}
+
+// diag(1, ph) on global bit `bit` as a single-selector phase micro-op (a sign flip for -1).
+static FOp phase_fop(int bit, cd ph, std::vector<double2>* xt) {
+  FOp f;
+  f.type = MOP_CPHASE;
+  f.nb = 1;
+  f.bits[0] = bit;
+  f.ctrl[0] = bit;
+  f.nctrl = 1;
+  f.cls = CLS_DIAG;
+  f.neg = ph == cd(-1, 0);
+  f.off[0] = xtab_push(xt, make_double2(ph.real(), ph.imag()));
+  finalize_masks(f);
+  return f;
+}
+
+// Phase merging for forward schedules. Every fixed single-qubit phase is held back and
+// multiplied into the next phase on the same bit until a non-diagonal op acts on that bit
+// (all diagonal ops commute, and a phase on a control bit commutes with the controlled op),
+// so a chain U3, CZ, U3 on one qubit costs one phase between the two rotations. Global
+// factors are collected into one diagonal micro-op (pure states; for density matrices the row
+// and column factors cancel).
+static void merge_phases(std::vector<FOp>& seq, bool dm, std::vector<double2>* xt) {
+  std::vector<FOp> out;
+  out.reserve(seq.size());
+  cd pend[64];
+  bool has[64] = {false};
+  cd glob(1, 0);
+  auto flush = [&](int q) {
+    if (!has[q]) return;
+    has[q] = false;
+    if (pend[q] != cd(1, 0)) out.push_back(phase_fop(q, pend[q], xt));
+  };
+  for (FOp& f : seq) {
+    if (f.merge) {
+      const int q = f.bits[0];
+      pend[q] = has[q] ? pend[q] * f.ph : f.ph;
+      has[q] = true;
+      glob *= f.glob;
+      continue;
+    }
+    for (int q = 0; q < 64; ++q)
+      if ((f.nd >> q) & 1) flush(q);
+    out.push_back(f);
+  }
+  for (int q = 0; q < 64; ++q) flush(q);
+  if (!dm && glob != cd(1, 0)) {
+    FOp f;
+    f.type = MOP_DIAG;
+    f.nb = 1;
+    f.bits[0] = 0;
+    f.cls = CLS_DIAG;
+    f.off[0] = f.off[1] = xtab_push(xt, make_double2(glob.real(), glob.imag()));
+    f.active = 3;
+    finalize_masks(f);
+    out.push_back(f);
+  }
+  seq.swap(out);
+}
+
+// One half of a fixed single-qubit gate (xt != nullptr, forward): a general unitary becomes
+// phase, three-shear rotation, phase (and a global factor); a diagonal becomes a phase and a
+// global factor. The phases are marked for merge_phases. Returns false to keep `f` as it is.
+static bool split_fixed_1q(mb_circuit c, const COp& op, const FOp& f, bool dm, std::vector<double2>* xt,
+                           std::vector<FOp>& seq) {
+  if (op.kind != MB_OP_GATE || op.k != 1 || op.parametric) return false;
+  const double2* M = c->fixed_table.data();
+  auto eff = [&](int e) {
+    const double2 x = M[f.off[e]];
+    return cd(x.x, f.conj ? -x.y : x.y);
+  };
+  const int q = f.bits[0];
+  if (f.type == MOP_DIAG && f.nb == 1) {
+    const cd d0 = eff(0), d1 = eff(1);
+    if (!(std::abs(d0) > 0.0)) return false;
+    if (dm && (std::abs(std::abs(d0) - 1.0) > 1e-14 || std::abs(std::abs(d1) - 1.0) > 1e-14)) return false;
+    FOp p;
+    p.merge = true;
+    p.bits[0] = q;
+    p.ph = d1 / d0;
+    p.glob = d0;
+    seq.push_back(p);
+    return true;
+  }
+  if (f.type == MOP_CPHASE && f.nctrl == 1) {
+    FOp p;
+    p.merge = true;
+    p.bits[0] = q;
+    p.ph = f.neg ? cd(-1, 0) : eff(0);
+    seq.push_back(p);
+    return true;
+  }
+  if (f.type != MOP_U1) return false;
+  const cd E[4] = {eff(0), eff(1), eff(2), eff(3)};
+  cd g, A, B;
+  double mt, sn;
+  if (!decompose_u2(E, &g, &A, &B, &mt, &sn)) return false;
+  FOp pb;
+  pb.merge = true;
+  pb.bits[0] = q;
+  pb.ph = B;
+  pb.glob = g;
+  seq.push_back(pb);
+  FOp r;
+  r.type = MOP_LIFT;
+  r.nb = 1;
+  r.bits[0] = q;
+  r.tgt[0] = q;
+  r.ntgt = 1;
+  r.cls = CLS_DENSE;
+  r.off[0] = xtab_push(xt, make_double2(mt, sn));
+  finalize_masks(r);
+  seq.push_back(r);
+  FOp pa;
+  pa.merge = true;
+  pa.bits[0] = q;
+  pa.ph = A;
+  seq.push_back(pa);
+  return true;
+}
+
+// xt: the schedule's derived table; when given (forward schedules), fixed single-qubit gates
+// are split into phases and shear rotations and the phases are merged.
+static void build_fops(mb_circuit c, int n, int dm, bool dagger, std::vector<FOp>& out, int lo = 0, int hi = -1,
+                       std::vector<double2>* xt = nullptr) {
   out.clear();
   std::vector<FOp> seq;
   if (hi < 0) hi = int(c->ops.size());
+  if (dagger) xt = nullptr;
+  if (xt && getenv("MB_NO_SPLIT")) xt = nullptr;
   for (int oi = lo; oi < hi; ++oi) {
     const COp& op = c->ops[oi];
     if (op.kind == MB_OP_CHANNEL) {
@@ -404,11 +589,15 @@ static void build_fops(mb_circuit c, int n, int dm, bool dagger, std::vector<FOp
       seq.push_back(f);
       continue;
     }
-    seq.push_back(gate_fop(c, op, 0, 0, dagger));
-    if (dm) seq.push_back(gate_fop(c, op, n, 1, dagger));
+    for (int half = 0; half < (dm ? 2 : 1); ++half) {
+      const FOp f = gate_fop(c, op, half ? n : 0, half, dagger);
+      if (xt && split_fixed_1q(c, op, f, dm, xt, seq)) continue;
+      seq.push_back(f);
+    }
   }
   for (FOp& f : seq) mark_unfusable_masks(f);
   if (dagger) std::reverse(seq.begin(), seq.end());
+  if (xt) merge_phases(seq, dm, xt);
   out = seq;
 }
 
@@ -584,6 +773,7 @@ static void plan_stages(const std::vector<FOp>& fops, const std::vector<int>& op
     sd.op0 = int(p.mops.size());
     for (int idx : taken) {
       const FOp& f = fops[idx];
+      p.fop_order.push_back(idx);
       MOp m{};
       m.type = int16_t(f.type);
       m.conj = int16_t(f.conj);
@@ -652,6 +842,7 @@ static void encode_reg_pass(const std::vector<FOp>& fops, const std::vector<int>
   sd.op0 = 0;
   for (int idx : ops) {
     const FOp& f = fops[idx];
+    p.fop_order.push_back(idx);
     MOp m{};
     m.type = int16_t(f.type);
     m.conj = int16_t(f.conj);
@@ -711,6 +902,7 @@ static void build_schedule(Schedule& S, int nsamples, bool allow_reg = true) {
       Pass p;
       p.kind = PASS_PLAIN;
       p.plain_fop = rem[0];
+      p.fop_order.push_back(rem[0]);
       S.passes.push_back(p);
       rem.erase(rem.begin());
       continue;
@@ -782,6 +974,7 @@ static void build_schedule(Schedule& S, int nsamples, bool allow_reg = true) {
       Pass p;
       p.kind = PASS_PLAIN;
       p.plain_fop = rem[0];
+      p.fop_order.push_back(rem[0]);
       S.passes.push_back(p);
       rem.erase(rem.begin());
       continue;
@@ -945,7 +1138,7 @@ int get_schedule_ex(mb_circuit c, int n, int dm, int adjoint, int lo, int hi, in
       return MB_EUNSUPPORTED;
     }
   } else {
-    build_fops(c, n, dm, false, S->fops, lo, hi);
+    build_fops(c, n, dm, false, S->fops, lo, hi, &S->xtab);
   }
   build_schedule(*S, nsamples, !adjoint);
   if (S->unschedulable) {
@@ -957,7 +1150,7 @@ int get_schedule_ex(mb_circuit c, int n, int dm, int adjoint, int lo, int hi, in
     const int R = p.kind == PASS_REG ? p.t : S->R;
     for (const MOp& m : p.mops) {
       const bool needs = m.type == MOP_U1 || m.type == MOP_CTRL || m.type == MOP_CTRLX || m.type == MOP_U2 ||
-                         m.type == MOP_GRAD;
+                         m.type == MOP_GRAD || m.type == MOP_RROT || m.type == MOP_IROT || m.type == MOP_LIFT;
       const bool two = m.type == MOP_U2 || (m.type == MOP_GRAD && m.nsel == 2);
       if (needs && (m.r0 < 0 || m.r0 >= R || (two && (m.r1 <= m.r0 || m.r1 >= R)))) {
         set_error("internal scheduling error: micro-op %d without a register target", int(m.type));
@@ -994,6 +1187,11 @@ int get_schedule_ex(mb_circuit c, int n, int dm, int adjoint, int lo, int hi, in
     if ((rc = dev_alloc((void**)&S->d_gslots, sizeof(int) * gs.size()))) return rc;
     MB_CHECK_CUDA(cudaMemcpyAsync(S->d_gslots, gs.data(), sizeof(int) * gs.size(), cudaMemcpyHostToDevice, g_ctx.stream));
   }
+  if (!S->xtab.empty()) {
+    if ((rc = dev_alloc((void**)&S->d_xtab, sizeof(double2) * S->xtab.size()))) return rc;
+    MB_CHECK_CUDA(cudaMemcpyAsync(S->d_xtab, S->xtab.data(), sizeof(double2) * S->xtab.size(), cudaMemcpyHostToDevice,
+                                  g_ctx.stream));
+  }
   MB_CHECK_CUDA(cudaStreamSynchronize(g_ctx.stream));
   if (!adjoint && S->R == 3 && !getenv("MB_REG_BITS")) {
     // Register width 3 exists only as specialised kernels: if they cannot all be built (source
@@ -1009,6 +1207,7 @@ int get_schedule_ex(mb_circuit c, int n, int dm, int adjoint, int lo, int hi, in
       dev_free(S->d_stages);
       dev_free(S->d_mops);
       dev_free(S->d_gslots);
+      dev_free(S->d_xtab);
       return get_schedule_ex(c, n, dm, adjoint, lo, hi, nsamples, out);
     }
   }
@@ -1115,6 +1314,7 @@ int run_schedule(mb_circuit c, Schedule* S, double2* v, int nsamples, int64_t ms
       a.stages = S->d_stages + p.stage_off;
       a.mops = S->d_mops;
       a.table = c->d_table;
+      a.xtab = S->d_xtab;
       a.err = g_ctx.flags + 2;
       const int threads = 1 << (p.t - S->R);
       const size_t shm = (size_t(32) << p.t) + 1024;  // two tile buffers + alignment slack
@@ -1124,8 +1324,8 @@ int run_schedule(mb_circuit c, Schedule* S, double2* v, int nsamples, int64_t ms
       if (S->jit == 1 && p.jit_fn) {
         ProfScope ps("k_tile_pass_jit", 32.0 * double(elems) * nsamples, st,
                      pass_flops_per_amp(p, false) * double(elems) * nsamples);
-        rc = jit_launch_tile((CUfunction)p.jit_fn, &map, c->d_table, mstride, a.tiles_per_sample, a.ntiles, a.err,
-                             threads, shm, int(grid), st);
+        rc = jit_launch_tile((CUfunction)p.jit_fn, &map, c->d_table, S->d_xtab, mstride, a.tiles_per_sample, a.ntiles,
+                             a.err, threads, shm, int(grid), st);
         ++launch_counter();
         if (rc) return rc;
         continue;
@@ -1151,13 +1351,14 @@ int run_schedule(mb_circuit c, Schedule* S, double2* v, int nsamples, int64_t ms
       a.tstride = mstride;
       a.mops = S->d_mops + p.mop_off;
       a.table = c->d_table;
+      a.xtab = S->d_xtab;
       const int64_t work = a.groups * nsamples;
       const int block = 128;
       const int grid = grid_for(work, block, int64_t(g_ctx.sm_count) * 16);
       if (S->jit == 1 && p.jit_fn) {
         ProfScope ps("k_reg_pass_jit", 32.0 * double(elems) * nsamples, st,
                      pass_flops_per_amp(p, false) * double(elems) * nsamples);
-        rc = jit_launch_reg((CUfunction)p.jit_fn, v, c->d_table, mstride, a.groups, nsamples, grid, st);
+        rc = jit_launch_reg((CUfunction)p.jit_fn, v, c->d_table, S->d_xtab, mstride, a.groups, nsamples, grid, st);
         ++launch_counter();
         if (rc) return rc;
         continue;
@@ -1257,6 +1458,7 @@ void release_schedules(mb_circuit c) {
     dev_free(s->d_stages);
     dev_free(s->d_mops);
     dev_free(s->d_gslots);
+    dev_free(s->d_xtab);
     delete s;
   }
   c->scheds.clear();
@@ -1316,8 +1518,25 @@ extern "C" int mb_schedule_info(const mb_op* ops, size_t nops, int n, int dm, in
   S.t = std::min(tile_bits, N);
   S.R = reg_bits;
   S.nsamples = nsamples;
-  mb::build_fops(&c, n, S.dm, false, S.fops);
+  mb::build_fops(&c, n, S.dm, false, S.fops, 0, -1, &S.xtab);
   mb::build_schedule(S, nsamples);
+  if (const char* dir = getenv("MB_JIT_DUMP")) {
+    // Development aid: the specialised kernel source of every pass (compiled offline to read
+    // register and spill counts).
+    int i = 0;
+    for (mb::Pass& ps : S.passes) {
+      std::string src;
+      if (ps.kind == mb::PASS_TILE) src = mb::jit_tile_source(ps, S.R, N, nsamples == 1, mb::tile_ctas(ps.t));
+      else if (ps.kind == mb::PASS_REG) src = mb::jit_reg_source(ps, N, nsamples == 1);
+      else continue;
+      char path[512];
+      snprintf(path, sizeof(path), "%s/pass_%03d.cu", dir, i++);
+      if (FILE* f = fopen(path, "w")) {
+        fwrite(src.data(), 1, src.size(), f);
+        fclose(f);
+      }
+    }
+  }
   int t = 0, r = 0, p = 0;
   size_t covered = 0;
   for (const mb::Pass& ps : S.passes) {
@@ -1331,5 +1550,225 @@ extern "C" int mb_schedule_info(const mb_op* ops, size_t nops, int n, int dm, in
   *nreg = r;
   *nplain = p;
   *complete = covered == S.fops.size() ? 1 : 0;
+  return MB_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Host-only consistency check of the lowering (diagnostic; no device, no mb_init)
+// ---------------------------------------------------------------------------------------------
+namespace mb {
+namespace {
+
+typedef std::complex<double> hcd;
+
+struct HostLowering {
+  const mb_circuit_s* c;
+  const std::vector<double2>* xt;
+  hcd el(int off, int conj) const {
+    const double2 v = (off & kXtabFlag) ? (*xt)[off & ~kXtabFlag] : c->fixed_table[off];
+    return hcd(v.x, conj ? -v.y : v.y);
+  }
+};
+
+// Applies one fused op to a host vector of 2^N amplitudes.
+void host_apply_fop(const HostLowering& L, const FOp& f, std::vector<hcd>& v) {
+  const int64_t len = int64_t(v.size());
+  auto bit = [](int64_t i, int b) { return int((i >> b) & 1); };
+  if (f.type == F_UNFUSABLE) {
+    // dense in the fused op's mode on its bits (ordered matrix at mat_off)
+    const int k = f.nb, d = 1 << k;
+    std::vector<hcd> M(size_t(d) * d);
+    for (int r = 0; r < d; ++r)
+      for (int q = 0; q < d; ++q) {
+        const double2 x = L.c->fixed_table[f.mat_off + r + q * d];
+        hcd e(x.x, x.y);
+        if (f.mode == MAT_CONJ) e = std::conj(e);
+        M[r + q * d] = e;
+      }
+    if (f.mode == MAT_ADJOINT || f.mode == MAT_TRANSPOSE) {
+      std::vector<hcd> T(M.size());
+      for (int r = 0; r < d; ++r)
+        for (int q = 0; q < d; ++q) T[r + q * d] = f.mode == MAT_ADJOINT ? std::conj(M[q + r * d]) : M[q + r * d];
+      M.swap(T);
+    }
+    uint64_t mask = 0;
+    for (int j = 0; j < k; ++j) mask |= uint64_t(1) << f.bits[j];
+    std::vector<hcd> x(d), y(d);
+    for (int64_t base = 0; base < len; ++base) {
+      if (base & int64_t(mask)) continue;
+      for (int a = 0; a < d; ++a) {
+        int64_t idx = base;
+        for (int j = 0; j < k; ++j)
+          if ((a >> j) & 1) idx |= int64_t(1) << f.bits[j];
+        x[a] = v[idx];
+      }
+      for (int r = 0; r < d; ++r) {
+        hcd acc = 0;
+        for (int q = 0; q < d; ++q) acc += M[r + q * d] * x[q];
+        y[r] = acc;
+      }
+      for (int a = 0; a < d; ++a) {
+        int64_t idx = base;
+        for (int j = 0; j < k; ++j)
+          if ((a >> j) & 1) idx |= int64_t(1) << f.bits[j];
+        v[idx] = y[a];
+      }
+    }
+    return;
+  }
+  auto ctl_ok = [&](int64_t i) {
+    for (int j = 0; j < f.nctrl; ++j)
+      if (!bit(i, f.ctrl[j])) return false;
+    return true;
+  };
+  switch (f.type) {
+    case MOP_U1: case MOP_CTRL: case MOP_CTRLX: case MOP_RROT: case MOP_IROT: case MOP_LIFT: {
+      const int t = f.tgt[0];
+      hcd m00, m10, m01, m11;
+      double mt = 0, sn = 0;
+      if (f.type == MOP_CTRLX) {
+        m00 = m11 = 0;
+        m10 = m01 = 1;
+      } else if (f.type == MOP_LIFT) {
+        const hcd ts = L.el(f.off[0], 0);
+        mt = ts.real();
+        sn = ts.imag();
+      } else {
+        m00 = L.el(f.off[0], f.conj);
+        m10 = L.el(f.off[1], f.conj);
+        m01 = L.el(f.off[2], f.conj);
+        m11 = L.el(f.off[3], f.conj);
+        if (f.type == MOP_RROT) {
+          m00 = m00.real(); m10 = m10.real(); m01 = m01.real(); m11 = m11.real();
+        } else if (f.type == MOP_IROT) {
+          m00 = m00.real(); m11 = m11.real(); m01 = hcd(0, m01.imag()); m10 = hcd(0, m10.imag());
+        }
+      }
+      for (int64_t i = 0; i < len; ++i) {
+        if (bit(i, t) || !ctl_ok(i)) continue;
+        const int64_t jj = i | (int64_t(1) << t);
+        hcd x = v[i], y = v[jj];
+        if (f.type == MOP_LIFT) {
+          x += mt * y;
+          y += sn * x;
+          x += mt * y;
+          v[i] = x;
+          v[jj] = y;
+        } else {
+          v[i] = m00 * x + m01 * y;
+          v[jj] = m10 * x + m11 * y;
+        }
+      }
+      return;
+    }
+    case MOP_U2: {
+      hcd u[16];
+      for (int e = 0; e < 16; ++e) u[e] = L.el(f.off[e], f.conj);
+      const int b0 = f.tgt[0], b1 = f.tgt[1];
+      for (int64_t i = 0; i < len; ++i) {
+        if (bit(i, b0) || bit(i, b1)) continue;
+        const int64_t id[4] = {i, i | (int64_t(1) << b0), i | (int64_t(1) << b1), i | (int64_t(1) << b0) | (int64_t(1) << b1)};
+        hcd x[4], y[4];
+        for (int a = 0; a < 4; ++a) x[a] = v[id[a]];
+        for (int r = 0; r < 4; ++r) {
+          y[r] = 0;
+          for (int q = 0; q < 4; ++q) y[r] += u[r + 4 * q] * x[q];
+        }
+        for (int a = 0; a < 4; ++a) v[id[a]] = y[a];
+      }
+      return;
+    }
+    case MOP_DIAG: {
+      for (int64_t i = 0; i < len; ++i) {
+        int a = 0;
+        for (int j = 0; j < f.nb; ++j) a |= bit(i, f.bits[j]) << j;
+        if ((f.active >> a) & 1) v[i] *= L.el(f.off[a], f.conj);
+      }
+      return;
+    }
+    case MOP_CPHASE: {
+      const hcd fac = f.neg ? hcd(-1, 0) : L.el(f.off[0], f.conj);
+      for (int64_t i = 0; i < len; ++i)
+        if (ctl_ok(i)) v[i] *= fac;
+      return;
+    }
+    default:
+      return;
+  }
+}
+
+}  // namespace
+}  // namespace mb
+
+// Diagnostic: lowers a fixed (non-parametric) circuit for a state of n qubits (dm: density
+// matrix) exactly as a forward schedule does, then applies to one seeded random vector on the
+// host (a) every instruction with its compiled matrix and (b) the lowered micro-ops in the order
+// the scheduled passes run them. err_ops / err_sched: max |(a) - (b)| for the micro-op sequence
+// before scheduling and in the scheduled order. For tests of the host lowering only: it returns
+// no amplitudes and needs no device.
+extern "C" int mb_lowering_check(const mb_op* ops, size_t nops, int n, int dm, int tile_bits, int reg_bits,
+                                 uint64_t seed, double* err_ops, double* err_sched) {
+  if ((!ops && nops) || !err_ops || !err_sched) return MB_EINVAL;
+  const int N = dm ? 2 * n : n;
+  if (n < 1 || N > 22 || tile_bits < 8 || tile_bits > 12 || reg_bits < 3 || reg_bits > 5) {
+    mb::set_error("lowering check: at most 22 amplitude bits, tile bits 8..12, register bits 3..5");
+    return MB_EINVAL;
+  }
+  mb_circuit_s c;
+  if (int rc = mb::circuit_compile_host(ops, nops, n, &c)) return rc;
+  for (const mb::COp& op : c.ops)
+    if (op.parametric || op.k == 0) {
+      mb::set_error("lowering check: fixed gates and channels only");
+      return MB_EUNSUPPORTED;
+    }
+  mb::Schedule S;
+  S.N = N;
+  S.dm = dm ? 1 : 0;
+  S.t = std::min(tile_bits, N);
+  S.R = reg_bits;
+  mb::build_fops(&c, n, S.dm, false, S.fops, 0, -1, &S.xtab);
+  mb::build_schedule(S, 1);
+  // random start vector
+  std::vector<mb::hcd> v0(size_t(1) << N);
+  uint64_t st = seed * 0x9E3779B97F4A7C15ull + 1;
+  auto rnd = [&] {
+    st ^= st << 13; st ^= st >> 7; st ^= st << 17;
+    return double(st >> 11) * (1.0 / 9007199254740992.0) - 0.5;
+  };
+  for (auto& x : v0) x = mb::hcd(rnd(), rnd());
+  // (a) the instructions with their compiled (ordered) matrices
+  std::vector<mb::hcd> ref = v0;
+  for (const mb::COp& op : c.ops) {
+    mb::FOp f;
+    f.type = -1;  // dense on its bits
+    f.mat_off = op.mat_off;
+    f.mode = mb::MAT_PLAIN;
+    if (op.kind == MB_OP_CHANNEL) {
+      f.nb = 2 * op.k;
+      for (int j = 0; j < op.k; ++j) { f.bits[j] = op.pos[j]; f.bits[j + op.k] = op.pos[j] + n; }
+      mb::host_apply_fop(mb::HostLowering{&c, &S.xtab}, f, ref);
+      continue;
+    }
+    f.nb = op.k;
+    for (int j = 0; j < op.k; ++j) f.bits[j] = op.pos[j];
+    mb::host_apply_fop(mb::HostLowering{&c, &S.xtab}, f, ref);
+    if (dm) {
+      for (int j = 0; j < op.k; ++j) f.bits[j] = op.pos[j] + n;
+      f.mode = mb::MAT_CONJ;
+      mb::host_apply_fop(mb::HostLowering{&c, &S.xtab}, f, ref);
+    }
+  }
+  const mb::HostLowering L{&c, &S.xtab};
+  std::vector<mb::hcd> a = v0, b = v0;
+  for (const mb::FOp& f : S.fops) mb::host_apply_fop(L, f, a);
+  for (const mb::Pass& p : S.passes)
+    for (int idx : p.fop_order) mb::host_apply_fop(L, S.fops[idx], b);
+  double ea = 0, eb = 0;
+  for (size_t i = 0; i < ref.size(); ++i) {
+    ea = std::max(ea, std::abs(a[i] - ref[i]));
+    eb = std::max(eb, std::abs(b[i] - ref[i]));
+  }
+  *err_ops = ea;
+  *err_sched = eb;
   return MB_OK;
 }

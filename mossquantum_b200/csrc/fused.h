@@ -17,7 +17,16 @@ enum MopType : int16_t {
   MOP_CPHASE = 5, // factor off[0] (or a sign flip when r1 = 1) where every selector bit is 1
   MOP_GRAD = 6,   // adjoint sweep: accumulate Re<y|D|delta> over register bits r0 (,r1);
                   // nsel = 1 or 2 bits, active = gradient accumulator index within the pass
+  MOP_RROT = 7,   // 2x2 with real entries on register bit r0 (RY, H): the real parts of off[0..3]
+  MOP_IROT = 8,   // 2x2 with a real diagonal and an imaginary off-diagonal on r0 (RX): Re off[0],
+                  // Re off[3], Im off[2], Im off[1]
+  MOP_LIFT = 9,   // real rotation [[c,-s],[s,c]] (c >= 0) on r0 as three shears,
+                  // x -= t*y; y += s*x; x -= t*y with off[0] = (-t, s), t = s/(1+c)
 };
+
+// Matrix offsets with this bit set index the schedule's own table of derived coefficients
+// (rotations and phases of decomposed gates, merged phases) instead of the circuit's table.
+constexpr int32_t kXtabFlag = 1 << 29;
 
 // A selector names one index bit: values < 64 are bits of the pass-local amplitude index,
 // values >= 64 are bit (sel - 64) of the tile's global base index (constant per tile).
@@ -57,6 +66,7 @@ struct Pass {
   std::vector<int> bits;        // pass-local bit i -> global amplitude bit
   std::vector<StageDesc> stages;
   std::vector<MOp> mops;
+  std::vector<int> fop_order;   // the schedule's fused ops in the order this pass applies them
   int plain_fop = -1;           // PASS_PLAIN: index into the schedule's fused ops
   bool has_u2 = false;          // holds a 4x4 micro-op (selects the kernel variant)
   void* jit_fn = nullptr;       // specialised kernel (CUfunction) when the JIT is in use

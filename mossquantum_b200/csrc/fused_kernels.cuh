@@ -12,9 +12,11 @@
 namespace mb {
 namespace fk {
 
-__device__ __forceinline__ double2 ldm(const double2* m, int off, int conj) {
-  double2 x = __ldg(m + off);
-  return conj ? make_double2(x.x, -x.y) : x;
+// Matrix element at `off`: the circuit's table row m, or the schedule's derived table x when
+// the offset carries kXtabFlag.
+__device__ __forceinline__ double2 ldm(const double2* m, const double2* x, int off, int conj) {
+  const double2 v = (off & kXtabFlag) ? __ldg(x + (off & ~kXtabFlag)) : __ldg(m + off);
+  return conj ? make_double2(v.x, -v.y) : v;
 }
 
 // Index bit of amplitude j (j is a compile-time register index).
@@ -63,6 +65,48 @@ __device__ __forceinline__ void u1(double2 (&a)[1 << R], double2 m00, double2 m1
     }
 }
 
+// Real 2x2 [[a, b], [c, d]] on register bit K: four real multiply-adds per amplitude.
+template <int R, int K>
+__device__ __forceinline__ void rrot(double2 (&v)[1 << R], double a, double c, double b, double d) {
+#pragma unroll
+  for (int j = 0; j < (1 << R); ++j)
+    if (!((j >> K) & 1)) {
+      const double2 x = v[j], y = v[j | (1 << K)];
+      v[j] = make_double2(fma(b, y.x, a * x.x), fma(b, y.y, a * x.y));
+      v[j | (1 << K)] = make_double2(fma(d, y.x, c * x.x), fma(d, y.y, c * x.y));
+    }
+}
+
+// [[a, i*b], [i*c, d]] with real a, b, c, d on register bit K.
+template <int R, int K>
+__device__ __forceinline__ void irot(double2 (&v)[1 << R], double a, double ci, double bi, double d) {
+#pragma unroll
+  for (int j = 0; j < (1 << R); ++j)
+    if (!((j >> K) & 1)) {
+      const double2 x = v[j], y = v[j | (1 << K)];
+      v[j] = make_double2(fma(-bi, y.y, a * x.x), fma(bi, y.x, a * x.y));
+      v[j | (1 << K)] = make_double2(fma(-ci, x.y, d * y.x), fma(ci, x.x, d * y.y));
+    }
+}
+
+// Rotation by three shears (mt = -t, s): three fused multiply-adds per component and pair.
+template <int R, int K>
+__device__ __forceinline__ void lift(double2 (&v)[1 << R], double mt, double s) {
+#pragma unroll
+  for (int j = 0; j < (1 << R); ++j)
+    if (!((j >> K) & 1)) {
+      double2 x = v[j], y = v[j | (1 << K)];
+      x.x = fma(mt, y.x, x.x);
+      x.y = fma(mt, y.y, x.y);
+      y.x = fma(s, x.x, y.x);
+      y.y = fma(s, x.y, y.y);
+      x.x = fma(mt, y.x, x.x);
+      x.y = fma(mt, y.y, x.y);
+      v[j] = x;
+      v[j | (1 << K)] = y;
+    }
+}
+
 template <int R, int K>
 __device__ __forceinline__ void ctrl(double2 (&a)[1 << R], double2 m00, double2 m10, double2 m01, double2 m11,
                                      const MOp* __restrict__ op, int nsel, uint64_t lbase, const int* reg,
@@ -94,10 +138,11 @@ __device__ __forceinline__ void ctrl(double2 (&a)[1 << R], double2 m00, double2 
 }
 
 template <int R, int K0, int K1>
-__device__ __forceinline__ void u2(double2 (&a)[1 << R], const double2* m, const MOp* __restrict__ op, int conj) {
+__device__ __forceinline__ void u2(double2 (&a)[1 << R], const double2* m, const double2* x, const MOp* __restrict__ op,
+                                   int conj) {
   double2 u[16];
 #pragma unroll
-  for (int e = 0; e < 16; ++e) u[e] = ldm(m, op->off[e], conj);
+  for (int e = 0; e < 16; ++e) u[e] = ldm(m, x, op->off[e], conj);
 #pragma unroll
   for (int j = 0; j < (1 << R); ++j)
     if (!((j >> K0) & 1) && !((j >> K1) & 1)) {
@@ -111,8 +156,8 @@ __device__ __forceinline__ void u2(double2 (&a)[1 << R], const double2* m, const
 }
 
 template <int R>
-__device__ __forceinline__ void diag(double2 (&a)[1 << R], const double2* m, const MOp* __restrict__ op, int nsel,
-                                     int conj, uint64_t lbase, const int* reg, uint64_t gbase) {
+__device__ __forceinline__ void diag(double2 (&a)[1 << R], const double2* m, const double2* xt, const MOp* __restrict__ op,
+                                     int nsel, int conj, uint64_t lbase, const int* reg, uint64_t gbase) {
   const uint32_t active = op->active;
   Sel sl[3];
 #pragma unroll
@@ -120,7 +165,7 @@ __device__ __forceinline__ void diag(double2 (&a)[1 << R], const double2* m, con
   double2 f[8];
 #pragma unroll
   for (int e = 0; e < 8; ++e)
-    f[e] = (e < (1 << nsel) && ((active >> e) & 1)) ? ldm(m, op->off[e], conj) : make_double2(1.0, 0.0);
+    f[e] = (e < (1 << nsel) && ((active >> e) & 1)) ? ldm(m, xt, op->off[e], conj) : make_double2(1.0, 0.0);
 #pragma unroll
   for (int j = 0; j < (1 << R); ++j) {
     const uint32_t idx = sel_val(sl[0], j) | (sel_val(sl[1], j) << 1) | (sel_val(sl[2], j) << 2);
@@ -185,14 +230,44 @@ __device__ __forceinline__ void cphase_dispatch(double2 (&a)[1 << R], int need, 
 template <int R, bool HAS_U2>
 __device__ __forceinline__ void run_mops(double2 (&a)[1 << R], const MOp* __restrict__ mops, int nops,
                                          uint64_t lbase, const int* reg, uint64_t gbase,
-                                         const double2* __restrict__ tab, int64_t tstride, int b) {
+                                         const double2* __restrict__ tab, const double2* __restrict__ xt,
+                                         int64_t tstride, int b) {
   for (int q = 0; q < nops; ++q) {
     const MOp* __restrict__ op = mops + q;
     const int type = op->type, r0 = op->r0, nsel = op->nsel, conj = op->conj;
     const double2* m = tab + (op->param ? int64_t(b) * tstride : 0);
-    if (type == MOP_U1) {
-      const double2 m00 = ldm(m, op->off[0], conj), m10 = ldm(m, op->off[1], conj);
-      const double2 m01 = ldm(m, op->off[2], conj), m11 = ldm(m, op->off[3], conj);
+    if (type == MOP_LIFT) {
+      const double2 ts = ldm(m, xt, op->off[0], 0);
+      switch (r0) {
+        FK_CASE_K(R, 0, (lift<R, KK>(a, ts.x, ts.y)))
+        FK_CASE_K(R, 1, (lift<R, KK>(a, ts.x, ts.y)))
+        FK_CASE_K(R, 2, (lift<R, KK>(a, ts.x, ts.y)))
+        FK_CASE_K(R, 3, (lift<R, KK>(a, ts.x, ts.y)))
+        FK_CASE_K(R, 4, (lift<R, KK>(a, ts.x, ts.y)))
+      }
+    } else if (type == MOP_RROT || type == MOP_IROT) {
+      const double2 m00 = ldm(m, xt, op->off[0], conj), m10 = ldm(m, xt, op->off[1], conj);
+      const double2 m01 = ldm(m, xt, op->off[2], conj), m11 = ldm(m, xt, op->off[3], conj);
+      if (type == MOP_RROT) {
+        switch (r0) {
+          FK_CASE_K(R, 0, (rrot<R, KK>(a, m00.x, m10.x, m01.x, m11.x)))
+          FK_CASE_K(R, 1, (rrot<R, KK>(a, m00.x, m10.x, m01.x, m11.x)))
+          FK_CASE_K(R, 2, (rrot<R, KK>(a, m00.x, m10.x, m01.x, m11.x)))
+          FK_CASE_K(R, 3, (rrot<R, KK>(a, m00.x, m10.x, m01.x, m11.x)))
+          FK_CASE_K(R, 4, (rrot<R, KK>(a, m00.x, m10.x, m01.x, m11.x)))
+        }
+      } else {
+        switch (r0) {
+          FK_CASE_K(R, 0, (irot<R, KK>(a, m00.x, m10.y, m01.y, m11.x)))
+          FK_CASE_K(R, 1, (irot<R, KK>(a, m00.x, m10.y, m01.y, m11.x)))
+          FK_CASE_K(R, 2, (irot<R, KK>(a, m00.x, m10.y, m01.y, m11.x)))
+          FK_CASE_K(R, 3, (irot<R, KK>(a, m00.x, m10.y, m01.y, m11.x)))
+          FK_CASE_K(R, 4, (irot<R, KK>(a, m00.x, m10.y, m01.y, m11.x)))
+        }
+      }
+    } else if (type == MOP_U1) {
+      const double2 m00 = ldm(m, xt, op->off[0], conj), m10 = ldm(m, xt, op->off[1], conj);
+      const double2 m01 = ldm(m, xt, op->off[2], conj), m11 = ldm(m, xt, op->off[3], conj);
       switch (r0) {
         FK_CASE_K(R, 0, (u1<R, KK>(a, m00, m10, m01, m11)))
         FK_CASE_K(R, 1, (u1<R, KK>(a, m00, m10, m01, m11)))
@@ -220,7 +295,7 @@ __device__ __forceinline__ void run_mops(double2 (&a)[1 << R], const MOp* __rest
           }
         } else {
           const bool neg = op->r1 != 0;
-          const double2 f = neg ? make_double2(-1.0, 0.0) : ldm(m, op->off[0], conj);
+          const double2 f = neg ? make_double2(-1.0, 0.0) : ldm(m, xt, op->off[0], conj);
           cphase_dispatch<R>(a, need, f, neg);
         }
       }
@@ -228,10 +303,10 @@ __device__ __forceinline__ void run_mops(double2 (&a)[1 << R], const MOp* __rest
       const bool sw = false;
       double2 m00 = make_double2(0, 0), m10 = m00, m01 = m00, m11 = m00;
       if (!sw) {
-        m00 = ldm(m, op->off[0], conj);
-        m10 = ldm(m, op->off[1], conj);
-        m01 = ldm(m, op->off[2], conj);
-        m11 = ldm(m, op->off[3], conj);
+        m00 = ldm(m, xt, op->off[0], conj);
+        m10 = ldm(m, xt, op->off[1], conj);
+        m01 = ldm(m, xt, op->off[2], conj);
+        m11 = ldm(m, xt, op->off[3], conj);
       }
       switch (r0) {
         FK_CASE_K(R, 0, (ctrl<R, KK>(a, m00, m10, m01, m11, op, nsel, lbase, reg, gbase, sw)))
@@ -241,23 +316,23 @@ __device__ __forceinline__ void run_mops(double2 (&a)[1 << R], const MOp* __rest
         FK_CASE_K(R, 4, (ctrl<R, KK>(a, m00, m10, m01, m11, op, nsel, lbase, reg, gbase, sw)))
       }
     } else if (type == MOP_DIAG) {
-      diag<R>(a, m, op, nsel, conj, lbase, reg, gbase);
+      diag<R>(a, m, xt, op, nsel, conj, lbase, reg, gbase);
     } else if constexpr (HAS_U2) {
       if (type == MOP_U2) {
         switch (r0 * 8 + op->r1) {
-          case 0 * 8 + 1: u2<R, 0, 1>(a, m, op, conj); break;
-          case 0 * 8 + 2: u2<R, 0, 2>(a, m, op, conj); break;
-          case 0 * 8 + 3: u2<R, 0, 3>(a, m, op, conj); break;
-          case 1 * 8 + 2: u2<R, 1, 2>(a, m, op, conj); break;
-          case 1 * 8 + 3: u2<R, 1, 3>(a, m, op, conj); break;
-          case 2 * 8 + 3: u2<R, 2, 3>(a, m, op, conj); break;
+          case 0 * 8 + 1: u2<R, 0, 1>(a, m, xt, op, conj); break;
+          case 0 * 8 + 2: u2<R, 0, 2>(a, m, xt, op, conj); break;
+          case 0 * 8 + 3: u2<R, 0, 3>(a, m, xt, op, conj); break;
+          case 1 * 8 + 2: u2<R, 1, 2>(a, m, xt, op, conj); break;
+          case 1 * 8 + 3: u2<R, 1, 3>(a, m, xt, op, conj); break;
+          case 2 * 8 + 3: u2<R, 2, 3>(a, m, xt, op, conj); break;
           default:
             if constexpr (R > 4) {
               switch (r0 * 8 + op->r1) {
-                case 0 * 8 + 4: u2<R, 0, 4>(a, m, op, conj); break;
-                case 1 * 8 + 4: u2<R, 1, 4>(a, m, op, conj); break;
-                case 2 * 8 + 4: u2<R, 2, 4>(a, m, op, conj); break;
-                case 3 * 8 + 4: u2<R, 3, 4>(a, m, op, conj); break;
+                case 0 * 8 + 4: u2<R, 0, 4>(a, m, xt, op, conj); break;
+                case 1 * 8 + 4: u2<R, 1, 4>(a, m, xt, op, conj); break;
+                case 2 * 8 + 4: u2<R, 2, 4>(a, m, xt, op, conj); break;
+                case 3 * 8 + 4: u2<R, 3, 4>(a, m, xt, op, conj); break;
               }
             }
         }
@@ -370,6 +445,7 @@ struct TileArgs {
   const StageDesc* stages;
   const MOp* mops;
   const double2* table;
+  const double2* xtab;     // the schedule's derived coefficients (kXtabFlag offsets)
   unsigned* err;
 };
 
@@ -383,6 +459,7 @@ struct RegArgs {
   int64_t tstride;
   const MOp* mops;
   const double2* table;
+  const double2* xtab;
 };
 
 }  // namespace mb

@@ -190,6 +190,8 @@ struct StageGen {
         return m.conj ? "cj(" + x + ")" : x;
       }
     }
+    if (m.off[e] & kXtabFlag)
+      return std::string(m.conj ? "ldc" : "ld") + "(xtab + " + std::to_string(m.off[e] & ~kXtabFlag) + ")";
     return std::string(m.conj ? "ldc" : "ld") + "(" + (m.param ? "tb" : "tab") + " + " + std::to_string(m.off[e]) + ")";
   }
 
@@ -204,6 +206,46 @@ struct StageGen {
           if (!(j & b))
             o << "  { const double2 ux = " << v(j) << ", uy = " << v(j | b) << "; " << v(j)
               << " = cfma(m01, uy, cmul(m00, ux)); " << v(j | b) << " = cfma(m11, uy, cmul(m10, ux)); }\n";
+        o << "}\n";
+        break;
+      }
+      case MOP_RROT: {
+        const int b = 1 << m.r0;
+        o << "{ const double ra = (" << ldm(m, 0) << ").x, rc = (" << ldm(m, 1) << ").x, rb = (" << ldm(m, 2)
+          << ").x, rd = (" << ldm(m, 3) << ").x;\n";
+        for (int j = 0; j < A; ++j)
+          if (!(j & b))
+            o << "  { const double2 ux = " << v(j) << ", uy = " << v(j | b) << "; " << v(j)
+              << " = make_double2(fma(rb, uy.x, ra * ux.x), fma(rb, uy.y, ra * ux.y)); " << v(j | b)
+              << " = make_double2(fma(rd, uy.x, rc * ux.x), fma(rd, uy.y, rc * ux.y)); }\n";
+        o << "}\n";
+        break;
+      }
+      case MOP_IROT: {
+        // [[a, i bi], [i ci, d]]
+        const int b = 1 << m.r0;
+        o << "{ const double ra = (" << ldm(m, 0) << ").x, ci = (" << ldm(m, 1) << ").y, bi = (" << ldm(m, 2)
+          << ").y, rd = (" << ldm(m, 3) << ").x;\n";
+        for (int j = 0; j < A; ++j)
+          if (!(j & b))
+            o << "  { const double2 ux = " << v(j) << ", uy = " << v(j | b) << "; " << v(j)
+              << " = make_double2(fma(-bi, uy.y, ra * ux.x), fma(bi, uy.x, ra * ux.y)); " << v(j | b)
+              << " = make_double2(fma(-ci, ux.y, rd * uy.x), fma(ci, ux.x, rd * uy.y)); }\n";
+        o << "}\n";
+        break;
+      }
+      case MOP_LIFT: {
+        // three shears: x += mt*y; y += s*x; x += mt*y (per component)
+        const int b = 1 << m.r0;
+        o << "{ const double2 ts = " << ldm(m, 0) << ";\n";
+        for (int j = 0; j < A; ++j)
+          if (!(j & b)) {
+            const std::string x = v(j), y = v(j | b);
+            o << "  " << x << ".x = fma(ts.x, " << y << ".x, " << x << ".x); " << x << ".y = fma(ts.x, " << y << ".y, " << x
+              << ".y); " << y << ".x = fma(ts.y, " << x << ".x, " << y << ".x); " << y << ".y = fma(ts.y, " << x << ".y, "
+              << y << ".y); " << x << ".x = fma(ts.x, " << y << ".x, " << x << ".x); " << x << ".y = fma(ts.x, " << y
+              << ".y, " << x << ".y);\n";
+          }
         o << "}\n";
         break;
       }
@@ -289,6 +331,8 @@ struct StageGen {
           int ct = 0;
           for (int c = 0; c < m.nsel; ++c)
             if (rk[c] >= 0 && ((j >> rk[c]) & 1)) ct |= 1 << c;
+          // With every selector in registers the factor index is known here: skip factors of 1.
+          if (rtpart.empty() && !((m.active >> ct) & 1)) continue;
           o << "  " << v(j) << " = cmul(F[" << ct << "u | ri], " << v(j) << ");\n";
         }
         o << "}\n";
@@ -404,7 +448,8 @@ static SharedMats shared_mats(const Pass& p, bool with_params) {
   for (const MOp& m : p.mops) {
     if (m.param && !with_params) continue;
     switch (m.type) {
-      case MOP_U1: case MOP_CTRL: for (int e = 0; e < 4; ++e) add(m.off[e]); break;
+      case MOP_U1: case MOP_CTRL: case MOP_RROT: case MOP_IROT: for (int e = 0; e < 4; ++e) add(m.off[e]); break;
+      case MOP_LIFT: add(m.off[0]); break;
       case MOP_U2: for (int e = 0; e < 16; ++e) add(m.off[e]); break;
       case MOP_DIAG: for (int e = 0; e < (1 << m.nsel); ++e) if ((m.active >> e) & 1) add(m.off[e]); break;
       case MOP_CPHASE: if (!m.r1) add(m.off[0]); break;
@@ -429,7 +474,8 @@ static std::string shared_mats_fill(const SharedMats& sm) {
   if (sm.offs.empty()) return "";
   std::ostringstream o;
   o << "  __shared__ double2 smat[" << sm.offs.size() << "];\n  for (u32 i = threadIdx.x; i < " << sm.offs.size()
-    << "u; i += blockDim.x) smat[i] = __ldg(tab + k_moffs[i]);\n";
+    << "u; i += blockDim.x) { const int mo = k_moffs[i]; smat[i] = (mo & " << kXtabFlag << ") ? __ldg(xtab + (mo & "
+    << (kXtabFlag - 1) << ")) : __ldg(tab + mo); }\n";
   return o.str();
 }
 
@@ -442,7 +488,8 @@ std::string jit_tile_source(const Pass& p, int R, int N, bool stage_params, int 
   o << kPrelude << shared_mats_decl(smats);
   o << "extern \"C\" __global__ void __launch_bounds__(" << threads << ", " << std::max(1, ctas)
     << ") mbk_tile(const __grid_constant__ TMap tmap, "
-    << "const double2* __restrict__ tab, long long tstride, long long tps, long long ntiles, u32* err) {\n";
+    << "const double2* __restrict__ tab, const double2* __restrict__ xtab, long long tstride, long long tps, "
+    << "long long ntiles, u32* err) {\n";
   o << "  extern __shared__ unsigned char smem_raw[];\n  __shared__ __align__(8) u64 bar[2];\n  __shared__ int s_abort;\n";
   o << shared_mats_fill(smats);
   o << "  double2* buf0 = (double2*)(((unsigned long long)smem_raw + 1023ull) & ~1023ull);\n";
@@ -711,7 +758,7 @@ std::string jit_reg_source(const Pass& p, int N, bool stage_params) {
   const SharedMats smats = shared_mats(p, stage_params);
   o << kPrelude << shared_mats_decl(smats);
   o << "extern \"C\" __global__ void __launch_bounds__(128) mbk_reg(double2* __restrict__ v, const double2* __restrict__ tab, "
-    << "long long tstride, long long groups, int nsamples) {\n";
+    << "const double2* __restrict__ xtab, long long tstride, long long groups, int nsamples) {\n";
   if (!smats.offs.empty()) o << shared_mats_fill(smats) << "  __syncthreads();\n";
   o << "  const long long total = groups * nsamples;\n";
   o << "  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < total; g += (long long)gridDim.x * blockDim.x) {\n";
@@ -773,12 +820,12 @@ int jit_prepare(std::vector<std::string>& sources, std::vector<CUfunction>& out,
   return MB_OK;
 }
 
-int jit_launch_tile(CUfunction fn, const CUtensorMap* map, const double2* tab, int64_t tstride, int64_t tps,
-                    int64_t ntiles, unsigned* err, int threads, size_t shm, int grid, cudaStream_t st) {
+int jit_launch_tile(CUfunction fn, const CUtensorMap* map, const double2* tab, const double2* xtab, int64_t tstride,
+                    int64_t tps, int64_t ntiles, unsigned* err, int threads, size_t shm, int grid, cudaStream_t st) {
   Drv& d = drv();
   if (d.setattr(fn, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, int(shm)) != CUDA_SUCCESS) return MB_EDEVICE;
   long long ts = tstride, tp = tps, nt = ntiles;
-  void* params[] = {(void*)map, (void*)&tab, &ts, &tp, &nt, &err};
+  void* params[] = {(void*)map, (void*)&tab, (void*)&xtab, &ts, &tp, &nt, &err};
   if (d.launch(fn, grid, 1, 1, threads, 1, 1, unsigned(shm), (CUstream)st, params, nullptr) != CUDA_SUCCESS) {
     set_error("JIT tile launch failed");
     return MB_EDEVICE;
@@ -786,12 +833,12 @@ int jit_launch_tile(CUfunction fn, const CUtensorMap* map, const double2* tab, i
   return MB_OK;
 }
 
-int jit_launch_reg(CUfunction fn, double2* v, const double2* tab, int64_t tstride, int64_t groups, int nsamples,
-                   int grid, cudaStream_t st) {
+int jit_launch_reg(CUfunction fn, double2* v, const double2* tab, const double2* xtab, int64_t tstride, int64_t groups,
+                   int nsamples, int grid, cudaStream_t st) {
   Drv& d = drv();
   long long ts = tstride, gr = groups;
   int ns = nsamples;
-  void* params[] = {&v, (void*)&tab, &ts, &gr, &ns};
+  void* params[] = {&v, (void*)&tab, (void*)&xtab, &ts, &gr, &ns};
   if (d.launch(fn, grid, 1, 1, 128, 1, 1, 0, (CUstream)st, params, nullptr) != CUDA_SUCCESS) {
     set_error("JIT sweep launch failed");
     return MB_EDEVICE;

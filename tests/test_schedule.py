@@ -59,3 +59,82 @@ def test_long_range_gates_get_plain_passes():
     gates += [mq.QuantumGate((6, 26), q), mq.QuantumGate((1, 28), q), mq.QuantumGate((4, 20), q), mq.RyGate(14, 0.3)]
     npasses, ntile, nreg, nplain, complete = schedule_info(mq.QCircuit(gates), n)
     assert complete == 1 and nplain == 2
+
+
+def lowering_errors(circ, n, dm=False, t=11, R=3, seed=1):
+    keep, ops, slot = [], [], 0
+    for it in circ.flat():
+        o, used = it._ops(slot, keep)
+        ops.extend(o)
+        slot += used
+    arr = (N.MbOp * max(1, len(ops)))(*ops)
+    ea, eb = ctypes.c_double(), ctypes.c_double()
+    N.check(N.load().mb_lowering_check(arr, len(ops), n, int(dm), t, R, seed, ctypes.byref(ea), ctypes.byref(eb)),
+            "mb_lowering_check")
+    return ea.value, eb.value
+
+
+def random_unitary(d, rng):
+    z = rng.normal(size=(d, d)) + 1j * rng.normal(size=(d, d))
+    q, r = np.linalg.qr(z)
+    return q * (np.diag(r) / np.abs(np.diag(r)))
+
+
+# The forward lowering splits fixed single-qubit gates into phase, three-shear rotation and
+# phase, merges phases across diagonal gates and runs real / RX-type matrices as real
+# micro-ops. On the host, the lowered micro-ops applied in the scheduled order must reproduce
+# the compiled instructions on a random vector (random entries of size ~0.5: 1e-12 relative).
+@pytest.mark.parametrize("t,R", [(8, 3), (10, 3), (11, 3), (12, 4)])
+def test_lowering_u3_brickwork(t, R):
+    n = 14
+    c = W.u3_brickwork(n, 6, W.u3_params(n, 6, W.rng_for(1, 14)))
+    ea, eb = lowering_errors(c, n, t=t, R=R)
+    assert ea <= 1e-12 and eb <= 1e-12, (ea, eb)
+
+
+def test_lowering_named_and_random_gates():
+    rng = np.random.default_rng(12)
+    n = 9
+    t = lambda: float(rng.uniform(-np.pi, np.pi))
+    gates = [mq.HGate(1), mq.XGate(2), mq.YGate(3), mq.ZGate(4), mq.SGate(5), mq.TGate(6), mq.sqrtXGate(7),
+             mq.sqrtYGate(8), mq.RxGate(9, t()), mq.RyGate(1, t()), mq.RzGate(2, t()), mq.PHASEGate(3, t()),
+             mq.SWAPGate(4, 8), mq.iSWAPGate(2, 6), mq.CZGate(1, 9), mq.CNOTGate(5, 2), mq.TOFFOLIGate(9, 1, 4),
+             mq.FREDKINGate(3, 7, 2), mq.CRxGate(4, 6, t()), mq.CRyGate(8, 1, t()), mq.CRzGate(2, 9, t()),
+             mq.CPHASEGate(3, 5, t()), mq.CCPHASEGate(1, 2, 3, t())]
+    # parametric families are bound on the device; here they enter as their fixed matrices
+    gates = [mq.QuantumGate(g.positions, g.mat()) for g in gates]
+    for _ in range(3):
+        for q in range(1, n + 1):
+            gates.append(mq.QuantumGate(q, random_unitary(2, rng)))
+        gates.append(mq.QuantumGate((2, 7), random_unitary(4, rng)))
+        gates.append(mq.QuantumGate((9, 3, 5), random_unitary(8, rng)))
+        gates.append(mq.QuantumGate(4, np.diag(np.exp(1j * rng.uniform(0, 6, size=2)))))
+    c = mq.QCircuit(gates)
+    for t_bits, R in ((8, 3), (9, 4)):
+        ea, eb = lowering_errors(c, n, t=t_bits, R=R)
+        assert ea <= 1e-12 and eb <= 1e-12, (ea, eb)
+
+
+def test_lowering_density_with_channels():
+    n = 5
+    c = W.u3_brickwork(n, 4, W.u3_params(n, 4, W.rng_for(1, 5)))
+    noisy = mq.QCircuit()
+    for g in c.flat():
+        noisy.push(g)
+        for q in g.positions:
+            noisy.push(mq.Depolarizing(q, 0.01))
+            noisy.push(mq.AmplitudeDamping(q, 0.02))
+    for t_bits, R in ((8, 3), (10, 4)):
+        ea, eb = lowering_errors(noisy, n, dm=True, t=t_bits, R=R)
+        assert ea <= 1e-12 and eb <= 1e-12, (ea, eb)
+
+
+def test_lowering_reference_recorded_circuit():
+    import json
+    import os
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "cpu_scan_circuits.json")
+    with open(path) as f:
+        case = json.load(f)["cases"]["n15-d20"]
+    c = mq.QCircuit([mq.QuantumGate(g.positions, g.mat()) for g in W.cpu_scan_circuit(case["angles_by_layer"]).flat()])
+    ea, eb = lowering_errors(c, 15, t=11, R=3)
+    assert ea <= 1e-12 and eb <= 1e-12, (ea, eb)
