@@ -50,8 +50,8 @@ def parse():
                          "serve: Poisson request stream through the continuous-batching server; kernel: one small "
                          "case per kernel family, each launch timed with CUDA events (the ncu capture command)")
     ap.add_argument("--plain-samples", type=int, default=48)
-    ap.add_argument("--rates", default="4,8,16", help="serve: arrival rates (requests/s) to sweep")
-    ap.add_argument("--requests", type=int, default=96, help="serve: requests per rate")
+    ap.add_argument("--rates", default="sat", help="serve: arrival rates (requests/s) to sweep; sat = saturating")
+    ap.add_argument("--requests", type=int, default=200, help="serve: requests per rate")
     return ap.parse_args()
 
 
@@ -507,126 +507,129 @@ def grad_workload(args):
     return 0
 
 
-def serve_workload(args):
-    """Serving: Poisson arrivals at each swept rate; 70% pure requests (8..26 qubits), 30%
-    density-matrix requests (6..12 qubits, depolarizing p=0.01 and amplitude damping
-    gamma=0.02 after every gate); 4..32 hardware-efficient layers with random angles; TFIM
-    or XXZ; expectation or adjoint gradient (50/50). Requests go through the continuous-
-    batching server (HBM admission budget 160 GB). The plain per-request path (each request
-    alone through the per-call API with one plain kernel per gate) is timed on a sample of the
-    same requests and its latency under the same arrivals follows from a FIFO queue."""
+def serve_measure(requests, rate, plain=True, seed_stream=0, log_prefix="serve"):
+    """Serving at one arrival rate (None = saturating: every request arrives at t = 0).
+
+    The request mix: 70% pure (8..26 qubits), 30% density matrices (6..12 qubits, depolarizing
+    p = 0.01 and amplitude damping gamma = 0.02 after every gate), 4..32 hardware-efficient
+    layers with random angles, TFIM or XXZ, half of them adjoint gradients. The server admits
+    them against its HBM budget (160 GB or 90% of what the library holds). The plain
+    per-request path then replays the same arrivals: each request alone through the per-call
+    API (one plain kernel per gate, plain adjoint) in arrival order, its latency measured from
+    its arrival to its completion."""
     import mossquantum_b200 as mq
     from mossquantum_b200 import _native as N
     from mossquantum_b200 import workloads as W
     from mossquantum_b200.serving import Server
     mq.init(0)
     budget = min(160 * 10**9, int(mq.memory_info()[1] * 0.9))
-    blocks = {}
+    blocks, obs = {}, {}
 
     def block(kind, n):
         if (kind, n) not in blocks:
             blocks[(kind, n)] = W.hea_layer(n, noise=W.SERVING_NOISE if kind == "density" else None)
         return blocks[(kind, n)]
-    obs = {}
 
     def observable(name, n):
         if (name, n) not in obs:
             obs[(name, n)] = W.tfim(n) if name == "tfim" else W.xxz(n)
         return obs[(name, n)]
-    rates = [float(r) for r in args.rates.split(",")]
     srv = Server(budget_bytes=budget)
-    # warm-up: every class once alone and in a batch (schedules, specialised kernels)
     t0 = time.perf_counter()
     classes = [("pure", n) for n in range(8, 27)] + [("density", n) for n in range(6, 13)]
-    # one request per class alone, then three together (both shapes of every specialised kernel)
+    # warm-up: every class alone, then three together (schedules and specialised kernels of both
+    # batch shapes), outside the measurement
     for wave in ((("tfim", True),), (("tfim", True), ("xxz", False), ("tfim", False))):
-        warm = []
-        for k, n in classes:
-            for o, g in wave:
-                warm.append(srv.submit(block(k, n), n, observable(o, n), np.zeros((2, 3 * n)), kind=k, gradient=g))
+        warm = [srv.submit(block(k, n), n, observable(o, n), np.zeros((2, 3 * n)), kind=k, gradient=g)
+                for k, n in classes for o, g in wave]
         for t in warm:
             srv.wait(t)
-        log(f"serve warm-up wave done after {time.perf_counter() - t0:.1f} s")
-    levels = []
+    warm_s = time.perf_counter() - t0
+    log(f"{log_prefix}: warm-up {warm_s:.1f} s")
+    rng = W.rng_for(5, seed_stream)
+    reqs = W.serving_requests(requests, rng)
+    arrivals = np.zeros(len(reqs)) if rate is None else np.cumsum(rng.exponential(1.0 / rate, size=len(reqs)))
+    srv.reset_stats()
     l0 = N.launch_count()
-    all_reqs = []
+    tickets = []
     with ClockSampler(0) as clk:
-        for li, rate in enumerate(rates):
-            rng = W.rng_for(5, li)
-            reqs = W.serving_requests(args.requests, rng)
-            gaps = rng.exponential(1.0 / rate, size=len(reqs))
-            srv.reset_stats()
-            tickets = []
-            t_start = time.perf_counter()
-            t_next = t_start
-            for (k, n, L, o, g, th), gap in zip(reqs, gaps):
-                t_next += gap
-                d = t_next - time.perf_counter()
-                if d > 0:
-                    time.sleep(d)
-                tickets.append(srv.submit(block(k, n), n, observable(o, n), th, kind=k, gradient=g))
-            results = [srv.wait(t) for t in tickets]
-            span = time.perf_counter() - t_start
-            st = srv.stats()
-            levels.append({"rate_req_per_s": rate, "requests": len(reqs), "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
-                           "evals_per_s": st["evals_per_s"], "span_s": span, "iterations": st["iterations"],
-                           "peak_hbm_bytes": st["peak_bytes"]})
-            all_reqs += [(r, a, res) for r, a, res in zip(reqs, np.cumsum(gaps), results)]
-            log(f"rate {rate}: p50 {st['p50_ms']:.1f} ms p99 {st['p99_ms']:.1f} ms {st['evals_per_s']:.1f} evals/s")
+        t_start = time.perf_counter()
+        for (k, n, L, o, g, th), a in zip(reqs, arrivals):
+            d = t_start + a - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            tickets.append(srv.submit(block(k, n), n, observable(o, n), th, kind=k, gradient=g))
+        results = [srv.wait(t) for t in tickets]
+        span = time.perf_counter() - t_start
+    st = srv.stats()
     launches = N.launch_count() - l0
     srv.close()
-    # Plain per-request path on a sample (same requests, each alone, one plain kernel per gate).
-    rng = W.rng_for(5, 99)
-    sample = [all_reqs[i] for i in rng.choice(len(all_reqs), size=min(args.plain_samples, len(all_reqs)), replace=False)]
+    out = {"rate_req_per_s": "saturating" if rate is None else rate, "requests": len(reqs),
+           "server": {"p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "evals_per_s": st["evals_per_s"],
+                      "wall_evals_per_s": len(reqs) / span, "iterations": st["iterations"],
+                      "peak_hbm_bytes": st["peak_bytes"], "warmup_s": warm_s},
+           "gpu_launches": launches, "clocks": clk.summary(),
+           "h2d_bytes": int(sum(8 * r[5].size for r in reqs)),
+           "d2h_bytes": int(sum(16 + (8 * r[5].size if r[4] else 0) for r in reqs))}
+    log(f"{log_prefix}: server p50 {st['p50_ms']:.0f} ms p99 {st['p99_ms']:.0f} ms "
+        f"{st['evals_per_s']:.2f} evals/s over {span:.1f} s")
+    if not plain:
+        return out
     os.environ["MB_ADJOINT_PLAIN"] = "1"
-    service = []
-    max_err = 0.0
-    for (k, n, L, o, g, th), _, res in sample:
-        noise = W.SERVING_NOISE if k == "density" else None
-        circ = W.unrolled(lambda row: W.hea_layer_bound(n, row, noise=noise), th)
-        t1 = time.perf_counter()
-        init = mq.DensityMatrix(n) if k == "density" else mq.StateVector(n)
-        if g:
-            tmpl = W.unrolled(lambda row: W.hea_layer(n, noise=noise), th)
-            objp = mq.ExpectationObjective(tmpl, observable(o, n), init)
-            v, grad = mq.value_and_gradient(mq.AdjointGradient(), objp, th.reshape(-1))
-            max_err = max(max_err, float(np.max(np.abs(grad - res.gradient.reshape(-1)))))
-        else:
-            st_ = mq.apply_(circ, init, plain=True)
-            v = mq.expectation(observable(o, n), st_).real
-        service.append(time.perf_counter() - t1)
-        max_err = max(max_err, abs(v - res.value.real))
-    del os.environ["MB_ADJOINT_PLAIN"]
-    mean_service = float(np.mean(service))
-    plain_levels = []
-    for lv in levels:
-        # FIFO single-server queue with the sampled service times under the same arrival rate
-        rng = W.rng_for(5, 77)
-        arr = np.cumsum(rng.exponential(1.0 / lv["rate_req_per_s"], size=lv["requests"]))
-        svc = rng.choice(service, size=lv["requests"])
-        done, lat = 0.0, []
-        for a, sv in zip(arr, svc):
-            done = max(done, a) + sv
-            lat.append((done - a) * 1e3)
-        plain_levels.append({"rate_req_per_s": lv["rate_req_per_s"], "p50_ms": float(np.percentile(lat, 50)),
-                             "p99_ms": float(np.percentile(lat, 99)), "evals_per_s": lv["requests"] / done})
-    best = max(levels, key=lambda lv: lv["evals_per_s"])
-    line = {"metric": "serving circuit-evals/s (continuous batching) with p50/p99 latency", "value": best["evals_per_s"],
-            "unit": "evals/s", "n_gpus": 1, "steps": len(rates), "warmup": 1, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "complex128 (f64)", "data": "synthetic (seeded)",
+    lat, max_err = [], 0.0
+    try:
+        t_start = time.perf_counter()
+        for ((k, n, L, o, g, th), a), res in zip(zip(reqs, arrivals), results):
+            d = t_start + a - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            noise = W.SERVING_NOISE if k == "density" else None
+            init = mq.DensityMatrix(n) if k == "density" else mq.StateVector(n)
+            if g:
+                tmpl = W.unrolled(lambda row: W.hea_layer(n, noise=noise), th)
+                objp = mq.ExpectationObjective(tmpl, observable(o, n), init)
+                v, grad = mq.value_and_gradient(mq.AdjointGradient(), objp, th.reshape(-1))
+                max_err = max(max_err, float(np.max(np.abs(grad - res.gradient.reshape(-1)))))
+            else:
+                circ = W.unrolled(lambda row: W.hea_layer_bound(n, row, noise=noise), th)
+                s_ = mq.apply_(circ, init, plain=True)
+                v = mq.expectation(observable(o, n), s_).real
+            max_err = max(max_err, abs(v - res.value.real))
+            lat.append((time.perf_counter() - (t_start + a)) * 1e3)
+        pspan = time.perf_counter() - t_start
+    finally:
+        del os.environ["MB_ADJOINT_PLAIN"]
+    out["plain_per_request"] = {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                                "evals_per_s": len(reqs) / pspan,
+                                "method": "the same requests replayed at the same arrival times, each alone "
+                                          "through the per-call API (one plain kernel per gate, plain adjoint)"}
+    out["speedup_evals_per_s"] = out["server"]["evals_per_s"] / out["plain_per_request"]["evals_per_s"]
+    out["max_abs_diff_vs_plain"] = max_err
+    log(f"{log_prefix}: plain p50 {out['plain_per_request']['p50_ms']:.0f} ms "
+        f"{out['plain_per_request']['evals_per_s']:.2f} evals/s")
+    return out
+
+
+def serve_workload(args):
+    """Serving: the request mix of serve_measure at each rate of --rates ("sat" = saturating),
+    --requests requests per rate, beside the plain per-request path replaying the same
+    arrivals."""
+    levels = []
+    for i, r in enumerate(args.rates.split(",")):
+        rate = None if r.strip() in ("sat", "inf") else float(r)
+        levels.append(serve_measure(args.requests, rate, seed_stream=i, log_prefix=f"serve[{r}]"))
+    best = max(levels, key=lambda lv: lv["server"]["evals_per_s"])
+    line = {"metric": "serving circuit-evals/s (continuous batching) with p50/p99 latency",
+            "value": best["server"]["evals_per_s"], "unit": "evals/s", "n_gpus": 1, "steps": len(levels),
+            "warmup": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "complex128 (f64)", "data": "synthetic (seeded)",
             "config": {"workload": "Poisson stream: 70% pure 8..26q, 30% density 6..12q (noisy), 4..32 layers, "
-                                   "TFIM/XXZ, 50% adjoint gradients", "hbm_budget_bytes": budget,
-                       "requests_per_rate": args.requests},
-            "levels": levels, "plain_per_request": {"mean_service_ms": mean_service * 1e3,
-                                                    "evals_per_s": 1.0 / mean_service, "levels": plain_levels,
-                                                    "sample": f"{len(sample)} requests timed alone"},
-            "max_abs_diff_vs_plain": max_err,
-            "e2e": {"value": best["evals_per_s"], "unit": "evals/s",
-                    "h2d_bytes_per_step": int(sum(8 * r[0][5].size for r in all_reqs) / max(1, len(rates))),
-                    "d2h_bytes_per_step": int(sum(16 + (8 * r[0][5].size if r[0][4] else 0) for r in all_reqs)
-                                              / max(1, len(rates))),
+                                   "TFIM/XXZ, 50% adjoint gradients", "requests_per_rate": args.requests},
+            "levels": levels,
+            "e2e": {"value": best["server"]["wall_evals_per_s"], "unit": "evals/s",
+                    "h2d_bytes_per_step": best["h2d_bytes"], "d2h_bytes_per_step": best["d2h_bytes"],
                     "note": "requests submitted from host memory, results read back on the host"},
-            "gpu_launches": launches, "clocks": clk.summary()}
+            "gpu_launches": sum(lv["gpu_launches"] for lv in levels), "clocks": best["clocks"]}
     print(json.dumps(line), flush=True)
     return 0
 

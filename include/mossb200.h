@@ -175,11 +175,12 @@ MB_API int mb_schedule_info(const mb_op* ops, size_t nops, int n, int dm, int ti
 /* Host-only check of the forward lowering (needs no device and no mb_init; a test hook, no
  * counterpart in the reference): lowers a circuit of fixed gates and channels for an n-qubit
  * pure state or density matrix (at most 22 amplitude bits) as the fused schedules do, applies
- * both the compiled instructions and the lowered micro-ops (before scheduling, and in the
- * order the scheduled passes run them) to one seeded random vector on the host, and reports
- * the two maximum deviations. Returns no amplitudes. */
+ * both the compiled instructions and the lowered micro-ops (before scheduling, in the order
+ * the scheduled passes run them, and as the passes' encoded register-stage micro-ops) to one
+ * seeded random vector on the host, and reports the three maximum deviations. Returns no
+ * amplitudes. */
 MB_API int mb_lowering_check(const mb_op* ops, size_t nops, int n, int dm, int tile_bits, int reg_bits, uint64_t seed,
-                             double* err_ops, double* err_sched);
+                             double* err_ops, double* err_sched, double* err_mops);
 /* apply!(circuit, state) (execution/gates.jl:21-36, batch_gates.jl, channels.jl).
  * theta: host array of nslots values (or B*nslots with MB_APPLY_PER_SAMPLE).
  * A circuit with channels requires a density kind (pure states must be promoted first,

@@ -125,7 +125,7 @@ def load():
         "mb_schedule_info": ([ctypes.POINTER(MbOp), sz, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                               ctypes.c_int, ip, ip, ip, ip, ip], ctypes.c_int),
         "mb_lowering_check": ([ctypes.POINTER(MbOp), sz, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
-                               ctypes.c_uint64, dp, dp], ctypes.c_int),
+                               ctypes.c_uint64, dp, dp, dp], ctypes.c_int),
         "mb_apply": ([vp, vp, dp, sz, ctypes.c_int], ctypes.c_int),
         "mb_observable_create": ([ctypes.POINTER(MbTerm), sz, ctypes.POINTER(vp)], ctypes.c_int),
         "mb_observable_free": ([vp], ctypes.c_int),

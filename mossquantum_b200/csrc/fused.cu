@@ -700,7 +700,8 @@ static bool tile_geom(const std::vector<int>& bits, int N, int nsamples, TmaGeom
 
 // Register stages of a tile pass: every stage loads 2^R amplitudes per thread over R
 // tile-local bits and applies the ops whose targets lie among them.
-static void plan_stages(const std::vector<FOp>& fops, const std::vector<int>& ops, Pass& p, int R) {
+static void plan_stages(const std::vector<FOp>& fops, const std::vector<int>& ops, Pass& p, int R,
+                        std::vector<double2>* xt = nullptr) {
   const int t = p.t;
   std::vector<int> loc(64, -1);
   for (int i = 0; i < t; ++i) loc[p.bits[i]] = i;
@@ -771,64 +772,136 @@ static void plan_stages(const std::vector<FOp>& fops, const std::vector<int>& op
     sd.ntid = int(tidb.size());
     for (int q = 0; q < sd.ntid; ++q) sd.tid[q] = tidb[q];
     sd.op0 = int(p.mops.size());
-    for (int idx : taken) {
-      const FOp& f = fops[idx];
-      p.fop_order.push_back(idx);
-      MOp m{};
-      m.type = int16_t(f.type);
-      m.conj = int16_t(f.conj);
-      m.param = int16_t(f.param);
-      std::memcpy(m.off, f.off, sizeof(m.off));
-      auto regidx = [&](int gbit) {
-        for (int k = 0; k < R; ++k)
-          if (regs[k] == loc[gbit]) return k;
-        return -1;
+    auto emit = [&](const FOp& f) {
+        MOp m{};
+        m.type = int16_t(f.type);
+        m.conj = int16_t(f.conj);
+        m.param = int16_t(f.param);
+        std::memcpy(m.off, f.off, sizeof(m.off));
+        auto regidx = [&](int gbit) {
+          for (int k = 0; k < R; ++k)
+            if (regs[k] == loc[gbit]) return k;
+          return -1;
+        };
+        auto sel = [&](int gbit) { return int16_t(loc[gbit] >= 0 ? loc[gbit] : 64 + gbit); };
+        if (f.type == MOP_GRAD) {
+          m.nsel = int16_t(f.nb);
+          m.active = uint32_t(p.grad_slots.size());
+          p.grad_slots.push_back(f.slot);
+          int ra = regidx(f.tgt[0]), rb = f.nb > 1 ? regidx(f.tgt[1]) : -1;
+          if (f.nb > 1 && ra > rb) {
+            int o2[16];
+            const int sw[4] = {0, 2, 1, 3};
+            for (int r = 0; r < 4; ++r)
+              for (int cc = 0; cc < 4; ++cc) o2[r + 4 * cc] = f.off[sw[r] + 4 * sw[cc]];
+            std::memcpy(m.off, o2, sizeof(o2));
+            std::swap(ra, rb);
+          }
+          m.r0 = int16_t(ra);
+          m.r1 = int16_t(rb);
+        } else if (f.type == MOP_U2) {
+          int ra = regidx(f.tgt[0]), rb = regidx(f.tgt[1]);
+          if (ra > rb) {
+            // swap the local bits of the 4x4 matrix so that local bit 0 is the lower register
+            int o2[16];
+            const int sw[4] = {0, 2, 1, 3};
+            for (int r = 0; r < 4; ++r)
+              for (int cc = 0; cc < 4; ++cc) o2[r + 4 * cc] = f.off[sw[r] + 4 * sw[cc]];
+            std::memcpy(m.off, o2, sizeof(o2));
+            std::swap(ra, rb);
+          }
+          m.r0 = int16_t(ra);
+          m.r1 = int16_t(rb);
+        } else if (f.type == MOP_DIAG) {
+          m.nsel = int16_t(f.nb);
+          for (int j = 0; j < f.nb; ++j) m.sel[j] = sel(f.bits[j]);
+          m.active = f.active;
+        } else if (f.type == MOP_CPHASE) {
+          m.nsel = int16_t(f.nctrl);
+          for (int j = 0; j < f.nctrl; ++j) m.sel[j] = sel(f.ctrl[j]);
+          m.r1 = int16_t(f.neg ? 1 : 0);
+        } else {
+          m.r0 = int16_t(regidx(f.tgt[0]));
+          m.nsel = int16_t(f.nctrl);
+          for (int j = 0; j < f.nctrl; ++j) m.sel[j] = sel(f.ctrl[j]);
+        }
+        p.mops.push_back(m);
       };
-      auto sel = [&](int gbit) { return int16_t(loc[gbit] >= 0 ? loc[gbit] : 64 + gbit); };
-      if (f.type == MOP_GRAD) {
-        m.nsel = int16_t(f.nb);
-        m.active = uint32_t(p.grad_slots.size());
-        p.grad_slots.push_back(f.slot);
-        int ra = regidx(f.tgt[0]), rb = f.nb > 1 ? regidx(f.tgt[1]) : -1;
-        if (f.nb > 1 && ra > rb) {
-          int o2[16];
-          const int sw[4] = {0, 2, 1, 3};
-          for (int r = 0; r < 4; ++r)
-            for (int cc = 0; cc < 4; ++cc) o2[r + 4 * cc] = f.off[sw[r] + 4 * sw[cc]];
-          std::memcpy(m.off, o2, sizeof(o2));
-          std::swap(ra, rb);
-        }
-        m.r0 = int16_t(ra);
-        m.r1 = int16_t(rb);
-      } else if (f.type == MOP_U2) {
-        int ra = regidx(f.tgt[0]), rb = regidx(f.tgt[1]);
-        if (ra > rb) {
-          // swap the local bits of the 4x4 matrix so that local bit 0 is the lower register
-          int o2[16];
-          const int sw[4] = {0, 2, 1, 3};
-          for (int r = 0; r < 4; ++r)
-            for (int cc = 0; cc < 4; ++cc) o2[r + 4 * cc] = f.off[sw[r] + 4 * sw[cc]];
-          std::memcpy(m.off, o2, sizeof(o2));
-          std::swap(ra, rb);
-        }
-        m.r0 = int16_t(ra);
-        m.r1 = int16_t(rb);
-      } else if (f.type == MOP_DIAG) {
-        m.nsel = int16_t(f.nb);
-        for (int j = 0; j < f.nb; ++j) m.sel[j] = sel(f.bits[j]);
-        m.active = f.active;
-      } else if (f.type == MOP_CPHASE) {
-        m.nsel = int16_t(f.nctrl);
-        for (int j = 0; j < f.nctrl; ++j) m.sel[j] = sel(f.ctrl[j]);
-        m.r1 = int16_t(f.neg ? 1 : 0);
-      } else {
-        m.r0 = int16_t(regidx(f.tgt[0]));
-        m.nsel = int16_t(f.nctrl);
-        for (int j = 0; j < f.nctrl; ++j) m.sel[j] = sel(f.ctrl[j]);
+    // Phases on register bits of this stage are grouped: each phase may move back to just after
+    // the last op of the stage that acts non-diagonally on its bit (everything it passes
+    // commutes with it), and phases whose windows overlap run as one diagonal over up to three
+    // register bits (7 complex multiplies for three phases instead of 12).
+    const int T = int(taken.size());
+    std::vector<int> wstart(T, -1);
+    auto regof = [&](int gbit) {
+      for (int k = 0; k < R; ++k)
+        if (regs[k] == loc[gbit]) return k;
+      return -1;
+    };
+    if (xt)
+      for (int i = 0; i < T; ++i) {
+        const FOp& f = fops[taken[i]];
+        if (f.type != MOP_CPHASE || f.nctrl != 1 || f.neg || !(f.off[0] & kXtabFlag) || regof(f.ctrl[0]) < 0) continue;
+        const int q = f.ctrl[0];
+        int st = 0;
+        for (int j = i - 1; j >= 0; --j)
+          if ((fops[taken[j]].nd >> q) & 1) {
+            st = j + 1;
+            break;
+          }
+        wstart[i] = st;
       }
-      p.mops.push_back(m);
+    std::vector<std::vector<int>> group_at(T);
+    std::vector<char> grouped(T, 0);
+    for (int i = 0; i < T; ++i) {
+      if (wstart[i] < 0 || grouped[i]) continue;
+      uint64_t bits = 0;
+      for (int k = i; k < T && __builtin_popcountll(bits) < 3; ++k) {
+        if (wstart[k] < 0 || grouped[k] || wstart[k] > i) continue;
+        const int q = fops[taken[k]].ctrl[0];
+        if ((bits >> q) & 1) continue;
+        bits |= uint64_t(1) << q;
+        grouped[k] = 1;
+        group_at[i].push_back(k);
+      }
     }
-    sd.nops = int(taken.size());
+    int nemit = 0;
+    for (int i = 0; i < T; ++i) {
+      const std::vector<int>& g = group_at[i];
+      if (g.size() == 1) {
+        emit(fops[taken[g[0]]]);
+        p.fop_order.push_back(taken[g[0]]);
+        ++nemit;
+      } else if (g.size() > 1) {
+        FOp d;
+        d.type = MOP_DIAG;
+        d.cls = CLS_DIAG;
+        d.nb = int(g.size());
+        std::vector<cd> ph(g.size());
+        for (size_t j = 0; j < g.size(); ++j) {
+          const FOp& f = fops[taken[g[j]]];
+          d.bits[j] = f.ctrl[0];
+          const double2 v = (*xt)[f.off[0] & ~kXtabFlag];
+          ph[j] = cd(v.x, v.y);
+          p.fop_order.push_back(taken[g[j]]);
+        }
+        d.active = ((1u << (1 << d.nb)) - 1) & ~1u;
+        for (int a = 1; a < (1 << d.nb); ++a) {
+          cd prod(1, 0);
+          for (int j = 0; j < d.nb; ++j)
+            if ((a >> j) & 1) prod *= ph[j];
+          d.off[a] = xtab_push(xt, make_double2(prod.real(), prod.imag()));
+        }
+        finalize_masks(d);
+        emit(d);
+        ++nemit;
+      }
+      if (wstart[i] >= 0) continue;  // a grouped phase: emitted with its group
+      emit(fops[taken[i]]);
+      p.fop_order.push_back(taken[i]);
+      ++nemit;
+    }
+    sd.nops = nemit;
     p.stages.push_back(sd);
     rem.swap(left);
   }
@@ -984,7 +1057,7 @@ static void build_schedule(Schedule& S, int nsamples, bool allow_reg = true) {
     p.bits = cands[bi].bits;
     p.t = int(p.bits.size());
     p.geom = bg;
-    if (p.kind == PASS_TILE) plan_stages(S.fops, best_taken, p, R);
+    if (p.kind == PASS_TILE) plan_stages(S.fops, best_taken, p, R, S.adjoint ? nullptr : &S.xtab);
     else encode_reg_pass(S.fops, best_taken, p);
     for (const MOp& m : p.mops) p.has_u2 |= m.type == MOP_U2;
     S.passes.push_back(p);
@@ -1543,7 +1616,7 @@ extern "C" int mb_schedule_info(const mb_op* ops, size_t nops, int n, int dm, in
     if (ps.kind == mb::PASS_TILE) ++t;
     else if (ps.kind == mb::PASS_REG) ++r;
     else ++p;
-    covered += ps.kind == mb::PASS_PLAIN ? 1 : ps.mops.size();
+    covered += ps.fop_order.size();
   }
   *npasses = int(S.passes.size());
   *ntile = t;
@@ -1697,6 +1770,86 @@ void host_apply_fop(const HostLowering& L, const FOp& f, std::vector<hcd>& v) {
   }
 }
 
+// Applies one encoded micro-op of a pass the way the pass kernels do: register index k names
+// global bit gbit(reg[k]); a selector below 64 names a pass-local bit (tile passes) or a
+// global bit (register sweeps), 64 + b the tile base bit b.
+void host_apply_mop(const HostLowering& L, const Pass& p, const StageDesc& sd, const MOp& m, std::vector<hcd>& v) {
+  const int64_t len = int64_t(v.size());
+  const bool tile = p.kind == PASS_TILE;
+  auto gbit_of_reg = [&](int k) { return tile ? p.bits[sd.reg[k]] : sd.reg[k]; };
+  auto gbit_of_sel = [&](int sel) { return sel >= 64 ? sel - 64 : (tile ? p.bits[sel] : sel); };
+  auto bit = [](int64_t i, int b) { return int((i >> b) & 1); };
+  auto el = [&](int e) { return L.el(m.off[e], m.conj); };
+  auto sel_ok = [&](int64_t i) {
+    for (int j = 0; j < m.nsel; ++j)
+      if (!bit(i, gbit_of_sel(m.sel[j]))) return false;
+    return true;
+  };
+  switch (m.type) {
+    case MOP_U1: case MOP_CTRL: case MOP_CTRLX: case MOP_RROT: case MOP_IROT: case MOP_LIFT: {
+      const int t = gbit_of_reg(m.r0);
+      for (int64_t i = 0; i < len; ++i) {
+        if (bit(i, t)) continue;
+        if ((m.type == MOP_CTRL || m.type == MOP_CTRLX) && !sel_ok(i)) continue;
+        const int64_t jj = i | (int64_t(1) << t);
+        hcd x = v[i], y = v[jj];
+        if (m.type == MOP_CTRLX) {
+          v[i] = y;
+          v[jj] = x;
+        } else if (m.type == MOP_LIFT) {
+          const hcd ts = L.el(m.off[0], 0);
+          x += ts.real() * y;
+          y += ts.imag() * x;
+          x += ts.real() * y;
+          v[i] = x;
+          v[jj] = y;
+        } else {
+          hcd m00 = el(0), m10 = el(1), m01 = el(2), m11 = el(3);
+          if (m.type == MOP_RROT) {
+            m00 = m00.real(); m10 = m10.real(); m01 = m01.real(); m11 = m11.real();
+          } else if (m.type == MOP_IROT) {
+            m00 = m00.real(); m11 = m11.real(); m01 = hcd(0, m01.imag()); m10 = hcd(0, m10.imag());
+          }
+          v[i] = m00 * x + m01 * y;
+          v[jj] = m10 * x + m11 * y;
+        }
+      }
+      return;
+    }
+    case MOP_U2: {
+      const int b0 = gbit_of_reg(m.r0), b1 = gbit_of_reg(m.r1);
+      for (int64_t i = 0; i < len; ++i) {
+        if (bit(i, b0) || bit(i, b1)) continue;
+        const int64_t id[4] = {i, i | (int64_t(1) << b0), i | (int64_t(1) << b1), i | (int64_t(1) << b0) | (int64_t(1) << b1)};
+        hcd x[4], y[4];
+        for (int a = 0; a < 4; ++a) x[a] = v[id[a]];
+        for (int r = 0; r < 4; ++r) {
+          y[r] = 0;
+          for (int q = 0; q < 4; ++q) y[r] += el(r + 4 * q) * x[q];
+        }
+        for (int a = 0; a < 4; ++a) v[id[a]] = y[a];
+      }
+      return;
+    }
+    case MOP_DIAG: {
+      for (int64_t i = 0; i < len; ++i) {
+        int a = 0;
+        for (int j = 0; j < m.nsel; ++j) a |= bit(i, gbit_of_sel(m.sel[j])) << j;
+        if ((m.active >> a) & 1) v[i] *= el(a);
+      }
+      return;
+    }
+    case MOP_CPHASE: {
+      const hcd fac = m.r1 ? hcd(-1, 0) : el(0);
+      for (int64_t i = 0; i < len; ++i)
+        if (sel_ok(i)) v[i] *= fac;
+      return;
+    }
+    default:
+      return;
+  }
+}
+
 }  // namespace
 }  // namespace mb
 
@@ -1707,8 +1860,8 @@ void host_apply_fop(const HostLowering& L, const FOp& f, std::vector<hcd>& v) {
 // before scheduling and in the scheduled order. For tests of the host lowering only: it returns
 // no amplitudes and needs no device.
 extern "C" int mb_lowering_check(const mb_op* ops, size_t nops, int n, int dm, int tile_bits, int reg_bits,
-                                 uint64_t seed, double* err_ops, double* err_sched) {
-  if ((!ops && nops) || !err_ops || !err_sched) return MB_EINVAL;
+                                 uint64_t seed, double* err_ops, double* err_sched, double* err_mops) {
+  if ((!ops && nops) || !err_ops || !err_sched || !err_mops) return MB_EINVAL;
   const int N = dm ? 2 * n : n;
   if (n < 1 || N > 22 || tile_bits < 8 || tile_bits > 12 || reg_bits < 3 || reg_bits > 5) {
     mb::set_error("lowering check: at most 22 amplitude bits, tile bits 8..12, register bits 3..5");
@@ -1759,16 +1912,26 @@ extern "C" int mb_lowering_check(const mb_op* ops, size_t nops, int n, int dm, i
     }
   }
   const mb::HostLowering L{&c, &S.xtab};
-  std::vector<mb::hcd> a = v0, b = v0;
+  std::vector<mb::hcd> a = v0, b = v0, e = v0;
   for (const mb::FOp& f : S.fops) mb::host_apply_fop(L, f, a);
   for (const mb::Pass& p : S.passes)
     for (int idx : p.fop_order) mb::host_apply_fop(L, S.fops[idx], b);
-  double ea = 0, eb = 0;
+  for (const mb::Pass& p : S.passes) {
+    if (p.kind == mb::PASS_PLAIN) {
+      mb::host_apply_fop(L, S.fops[p.plain_fop], e);
+      continue;
+    }
+    for (const mb::StageDesc& sd : p.stages)
+      for (int q = 0; q < sd.nops; ++q) mb::host_apply_mop(L, p, sd, p.mops[sd.op0 + q], e);
+  }
+  double ea = 0, eb = 0, ec = 0;
   for (size_t i = 0; i < ref.size(); ++i) {
     ea = std::max(ea, std::abs(a[i] - ref[i]));
     eb = std::max(eb, std::abs(b[i] - ref[i]));
+    ec = std::max(ec, std::abs(e[i] - ref[i]));
   }
   *err_ops = ea;
   *err_sched = eb;
+  *err_mops = ec;
   return MB_OK;
 }
