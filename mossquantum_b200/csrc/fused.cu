@@ -178,7 +178,8 @@ struct FOp {
   uint32_t active = 0;
   int conj = 0, param = 0;
   bool neg = false;           // MOP_CPHASE with factor -1 (a sign flip)
-  int slot = -1;              // MOP_GRAD: parameter slot
+  int slot = -1;              // MOP_GRAD / MOP_GRADP: parameter slot
+  int pauli = 0;              // MOP_GRADP: generator code (1 X, 2 Y, 3 Z, 4 PHASE)
   // plain fallback
   int cls = CLS_DENSE;
   int mat_off = 0, mode = MAT_PLAIN;
@@ -224,13 +225,15 @@ static double mop_flops(const MOp& m) {
     case MOP_GRAD: return 8.0 * double(1 << m.nsel) + 8.0;
     case MOP_RROT: case MOP_IROT: return 8.0;  // four real multiply-adds per amplitude
     case MOP_LIFT: return 6.0;                 // three fused multiply-adds per amplitude
+    case MOP_GRADP: return 4.0;                // two multiply-adds per amplitude
     default: return 0.0;
   }
 }
 
 static double pass_flops_per_amp(const Pass& p, bool dual) {
   double f = 0;
-  for (const MOp& m : p.mops) f += (dual && m.type != MOP_GRAD) ? 2.0 * mop_flops(m) : mop_flops(m);
+  for (const MOp& m : p.mops)
+    f += (dual && m.type != MOP_GRAD && m.type != MOP_GRADP) ? 2.0 * mop_flops(m) : mop_flops(m);
   return f;
 }
 
@@ -624,6 +627,17 @@ static bool build_adjoint_fops(mb_circuit c, int lo, int hi, std::vector<FOp>& o
         for (int cc = 0; cc < d; ++cc) g.off[r + d * cc] = op.gen_off + r + d * cc;
       g.param = op.parametric ? 1 : 0;
       g.slot = op.slot;
+      if (op.k == 1 && op.parametric) {
+        // Rotation families have constant generators (k_bind's family_matrix): no table reads
+        // and four multiply-adds per pair instead of a 2x2 apply and a dot product.
+        const int code = op.family == MB_FAM_RX ? 1 : op.family == MB_FAM_RY ? 2 : op.family == MB_FAM_RZ ? 3
+                         : op.family == MB_FAM_PHASE ? 4 : 0;
+        if (code) {
+          g.type = MOP_GRADP;
+          g.pauli = code;
+          g.neg = (op.flags & MB_OPF_ADJOINT) != 0;
+        }
+      }
       finalize_masks(g);
       g.nd = g.all;
       out.push_back(g);
@@ -740,14 +754,21 @@ static void plan_stages(const std::vector<FOp>& fops, const std::vector<int>& op
         regs.push_back(q);
         rmask |= uint64_t(1) << q;
       }
-    // Take the ops that fit.
+    // Take the ops that fit. A single-bit diagonal whose bit is a thread bit here is left for a
+    // later stage when a later op of the pass acts non-diagonally on that bit (and so brings it
+    // into registers): there it multiplies half the amplitudes instead of all of them.
     std::vector<int> taken, left;
+    std::vector<uint64_t> later_nd(rem.size() + 1, 0);
+    for (size_t i = rem.size(); i-- > 0;) later_nd[i] = later_nd[i + 1] | lmask(fops[rem[i]].nd);
     b_all = b_nd = 0;
-    for (int idx : rem) {
+    for (size_t ri = 0; ri < rem.size(); ++ri) {
+      const int idx = rem[ri];
       const FOp& f = fops[idx];
       const uint64_t nd = lmask(f.nd), al = lmask(f.all & mask_of(p.bits)) | nd;
       const bool comm = (nd & b_all) == 0 && (al & b_nd) == 0;
-      if ((nd & ~rmask) == 0 && comm) {
+      const bool diag1 = (f.type == MOP_DIAG && f.nb == 1) || (f.type == MOP_CPHASE && f.nctrl == 1 && !f.neg);
+      const bool defer = diag1 && (al & ~rmask) != 0 && (al & ~rmask & later_nd[ri + 1]) != 0;
+      if ((nd & ~rmask) == 0 && comm && !defer) {
         taken.push_back(idx);
       } else {
         left.push_back(idx);
@@ -784,7 +805,14 @@ static void plan_stages(const std::vector<FOp>& fops, const std::vector<int>& op
           return -1;
         };
         auto sel = [&](int gbit) { return int16_t(loc[gbit] >= 0 ? loc[gbit] : 64 + gbit); };
-        if (f.type == MOP_GRAD) {
+        if (f.type == MOP_GRADP) {
+          m.nsel = 1;
+          m.active = uint32_t(p.grad_slots.size());
+          p.grad_slots.push_back(f.slot);
+          m.r0 = int16_t(regidx(f.tgt[0]));
+          m.r1 = int16_t(f.pauli);
+          m.conj = int16_t(f.neg ? 1 : 0);
+        } else if (f.type == MOP_GRAD) {
           m.nsel = int16_t(f.nb);
           m.active = uint32_t(p.grad_slots.size());
           p.grad_slots.push_back(f.slot);
@@ -1182,9 +1210,13 @@ int get_schedule_ex(mb_circuit c, int n, int dm, int adjoint, int lo, int hi, in
   if (hi < 0) hi = int(c->ops.size());
   Tuning tu = tuning_for(N);
   if (adjoint) {
-    tu.t = std::min(tu.t, 11);  // y and delta tiles, double-buffered
-    tu.R = 4;                   // register width of the dual-state passes (MB_ADJOINT_REG_BITS: 3..4)
+    // y and delta tiles, double-buffered: MB_ADJOINT_TILE_BITS (8..11) and the register width of
+    // the dual-state passes MB_ADJOINT_REG_BITS (3..4)
+    tu.t = std::min(tu.t, 11);
+    tu.R = 4;
+    if (const char* e = getenv("MB_ADJOINT_TILE_BITS")) tu.t = std::max(8, std::min(11, atoi(e)));
     if (const char* e = getenv("MB_ADJOINT_REG_BITS")) tu.R = std::max(3, std::min(4, atoi(e)));
+    tu.t = std::min(tu.t, N);
   }
   for (Schedule* s : c->scheds)
     if (s->N == N && s->dm == dm && !s->dagger && s->t == tu.t && s->R == tu.R && s->nsamples == nsamples &&
@@ -1223,7 +1255,8 @@ int get_schedule_ex(mb_circuit c, int n, int dm, int adjoint, int lo, int hi, in
     const int R = p.kind == PASS_REG ? p.t : S->R;
     for (const MOp& m : p.mops) {
       const bool needs = m.type == MOP_U1 || m.type == MOP_CTRL || m.type == MOP_CTRLX || m.type == MOP_U2 ||
-                         m.type == MOP_GRAD || m.type == MOP_RROT || m.type == MOP_IROT || m.type == MOP_LIFT;
+                         m.type == MOP_GRAD || m.type == MOP_RROT || m.type == MOP_IROT || m.type == MOP_LIFT ||
+                         m.type == MOP_GRADP;
       const bool two = m.type == MOP_U2 || (m.type == MOP_GRAD && m.nsel == 2);
       if (needs && (m.r0 < 0 || m.r0 >= R || (two && (m.r1 <= m.r0 || m.r1 >= R)))) {
         set_error("internal scheduling error: micro-op %d without a register target", int(m.type));
@@ -1306,6 +1339,16 @@ static int tile_ctas(int t) {
   return std::max(1, std::min(cap, int((227 * 1024) / (shm + 256))));
 }
 
+// CTAs per SM of a dual-state adjoint pass: what shared memory holds of four double-buffered
+// tiles plus the gradient slots (allowing 8 KB), capped at MB_ADJOINT_CTAS (default 1); the
+// kernel's launch bounds ask the compiler to fit that many CTAs in the register file.
+static int adjoint_ctas(int t) {
+  const size_t shm = (size_t(64) << t) + 1024 + 8 * 1024;
+  int cap = 1;
+  if (const char* e = getenv("MB_ADJOINT_CTAS")) cap = std::max(1, std::min(4, atoi(e)));  // gpart holds 4 per SM
+  return std::max(1, std::min(cap, int((227 * 1024) / (shm + 256))));
+}
+
 static void prepare_jit(Schedule* S) {
   if (S->jit != 0) return;
   S->jit = -1;
@@ -1317,7 +1360,10 @@ static void prepare_jit(Schedule* S) {
   const bool single = S->nsamples == 1;
   for (Pass& p : S->passes) {
     if (p.kind == PASS_TILE && !S->adjoint) p.ctas = tile_ctas(p.t);
-    if (p.kind == PASS_TILE && S->adjoint) src.push_back(jit_adjoint_source(p, S->R, S->N, single));
+    if (p.kind == PASS_TILE && S->adjoint) {
+      p.ctas = adjoint_ctas(p.t);
+      src.push_back(jit_adjoint_source(p, S->R, S->N, single, p.ctas));
+    }
     else if (p.kind == PASS_TILE) src.push_back(jit_tile_source(p, S->R, S->N, single, p.ctas));
     else if (p.kind == PASS_REG) src.push_back(jit_reg_source(p, S->N, single));
     else continue;
@@ -1487,7 +1533,7 @@ int run_adjoint_schedule(mb_circuit c, Schedule* S, double2* y, double2* d, doub
     const size_t shm = (size_t(64) << p.t) + 1024 + sizeof(double) * std::max<size_t>(1, p.grad_slots.size() * nw);
     const int per_sm = std::max(1, int((227 * 1024) / (shm + 256)));
     const int64_t ntiles = int64_t(1) << (N - p.t);
-    const int grid = int(std::min<int64_t>(ntiles, int64_t(g_ctx.sm_count) * std::min(per_sm, 4)));
+    const int grid = int(std::min<int64_t>(ntiles, int64_t(g_ctx.sm_count) * std::min(per_sm, std::max(1, p.ctas))));
     ProfScope ps("k_adjoint_pass_jit", 64.0 * double(elems), st, pass_flops_per_amp(p, true) * double(elems));
     rc = jit_launch_adjoint((CUfunction)p.jit_fn, &my, &md, c->d_table, 0, ntiles, ntiles, g_ctx.flags + 2, gpart, gcount,
                             d_grad, S->d_gslots + p.grad_off, threads, shm, grid, st);
@@ -1595,7 +1641,30 @@ extern "C" int mb_schedule_info(const mb_op* ops, size_t nops, int n, int dm, in
   mb::build_schedule(S, nsamples);
   if (const char* dir = getenv("MB_JIT_DUMP")) {
     // Development aid: the specialised kernel source of every pass (compiled offline to read
-    // register and spill counts).
+    // register and spill counts); with MB_JIT_DUMP_ADJOINT the dual-state passes of the
+    // circuit's reverse sweep (pure states) as well.
+    if (getenv("MB_JIT_DUMP_ADJOINT") && !dm) {
+      mb::Schedule A;
+      A.N = N;
+      A.t = std::min(std::min(tile_bits, 11), N);
+      A.R = 4;
+      if (const char* e = getenv("MB_ADJOINT_REG_BITS")) A.R = std::max(3, std::min(4, atoi(e)));
+      A.adjoint = 1;
+      if (mb::build_adjoint_fops(&c, 0, int(c.ops.size()), A.fops)) {
+        mb::build_schedule(A, 1, false);
+        int j = 0;
+        for (mb::Pass& ps : A.passes) {
+          if (ps.kind != mb::PASS_TILE) continue;
+          const std::string src = mb::jit_adjoint_source(ps, A.R, N, true, mb::adjoint_ctas(ps.t));
+          char path[512];
+          snprintf(path, sizeof(path), "%s/adj_%03d.cu", dir, j++);
+          if (FILE* f = fopen(path, "w")) {
+            fwrite(src.data(), 1, src.size(), f);
+            fclose(f);
+          }
+        }
+      }
+    }
     int i = 0;
     for (mb::Pass& ps : S.passes) {
       std::string src;

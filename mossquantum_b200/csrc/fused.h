@@ -22,6 +22,9 @@ enum MopType : int16_t {
                   // Re off[3], Im off[2], Im off[1]
   MOP_LIFT = 9,   // real rotation [[c,-s],[s,c]] (c >= 0) on r0 as three shears,
                   // x -= t*y; y += s*x; x -= t*y with off[0] = (-t, s), t = s/(1+c)
+  MOP_GRADP = 10, // adjoint sweep: Re<y|D|delta> on register bit r0 for a constant generator of
+                  // a rotation family, D = (i/2)X, (i/2)Y, (i/2)Z or diag(0, -i) (r1 = 1..4),
+                  // negated when conj = 1 (adjoint gates); active = accumulator index
 };
 
 // Matrix offsets with this bit set index the schedule's own table of derived coefficients

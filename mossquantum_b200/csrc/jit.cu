@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <functional>
@@ -316,24 +317,45 @@ struct StageGen {
         break;
       }
       case MOP_DIAG: {
-        // index = compile-time register part | runtime part
+        // Factor index = register part (known here) | runtime part (thread or tile bits). For
+        // every register part the factor is chosen among the runtime combinations with selects,
+        // so nothing is indexed at run time (no local-memory array).
         int rk[4];
-        std::string rtpart;
+        std::vector<int> rtsel;
         for (int c = 0; c < m.nsel; ++c) {
           rk[c] = regbit(m.sel[c]);
-          if (rk[c] < 0) rtpart += (rtpart.empty() ? "" : " | ") + std::string("(") + rt(m.sel[c]) + " << " + std::to_string(c) + ")";
+          if (rk[c] < 0) rtsel.push_back(c);
         }
-        o << "{ double2 F[8]; ";
+        o << "{ ";
         for (int e = 0; e < (1 << m.nsel); ++e)
-          o << "F[" << e << "] = " << (((m.active >> e) & 1) ? ldm(m, e) : std::string("make_double2(1.0, 0.0)")) << "; ";
-        o << "const u32 ri = " << (rtpart.empty() ? std::string("0u") : rtpart) << ";\n";
+          if ((m.active >> e) & 1) o << "const double2 F" << e << " = " << ldm(m, e) << "; ";
+        for (size_t r = 0; r < rtsel.size(); ++r) o << "const bool r" << r << " = " << rt(m.sel[rtsel[r]]) << " != 0u; ";
+        o << "\n";
+        int ctmask = 0;
+        for (int c = 0; c < m.nsel; ++c)
+          if (rk[c] >= 0) ctmask |= 1 << c;
+        // factor expression for register part ct: a select tree over the runtime bits
+        std::function<std::string(int, size_t)> fexpr = [&](int idx, size_t r) -> std::string {
+          if (r == rtsel.size())
+            return ((m.active >> idx) & 1) ? "F" + std::to_string(idx) : std::string("make_double2(1.0, 0.0)");
+          const std::string a = fexpr(idx, r + 1), b = fexpr(idx | (1 << rtsel[r]), r + 1);
+          return a == b ? a : "(r" + std::to_string(r) + " ? " + b + " : " + a + ")";
+        };
+        std::map<int, std::string> gname;
         for (int j = 0; j < A; ++j) {
           int ct = 0;
           for (int c = 0; c < m.nsel; ++c)
             if (rk[c] >= 0 && ((j >> rk[c]) & 1)) ct |= 1 << c;
-          // With every selector in registers the factor index is known here: skip factors of 1.
-          if (rtpart.empty() && !((m.active >> ct) & 1)) continue;
-          o << "  " << v(j) << " = cmul(F[" << ct << "u | ri], " << v(j) << ");\n";
+          // factors of 1 for every runtime combination: nothing to do
+          bool any = false;
+          for (int rc = 0; rc < (1 << m.nsel); ++rc)
+            if ((rc & ctmask) == ct && ((m.active >> rc) & 1)) any = true;
+          if (!any) continue;
+          if (!gname.count(ct)) {
+            gname[ct] = "G" + std::to_string(ct);
+            o << "  const double2 " << gname[ct] << " = " << fexpr(ct, 0) << ";\n";
+          }
+          o << "  " << v(j) << " = cmul(" << gname[ct] << ", " << v(j) << ");\n";
         }
         o << "}\n";
         break;
@@ -591,7 +613,33 @@ static void emit_grad(std::ostringstream& o, const MOp& m, const StageGen& gy, c
     return "ld(" + tabn + " + " + std::to_string(m.off[e]) + ")";
   };
   o << "{ double gs = 0.0;\n";
-  if (m.nsel == 1) {
+  if (m.type == MOP_GRADP) {
+    // Constant generators: (i/2)X, (i/2)Y, (i/2)Z, diag(0, -i); Re<y|D|delta> per pair.
+    const int b = 1 << m.r0;
+    for (int j = 0; j < A; ++j)
+      if (!(j & b)) {
+        const std::string y0 = gy.v(j), y1 = gy.v(j | b), d0 = gd.v(j), d1 = gd.v(j | b);
+        switch (m.r1) {
+          case 1:
+            o << "  gs = fma(" << y0 << ".y, " << d1 << ".x, gs); gs = fma(-" << y0 << ".x, " << d1 << ".y, gs); gs = fma("
+              << y1 << ".y, " << d0 << ".x, gs); gs = fma(-" << y1 << ".x, " << d0 << ".y, gs);\n";
+            break;
+          case 2:
+            o << "  gs = fma(" << y0 << ".x, " << d1 << ".x, gs); gs = fma(" << y0 << ".y, " << d1 << ".y, gs); gs = fma(-"
+              << y1 << ".x, " << d0 << ".x, gs); gs = fma(-" << y1 << ".y, " << d0 << ".y, gs);\n";
+            break;
+          case 3:
+            o << "  gs = fma(" << y0 << ".y, " << d0 << ".x, gs); gs = fma(-" << y0 << ".x, " << d0 << ".y, gs); gs = fma(-"
+              << y1 << ".y, " << d1 << ".x, gs); gs = fma(" << y1 << ".x, " << d1 << ".y, gs);\n";
+            break;
+          default:
+            o << "  gs = fma(" << y1 << ".x, " << d1 << ".y, gs); gs = fma(-" << y1 << ".y, " << d1 << ".x, gs);\n";
+        }
+      }
+    // the 1/2 of the Pauli generators, and the sign of adjoint gates
+    const double scale = (m.r1 == 4 ? 1.0 : 0.5) * (m.conj ? -1.0 : 1.0);
+    o << "  gs *= " << (scale < 0 ? "-" : "") << (std::abs(scale) == 0.5 ? "0.5" : "1.0") << ";\n";
+  } else if (m.nsel == 1) {
     const int b = 1 << m.r0;
     o << "  const double2 D00 = " << L(0) << ", D10 = " << L(1) << ", D01 = " << L(2) << ", D11 = " << L(3) << ";\n";
     for (int j = 0; j < A; ++j)
@@ -620,7 +668,7 @@ static void emit_grad(std::ostringstream& o, const MOp& m, const StageGen& gy, c
   o << "  if ((tx & 31u) == 0u) gw[" << m.active << " * " << nw << " + (tx >> 5)] += gs;\n}\n";
 }
 
-std::string jit_adjoint_source(const Pass& p, int R, int N, bool stage_params) {
+std::string jit_adjoint_source(const Pass& p, int R, int N, bool stage_params, int ctas) {
   std::ostringstream o;
   const int A = 1 << R;
   const int threads = 1 << (p.t - R);
@@ -629,9 +677,12 @@ std::string jit_adjoint_source(const Pass& p, int R, int N, bool stage_params) {
   const TmaGeom& g = p.geom;
   const SharedMats smats = shared_mats(p, stage_params);
   o << kPrelude << shared_mats_decl(smats);
-  o << "extern \"C\" __global__ void __launch_bounds__(" << threads << ", 1) mbk_adj(const __grid_constant__ TMap tmy, "
+  o << "extern \"C\" __global__ void __launch_bounds__(" << threads << ", " << std::max(1, ctas)
+    << ") mbk_adj(const __grid_constant__ TMap tmy, "
     << "const __grid_constant__ TMap tmd, const double2* __restrict__ tab, long long tstride, long long tps, "
     << "long long ntiles, u32* err, double* gpart, u32* gcount, double* gout, const int* __restrict__ gslot) {\n";
+  // reverse sweeps use no derived coefficients (their gates stay in the circuit's table)
+  o << "  const double2* __restrict__ xtab = nullptr; (void)xtab;\n";
   o << "  extern __shared__ unsigned char smem_raw[];\n  __shared__ __align__(8) u64 bar[2];\n  __shared__ int s_abort;\n"
     << "  __shared__ bool lastcta;\n";
   o << shared_mats_fill(smats);
@@ -707,7 +758,7 @@ std::string jit_adjoint_source(const Pass& p, int R, int N, bool stage_params) {
     for (int j = 0; j < A; ++j) gy.nm[j] = gd.nm[j] = j;
     for (int q = 0; q < sd.nops; ++q) {
       const MOp& m = p.mops[sd.op0 + q];
-      if (m.type == MOP_GRAD) {
+      if (m.type == MOP_GRAD || m.type == MOP_GRADP) {
         emit_grad(o, m, gy, gd, R, nw);
       } else {
         gy.emit(m);

@@ -19,7 +19,7 @@ int jit_prepare(std::vector<std::string>& sources, std::vector<CUfunction>& out,
                 double budget_s = 0);
 int jit_launch_tile(CUfunction fn, const CUtensorMap* map, const double2* tab, const double2* xtab, int64_t tstride,
                     int64_t tps, int64_t ntiles, unsigned* err, int threads, size_t shm, int grid, cudaStream_t st);
-std::string jit_adjoint_source(const Pass& p, int R, int N, bool stage_params);
+std::string jit_adjoint_source(const Pass& p, int R, int N, bool stage_params, int ctas = 1);
 int jit_launch_adjoint(CUfunction fn, const CUtensorMap* my, const CUtensorMap* md, const double2* tab, int64_t tstride,
                        int64_t tps, int64_t ntiles, unsigned* err, double* gpart, unsigned* gcount, double* gout,
                        const int* gslot, int threads, size_t shm, int grid, cudaStream_t st);
