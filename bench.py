@@ -42,6 +42,8 @@ def parse():
     ap.add_argument("--layers", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the batch (config 2) and serving (config 4) measurements of the default run")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--case", default="all", help="kernel workload: one of " + ", ".join(KERNEL_CASES) + " or all")
     ap.add_argument("--workload", default="scale", choices=["scale", "batch", "grad", "serve", "kernel"],
@@ -246,13 +248,14 @@ def reference_arm(args):
     return 0
 
 
-def batch_workload(args):
+def batch_measure(steps=3, warmup=2, per_size=3, dm_samples=4):
     """Uneven batch: 512 pure states with n uniform in 10..22 running the hardware-efficient
     ansatz (depth 8) with per-sample angles, plus 64 ten-qubit density matrices with
     depolarizing (p=0.01) and amplitude damping (gamma=0.02) after every gate; output <XXZ>
-    per sample. One step = one evaluation of the whole batch through a BatchPlan (one CUDA
-    graph launch). The plain per-call path (each sample alone, one plain kernel per gate) is
-    timed on a bounded sample of the same workload."""
+    per sample. One step = one evaluation of the whole batch through BatchPlans (CUDA graph
+    replays). The plain per-call path (each sample alone, one plain kernel per gate) is timed
+    on a stratified sample: `per_size` samples of every qubit count and `dm_samples` density
+    matrices, each size's mean time weighted by its count in the batch."""
     import torch
     import mossquantum_b200 as mq
     from mossquantum_b200 import _native as N
@@ -266,71 +269,83 @@ def batch_workload(args):
     groups = {n: (W.hea_circuit(n, depth), B) for n, B in counts.items()}
     dm_groups = {10: (W.hea_circuit(10, depth, noise=(0.01, 0.02)), 64)}
     t0 = time.perf_counter()
-    log("building the pure-state plan")
     plan = BatchPlan(groups, W.xxz, autotune=True)
-    log(f"pure plan ready after {time.perf_counter() - t0:.1f} s; building the density plan")
     plan_dm = BatchPlan(dm_groups, W.xxz, kind="density", autotune=True)
     prep_s = time.perf_counter() - t0
-    log(f"plans ready after {prep_s:.1f} s")
+    log(f"batch: plans ready after {prep_s:.1f} s")
+
     def thetas(gr, seed):
         r = np.random.default_rng(seed)
         return {n: r.uniform(0, 2 * np.pi, size=(B, c.nparameters())) for n, (c, B) in gr.items()}
     th, thd = thetas(groups, 1), thetas(dm_groups, 2)
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         plan.run(th)
         plan_dm.run(thd)
     stream = torch.cuda.ExternalStream(N.stream_handle())
     l0 = N.launch_count()
-    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start, mid, end = (torch.cuda.Event(enable_timing=True) for _ in range(3))
     with ClockSampler(0) as clk:
         t1 = time.perf_counter()
-        start.record(stream)
-        for _ in range(args.steps):
+        pure_ms = dm_ms = 0.0
+        for _ in range(steps):
+            start.record(stream)
             plan.run(th)
+            mid.record(stream)
             plan_dm.run(thd)
-        end.record(stream)
-        end.synchronize()
-        wall = (time.perf_counter() - t1) / args.steps
-    ms_step = start.elapsed_time(end) / args.steps
-    log(f"timed {args.steps} steps: {ms_step:.2f} ms per step; timing the plain path")
+            end.record(stream)
+            end.synchronize()
+            pure_ms += start.elapsed_time(mid)
+            dm_ms += mid.elapsed_time(end)
+        wall = (time.perf_counter() - t1) / steps
+    ms_step = (pure_ms + dm_ms) / steps
+    launches = N.launch_count() - l0
     evals = 512 + 64
-    # plain per-call path on a bounded sample (uniform over the same sizes), extrapolated per sample
-    sub = {}
+    # plain per-call path: stratified sample
+    plain_s = {}
     for n in sorted(counts):
-        sub[n] = (groups[n][0], min(counts[n], max(1, args.plain_samples * counts[n] // 512)))
-    nsub = sum(b for _, b in sub.values())
-    run_plain(sub, W.xxz, {n: th[n][:b] for n, (c, b) in sub.items()})
-    N.synchronize()
-    t2 = time.perf_counter()
-    run_plain(sub, W.xxz, {n: th[n][:b] for n, (c, b) in sub.items()})
-    N.synchronize()
-    plain_per_eval = (time.perf_counter() - t2) / nsub
-    # weight plain time by the full size distribution
-    per_size = {}
-    for n, (c, b) in sub.items():
-        t3 = time.perf_counter()
-        run_plain({n: (c, 1)}, W.xxz, {n: th[n][:1]})
+        b = min(per_size, counts[n])
+        run_plain({n: (groups[n][0], 1)}, W.xxz, {n: th[n][:1]})      # warm this size
         N.synchronize()
-        per_size[n] = time.perf_counter() - t3
-    t4 = time.perf_counter()
-    run_plain({10: (dm_groups[10][0], 2)}, W.xxz, {10: thd[10][:2]}, kind="density")
+        t2 = time.perf_counter()
+        run_plain({n: (groups[n][0], b)}, W.xxz, {n: th[n][:b]})
+        N.synchronize()
+        plain_s[n] = (time.perf_counter() - t2) / b
+    run_plain({10: (dm_groups[10][0], 1)}, W.xxz, {10: thd[10][:1]}, kind="density")
     N.synchronize()
-    dm_plain = (time.perf_counter() - t4) / 2
-    plain_total = sum(per_size[n] * counts[n] for n in counts) + 64 * dm_plain
-    line = {"metric": "circuit-evals/s (uneven batch, per-sample parameters)", "value": evals / (ms_step / 1e3),
-            "unit": "evals/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+    t4 = time.perf_counter()
+    run_plain({10: (dm_groups[10][0], dm_samples)}, W.xxz, {10: thd[10][:dm_samples]}, kind="density")
+    N.synchronize()
+    dm_plain = (time.perf_counter() - t4) / dm_samples
+    plain_total = sum(plain_s[n] * counts[n] for n in counts) + 64 * dm_plain
+    log(f"batch: {ms_step:.1f} ms per step, plain per-call {plain_total * 1e3:.0f} ms per batch")
+    return {"evals_per_s": evals / (ms_step / 1e3), "ms_per_step": ms_step, "pure_ms_per_step": pure_ms / steps,
+            "density_ms_per_step": dm_ms / steps, "evals_per_step": evals, "steps": steps, "warmup": warmup,
+            "sizes": counts, "plan_build_s": prep_s,
+            "autotuned": {str(k): list(v) for k, v in {**plan.tuned, **plan_dm.tuned}.items()},
+            "plain_per_call": {"evals_per_s": evals / plain_total, "seconds_per_batch": plain_total,
+                               "sample": f"{per_size} samples per qubit count (10..22) and {dm_samples} density "
+                                         f"matrices, each timed alone; weighted by the batch's size mix"},
+            "speedup_vs_plain": plain_total / (ms_step / 1e3),
+            "e2e": {"evals_per_s": evals / wall, "h2d_bytes_per_step": int(8 * sum(
+                c.nparameters() * B for c, B in list(groups.values()) + list(dm_groups.values()))),
+                "d2h_bytes_per_step": 16 * evals},
+            "gpu_launches": launches, "clocks": clk.summary()}
+
+
+def batch_workload(args):
+    r = batch_measure(args.steps, args.warmup)
+    line = {"metric": "circuit-evals/s (uneven batch, per-sample parameters)", "value": r["evals_per_s"],
+            "unit": "evals/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "complex128 (f64)",
             "data": "synthetic (seeded)",
             "config": {"workload": "512 pure (n=10..22, HEA depth 8) + 64 density (n=10, noisy) <XXZ>",
-                       "sizes": counts, "plan_build_s": prep_s,
-                       "autotuned": {str(k): list(v) for k, v in {**plan.tuned, **plan_dm.tuned}.items()}},
-            "plain_per_call": {"value": evals / plain_total, "unit": "evals/s", "seconds_per_batch": plain_total,
-                               "sample": f"{nsub} pure samples + 2 density samples timed, weighted by the size mix"},
-            "speedup_vs_plain": plain_total / (ms_step / 1e3),
-            "e2e": {"value": evals / wall, "unit": "evals/s", "h2d_bytes_per_step": int(8 * sum(
-                c.nparameters() * B for c, B in list(groups.values()) + list(dm_groups.values()))),
-                "d2h_bytes_per_step": 16 * evals},
-            "gpu_launches": N.launch_count() - l0, "clocks": clk.summary()}
+                       "sizes": r["sizes"], "plan_build_s": r["plan_build_s"], "autotuned": r["autotuned"]},
+            "pure_ms_per_step": r["pure_ms_per_step"], "density_ms_per_step": r["density_ms_per_step"],
+            "plain_per_call": r["plain_per_call"], "speedup_vs_plain": r["speedup_vs_plain"],
+            "e2e": {"value": r["e2e"]["evals_per_s"], "unit": "evals/s",
+                    "h2d_bytes_per_step": r["e2e"]["h2d_bytes_per_step"],
+                    "d2h_bytes_per_step": r["e2e"]["d2h_bytes_per_step"]},
+            "gpu_launches": r["gpu_launches"], "clocks": r["clocks"]}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -728,6 +743,29 @@ def main():
                          f"of the reference CPU method, host-native build)",
                "anchor": cpu_anchor(threads)}
 
+    # The rest of the headline metric on the same run: circuit-evals/s of the uneven batch against
+    # the plain per-call path, and serving p50/p99 and evals/s at a saturating request stream
+    # against the plain per-request path replaying the same arrivals (single replica only).
+    extras = None
+    if not args.no_extras and world == 1:
+        extras = {}
+        b = batch_measure(steps=3, warmup=2)
+        extras["batch"] = {"workload": "512 pure (n=10..22, HEA depth 8, per-sample angles) + 64 density (n=10, "
+                                       "noisy) <XXZ>, one CUDA-graph replay per plan",
+                           "evals_per_s": b["evals_per_s"], "ms_per_step": b["ms_per_step"],
+                           "pure_ms_per_step": b["pure_ms_per_step"], "density_ms_per_step": b["density_ms_per_step"],
+                           "plain_per_call_evals_per_s": b["plain_per_call"]["evals_per_s"],
+                           "plain_sample": b["plain_per_call"]["sample"], "speedup_vs_plain": b["speedup_vs_plain"],
+                           "e2e_evals_per_s": b["e2e"]["evals_per_s"], "plan_build_s": b["plan_build_s"],
+                           "gpu_launches": b["gpu_launches"], "clocks": b["clocks"]}
+        srv = serve_measure(200, None, seed_stream=0)
+        extras["serving"] = {"workload": "200 requests arriving at once (saturating): 70% pure 8..26q, 30% density "
+                                         "6..12q (noisy), 4..32 layers, TFIM/XXZ, 50% adjoint gradients",
+                             "server": srv["server"], "plain_per_request": srv.get("plain_per_request"),
+                             "speedup_evals_per_s": srv.get("speedup_evals_per_s"),
+                             "max_abs_diff_vs_plain": srv.get("max_abs_diff_vs_plain"),
+                             "gpu_launches": srv["gpu_launches"], "clocks": srv["clocks"]}
+
     if rank == 0:
         line = {"metric": "gate-kernel HBM GB/s (effective, plain per-gate bytes)", "value": value, "unit": "GB/s",
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
@@ -736,8 +774,13 @@ def main():
                 "config": {"workload": f"u3_cz_brickwork n={n} layers={depth}", "qubits": n, "layers": depth,
                            "state_bytes": 16 << n, "variant": args.variant, "parallelism": f"replicas x{world}",
                            "l2": "state (4 GiB) is larger than L2; no flush needed"},
-                "layers_per_s": world * depth / (ms_step / 1e3), "roofline": roofline, "cpu_baseline": cpu,
-                "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary()}
+                "layers_per_s": world * depth / (ms_step / 1e3),
+                "value_note": "value counts the bytes the plain per-gate method would move (one sweep per gate); "
+                              "the fused passes move 32*2^n bytes per pass, see hbm_measured",
+                "hbm_measured": ({"gbs": roofline["hbm"]["achieved"], "frac": roofline["hbm"]["frac"],
+                                  "peak": roofline["hbm"]["peak"], "kernel": roofline["kernel"]} if roofline else None),
+                "roofline": roofline, "cpu_baseline": cpu,
+                "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(), "extras": extras}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
