@@ -27,6 +27,8 @@
 #include <mutex>
 
 #include "fused_kernels.cuh"
+#include "family.cuh"
+#include "fusemat.cuh"
 #include "jit.h"
 
 namespace mb {
@@ -121,7 +123,8 @@ __global__ void __launch_bounds__(TileBounds<R>::threads, TileBounds<R>::blocks)
       double2 v[1 << R];
 #pragma unroll
       for (int j = 0; j < (1 << R); ++j) v[j] = tl[fk::swz(lbase | uint32_t(fk::reg_offset<R>(j, reg)))];
-      fk::run_mops<R, U2>(v, a.mops + sd.op0, sd.nops, lbase, reg, base, a.table, a.xtab, a.tstride, b);
+      fk::run_mops<R, U2>(v, a.mops + sd.op0, sd.nops, lbase, reg, base, a.table, a.xtab, a.xtabs + b * a.xrow,
+                          a.tstride, b);
 #pragma unroll
       for (int j = 0; j < (1 << R); ++j) tl[fk::swz(lbase | uint32_t(fk::reg_offset<R>(j, reg)))] = v[j];
       __syncthreads();
@@ -152,10 +155,25 @@ __global__ void __launch_bounds__(128) k_reg_pass(double2* __restrict__ v, const
     double2 x[1 << R];
 #pragma unroll
     for (int j = 0; j < (1 << R); ++j) x[j] = vs[base | fk::reg_offset<R>(j, reg)];
-    fk::run_mops<R, U2>(x, a.mops, a.nops, base, reg, 0, a.table, a.xtab, a.tstride, b);
+    fk::run_mops<R, U2>(x, a.mops, a.nops, base, reg, 0, a.table, a.xtab, a.xtabs + b * a.xrow, a.tstride, b);
 #pragma unroll
     for (int j = 0; j < (1 << R); ++j) vs[base | fk::reg_offset<R>(j, reg)] = x[j];
   }
+}
+
+// Per-sample products of the fused single-qubit runs (after binding): row b of the derived
+// table's per-sample region gets every record's product formed from table row b.
+__global__ void k_fuse(const FuseRec* __restrict__ recs, int nrecs, const FuseComp* __restrict__ comps,
+                       const double2* __restrict__ table, int64_t tstride, double2* __restrict__ xs, int64_t xrow,
+                       int rows) {
+  const int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (idx >= int64_t(nrecs) * rows) return;
+  const int b = int(idx / nrecs);
+  const FuseRec r = recs[idx % nrecs];
+  double2 M[16];
+  fuse_product(r, comps, table, table + int64_t(b) * tstride, M);
+  double2* out = xs + int64_t(b) * xrow + r.out;
+  for (int e = 0; e < r.d * r.d; ++e) out[e] = M[e];
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -193,8 +211,14 @@ struct FOp {
 };
 
 struct Schedule {
-  std::vector<double2> xtab;      // derived coefficients (kXtabFlag offsets)
-  double2* d_xtab = nullptr;
+  std::vector<double2> xtab;      // derived coefficients (kXtabFlag offsets), the same for every sample
+  double2* d_xtab = nullptr;      // xtab, then nsamples rows of xrow per-sample entries
+  int xrow = 0;                   // per-sample entries (fused products) per row
+  bool fuse = true;               // bind-time fusion of single-qubit runs
+  std::vector<FuseComp> fcomps;   // per-sample fusion records, formed by k_fuse after binding
+  std::vector<FuseRec> frecs;
+  FuseComp* d_fcomps = nullptr;
+  FuseRec* d_frecs = nullptr;
   int N = 0, dm = 0, t = 0, R = 0, nsamples = 1;
   int lo = 0, hi = -1;  // instruction range [lo, hi) of the circuit
   int adjoint = 0;      // reverse sweep with gradient accumulators
@@ -496,20 +520,20 @@ static void merge_phases(std::vector<FOp>& seq, bool dm, std::vector<double2>* x
   seq.swap(out);
 }
 
-// One half of a fixed single-qubit gate (xt != nullptr, forward): a general unitary becomes
-// phase, three-shear rotation, phase (and a global factor); a diagonal becomes a phase and a
-// global factor. The phases are marked for merge_phases. Returns false to keep `f` as it is.
-static bool split_fixed_1q(mb_circuit c, const COp& op, const FOp& f, bool dm, std::vector<double2>* xt,
-                           std::vector<FOp>& seq) {
-  if (op.kind != MB_OP_GATE || op.k != 1 || op.parametric) return false;
-  const double2* M = c->fixed_table.data();
+// A fixed single-qubit op of a forward schedule (a gate half, or a fused run formed on the host):
+// a general unitary becomes phase, three-shear rotation, phase (and a global factor); a diagonal
+// becomes a phase and a global factor. The phases are marked for merge_phases. Returns false to
+// keep `f` as it is.
+static bool split_fixed_1q(mb_circuit c, const FOp& f, bool dm, std::vector<double2>* xt, std::vector<FOp>& seq) {
+  if (f.param || f.type == F_UNFUSABLE) return false;
   auto eff = [&](int e) {
-    const double2 x = M[f.off[e]];
+    const int off = f.off[e];
+    const double2 x = (off & kXtabFlag) ? (*xt)[off & ~kXtabFlag] : c->fixed_table[off];
     return cd(x.x, f.conj ? -x.y : x.y);
   };
   const int q = f.bits[0];
   if (f.type == MOP_DIAG && f.nb == 1) {
-    const cd d0 = eff(0), d1 = eff(1);
+    const cd d0 = (f.active & 1) ? eff(0) : cd(1, 0), d1 = (f.active & 2) ? eff(1) : cd(1, 0);
     if (!(std::abs(d0) > 0.0)) return false;
     if (dm && (std::abs(std::abs(d0) - 1.0) > 1e-14 || std::abs(std::abs(d1) - 1.0) > 1e-14)) return false;
     FOp p;
@@ -528,7 +552,7 @@ static bool split_fixed_1q(mb_circuit c, const COp& op, const FOp& f, bool dm, s
     seq.push_back(p);
     return true;
   }
-  if (f.type != MOP_U1) return false;
+  if (f.type != MOP_U1 || f.nctrl != 0 || f.nb != 1) return false;
   const cd E[4] = {eff(0), eff(1), eff(2), eff(3)};
   cd g, A, B;
   double mt, sn;
@@ -557,15 +581,137 @@ static bool split_fixed_1q(mb_circuit c, const COp& op, const FOp& f, bool dm, s
   return true;
 }
 
-// xt: the schedule's derived table; when given (forward schedules), fixed single-qubit gates
-// are split into phases and shear rotations and the phases are merged.
+// Bind-time fusion (forward schedules): every maximal run of ops that act only on qubit q (pure:
+// bit q; density matrices: bits q and q + n) and that no other op on q interrupts becomes one
+// 2x2 (pure) or 4x4 (density) op placed at the run's last member (the ops it passes act on other
+// qubits and commute with the run). Runs of fixed ops are multiplied here; runs with a
+// parametric member get a FuseRec that k_fuse evaluates per sample after binding. Density-matrix
+// runs are fused only when they hold a channel or three or more ops (two gate halves cost the
+// same as one 4x4, and fixed halves are cheaper split).
+static void fuse_runs(mb_circuit c, std::vector<FOp>& seq, int n, bool dm, Schedule* S) {
+  const int nq = n;
+  std::vector<std::vector<int>> open(nq);
+  std::vector<char> drop(seq.size(), 0);
+  std::vector<std::pair<int, FOp>> repl;
+  auto anchor_mask = [&](int q) { return (uint64_t(1) << q) | (dm ? uint64_t(1) << (q + n) : 0); };
+  auto fusable = [&](const FOp& f, int* q) {
+    int b = -1;
+    switch (f.type) {
+      case MOP_U1: case MOP_RROT: case MOP_IROT: case MOP_CTRLX: b = f.nctrl == 0 ? f.tgt[0] : -1; break;
+      case MOP_DIAG: b = f.nb == 1 ? f.bits[0] : -1; break;
+      case MOP_CPHASE: b = f.nctrl == 1 ? f.ctrl[0] : -1; break;
+      case MOP_U2:
+        if (dm && f.nb == 2 && f.bits[1] == f.bits[0] + n && f.bits[0] < n) {
+          *q = f.bits[0];
+          return true;
+        }
+        return false;
+      default: return false;
+    }
+    if (b < 0) return false;
+    *q = dm ? (b < n ? b : b - n) : b;
+    return *q >= 0 && *q < nq;
+  };
+  auto close = [&](int q) {
+    std::vector<int>& g = open[q];
+    bool channel = false, param = false;
+    for (int i : g) {
+      channel |= seq[i].type == MOP_U2;
+      param |= seq[i].param != 0;
+    }
+    const bool worth = dm ? (channel || g.size() >= 3) : g.size() >= 2;
+    if (!worth) {
+      g.clear();
+      return;
+    }
+    const int d = dm ? 4 : 2;
+    FuseRec rec{0, d, int(S->fcomps.size()), 0};
+    std::vector<FuseComp> comps;
+    for (int i : g) {
+      const FOp& m = seq[i];
+      FuseComp fc{};
+      fc.conj = int8_t(m.conj);
+      fc.param = int8_t(m.param);
+      fc.bit = int8_t(dm && m.type != MOP_U2 && m.bits[0] >= n ? 1 : 0);
+      if (m.type == MOP_U2) {
+        fc.kind = FC_DENSE4;
+        for (int e = 0; e < 16; ++e) fc.off[e] = m.off[e];
+      } else if (m.type == MOP_DIAG) {
+        fc.kind = FC_DIAG2;
+        fc.active = uint8_t(m.active);
+        fc.off[0] = m.off[0];
+        fc.off[1] = m.off[1];
+      } else if (m.type == MOP_CPHASE) {
+        fc.kind = FC_PHASE2;
+        fc.neg = int8_t(m.neg);
+        fc.off[0] = m.off[0];
+      } else {
+        fc.kind = FC_DENSE2;
+        for (int e = 0; e < 4; ++e) fc.off[e] = m.off[e];
+      }
+      comps.push_back(fc);
+    }
+    rec.nc = int(comps.size());
+    FOp f;
+    f.cls = CLS_DENSE;
+    if (dm) {
+      f.type = MOP_U2;
+      f.nb = 2;
+      f.bits[0] = f.tgt[0] = q;
+      f.bits[1] = f.tgt[1] = q + n;
+      f.ntgt = 2;
+    } else {
+      f.type = MOP_U1;
+      f.nb = 1;
+      f.bits[0] = f.tgt[0] = q;
+      f.ntgt = 1;
+    }
+    if (param) {
+      rec.out = S->xrow;
+      S->xrow += d * d;
+      S->fcomps.insert(S->fcomps.end(), comps.begin(), comps.end());
+      S->frecs.push_back(rec);
+      for (int e = 0; e < d * d; ++e) f.off[e] = (rec.out + e) | kXtabFlag;
+      f.param = 1;
+    } else {
+      rec.c0 = 0;
+      double2 M[16];
+      fuse_product(rec, comps.data(), c->fixed_table.data(), c->fixed_table.data(), M);
+      for (int e = 0; e < d * d; ++e) f.off[e] = xtab_push(&S->xtab, M[e]);
+    }
+    finalize_masks(f);
+    for (size_t k = 0; k + 1 < g.size(); ++k) drop[g[k]] = 1;
+    repl.push_back({g.back(), f});
+    g.clear();
+  };
+  for (size_t i = 0; i < seq.size(); ++i) {
+    int q;
+    if (fusable(seq[i], &q)) {
+      open[q].push_back(int(i));
+      continue;
+    }
+    for (int a = 0; a < nq; ++a)
+      if (!open[a].empty() && (seq[i].all & anchor_mask(a))) close(a);
+  }
+  for (int a = 0; a < nq; ++a)
+    if (!open[a].empty()) close(a);
+  for (auto& r : repl) seq[r.first] = r.second;
+  std::vector<FOp> out;
+  out.reserve(seq.size());
+  for (size_t i = 0; i < seq.size(); ++i)
+    if (!drop[i]) out.push_back(seq[i]);
+  seq.swap(out);
+}
+
+// S: the schedule being built; when given (forward schedules), single-qubit runs are fused at
+// bind time and fixed single-qubit ops are split into phases and shear rotations, with the
+// phases merged.
 static void build_fops(mb_circuit c, int n, int dm, bool dagger, std::vector<FOp>& out, int lo = 0, int hi = -1,
-                       std::vector<double2>* xt = nullptr) {
+                       Schedule* S = nullptr) {
   out.clear();
   std::vector<FOp> seq;
   if (hi < 0) hi = int(c->ops.size());
-  if (dagger) xt = nullptr;
-  if (xt && getenv("MB_NO_SPLIT")) xt = nullptr;
+  if (dagger) S = nullptr;
   for (int oi = lo; oi < hi; ++oi) {
     const COp& op = c->ops[oi];
     if (op.kind == MB_OP_CHANNEL) {
@@ -592,15 +738,22 @@ static void build_fops(mb_circuit c, int n, int dm, bool dagger, std::vector<FOp
       seq.push_back(f);
       continue;
     }
-    for (int half = 0; half < (dm ? 2 : 1); ++half) {
-      const FOp f = gate_fop(c, op, half ? n : 0, half, dagger);
-      if (xt && split_fixed_1q(c, op, f, dm, xt, seq)) continue;
-      seq.push_back(f);
-    }
+    seq.push_back(gate_fop(c, op, 0, 0, dagger));
+    if (dm) seq.push_back(gate_fop(c, op, n, 1, dagger));
   }
   for (FOp& f : seq) mark_unfusable_masks(f);
   if (dagger) std::reverse(seq.begin(), seq.end());
-  if (xt) merge_phases(seq, dm, xt);
+  if (S) {
+    if (S->fuse && !getenv("MB_NO_FUSE")) fuse_runs(c, seq, n, dm, S);
+    if (!getenv("MB_NO_SPLIT")) {
+      std::vector<FOp> split;
+      split.reserve(seq.size() * 2);
+      for (const FOp& f : seq)
+        if (!split_fixed_1q(c, f, dm, &S->xtab, split)) split.push_back(f);
+      merge_phases(split, dm, &S->xtab);
+      seq.swap(split);
+    }
+  }
   out = seq;
 }
 
@@ -1243,7 +1396,7 @@ int get_schedule_ex(mb_circuit c, int n, int dm, int adjoint, int lo, int hi, in
       return MB_EUNSUPPORTED;
     }
   } else {
-    build_fops(c, n, dm, false, S->fops, lo, hi, &S->xtab);
+    build_fops(c, n, dm, false, S->fops, lo, hi, S.get());
   }
   build_schedule(*S, nsamples, !adjoint);
   if (S->unschedulable) {
@@ -1293,10 +1446,21 @@ int get_schedule_ex(mb_circuit c, int n, int dm, int adjoint, int lo, int hi, in
     if ((rc = dev_alloc((void**)&S->d_gslots, sizeof(int) * gs.size()))) return rc;
     MB_CHECK_CUDA(cudaMemcpyAsync(S->d_gslots, gs.data(), sizeof(int) * gs.size(), cudaMemcpyHostToDevice, g_ctx.stream));
   }
-  if (!S->xtab.empty()) {
-    if ((rc = dev_alloc((void**)&S->d_xtab, sizeof(double2) * S->xtab.size()))) return rc;
-    MB_CHECK_CUDA(cudaMemcpyAsync(S->d_xtab, S->xtab.data(), sizeof(double2) * S->xtab.size(), cudaMemcpyHostToDevice,
+  if (!S->xtab.empty() || S->xrow > 0) {
+    // fixed derived entries, then nsamples rows of per-sample fused products
+    const size_t total = S->xtab.size() + size_t(S->xrow) * size_t(nsamples);
+    if ((rc = dev_alloc((void**)&S->d_xtab, sizeof(double2) * std::max<size_t>(1, total)))) return rc;
+    if (!S->xtab.empty())
+      MB_CHECK_CUDA(cudaMemcpyAsync(S->d_xtab, S->xtab.data(), sizeof(double2) * S->xtab.size(), cudaMemcpyHostToDevice,
+                                    g_ctx.stream));
+  }
+  if (!S->frecs.empty()) {
+    if ((rc = dev_alloc((void**)&S->d_frecs, sizeof(FuseRec) * S->frecs.size()))) return rc;
+    if ((rc = dev_alloc((void**)&S->d_fcomps, sizeof(FuseComp) * S->fcomps.size()))) return rc;
+    MB_CHECK_CUDA(cudaMemcpyAsync(S->d_frecs, S->frecs.data(), sizeof(FuseRec) * S->frecs.size(), cudaMemcpyHostToDevice,
                                   g_ctx.stream));
+    MB_CHECK_CUDA(cudaMemcpyAsync(S->d_fcomps, S->fcomps.data(), sizeof(FuseComp) * S->fcomps.size(),
+                                  cudaMemcpyHostToDevice, g_ctx.stream));
   }
   MB_CHECK_CUDA(cudaStreamSynchronize(g_ctx.stream));
   if (!adjoint && S->R == 3 && !getenv("MB_REG_BITS")) {
@@ -1314,6 +1478,8 @@ int get_schedule_ex(mb_circuit c, int n, int dm, int adjoint, int lo, int hi, in
       dev_free(S->d_mops);
       dev_free(S->d_gslots);
       dev_free(S->d_xtab);
+      dev_free(S->d_frecs);
+      dev_free(S->d_fcomps);
       return get_schedule_ex(c, n, dm, adjoint, lo, hi, nsamples, out);
     }
   }
@@ -1411,6 +1577,16 @@ int run_schedule(mb_circuit c, Schedule* S, double2* v, int nsamples, int64_t ms
     set_error("register width %d needs the specialised kernels, which are unavailable", S->R);
     return MB_EUNSUPPORTED;
   }
+  // Per-sample fused products (one row when every sample shares the parameters).
+  double2* xs = S->d_xtab ? S->d_xtab + S->xtab.size() : nullptr;
+  const int64_t xrow = mstride ? S->xrow : 0;
+  if (!S->frecs.empty()) {
+    const int rows = mstride ? nsamples : 1;
+    const int64_t work = int64_t(S->frecs.size()) * rows;
+    k_fuse<<<unsigned((work + 127) / 128), 128, 0, st>>>(S->d_frecs, int(S->frecs.size()), S->d_fcomps, c->d_table,
+                                                          mstride, xs, S->xrow, rows);
+    MB_LAUNCHED();
+  }
   for (const Pass& p : S->passes) {
     int rc = MB_OK;
     if (p.kind == PASS_PLAIN) {
@@ -1434,6 +1610,8 @@ int run_schedule(mb_circuit c, Schedule* S, double2* v, int nsamples, int64_t ms
       a.mops = S->d_mops;
       a.table = c->d_table;
       a.xtab = S->d_xtab;
+      a.xtabs = xs;
+      a.xrow = xrow;
       a.err = g_ctx.flags + 2;
       const int threads = 1 << (p.t - S->R);
       const size_t shm = (size_t(32) << p.t) + 1024;  // two tile buffers + alignment slack
@@ -1443,8 +1621,8 @@ int run_schedule(mb_circuit c, Schedule* S, double2* v, int nsamples, int64_t ms
       if (S->jit == 1 && p.jit_fn) {
         ProfScope ps("k_tile_pass_jit", 32.0 * double(elems) * nsamples, st,
                      pass_flops_per_amp(p, false) * double(elems) * nsamples);
-        rc = jit_launch_tile((CUfunction)p.jit_fn, &map, c->d_table, S->d_xtab, mstride, a.tiles_per_sample, a.ntiles,
-                             a.err, threads, shm, int(grid), st);
+        rc = jit_launch_tile((CUfunction)p.jit_fn, &map, c->d_table, S->d_xtab, xs, xrow, mstride, a.tiles_per_sample,
+                             a.ntiles, a.err, threads, shm, int(grid), st);
         ++launch_counter();
         if (rc) return rc;
         continue;
@@ -1471,13 +1649,16 @@ int run_schedule(mb_circuit c, Schedule* S, double2* v, int nsamples, int64_t ms
       a.mops = S->d_mops + p.mop_off;
       a.table = c->d_table;
       a.xtab = S->d_xtab;
+      a.xtabs = xs;
+      a.xrow = xrow;
       const int64_t work = a.groups * nsamples;
       const int block = 128;
       const int grid = grid_for(work, block, int64_t(g_ctx.sm_count) * 16);
       if (S->jit == 1 && p.jit_fn) {
         ProfScope ps("k_reg_pass_jit", 32.0 * double(elems) * nsamples, st,
                      pass_flops_per_amp(p, false) * double(elems) * nsamples);
-        rc = jit_launch_reg((CUfunction)p.jit_fn, v, c->d_table, S->d_xtab, mstride, a.groups, nsamples, grid, st);
+        rc = jit_launch_reg((CUfunction)p.jit_fn, v, c->d_table, S->d_xtab, xs, xrow, mstride, a.groups, nsamples, grid,
+                            st);
         ++launch_counter();
         if (rc) return rc;
         continue;
@@ -1578,6 +1759,8 @@ void release_schedules(mb_circuit c) {
     dev_free(s->d_mops);
     dev_free(s->d_gslots);
     dev_free(s->d_xtab);
+    dev_free(s->d_frecs);
+    dev_free(s->d_fcomps);
     delete s;
   }
   c->scheds.clear();
@@ -1637,7 +1820,7 @@ extern "C" int mb_schedule_info(const mb_op* ops, size_t nops, int n, int dm, in
   S.t = std::min(tile_bits, N);
   S.R = reg_bits;
   S.nsamples = nsamples;
-  mb::build_fops(&c, n, S.dm, false, S.fops, 0, -1, &S.xtab);
+  mb::build_fops(&c, n, S.dm, false, S.fops, 0, -1, &S);
   mb::build_schedule(S, nsamples);
   if (const char* dir = getenv("MB_JIT_DUMP")) {
     // Development aid: the specialised kernel source of every pass (compiled offline to read
@@ -1703,11 +1886,14 @@ namespace {
 
 typedef std::complex<double> hcd;
 
+// The circuit's bound table (one sample), the schedule's fixed derived entries and this
+// sample's row of per-sample fused products.
 struct HostLowering {
-  const mb_circuit_s* c;
+  const double2* tab;
   const std::vector<double2>* xt;
-  hcd el(int off, int conj) const {
-    const double2 v = (off & kXtabFlag) ? (*xt)[off & ~kXtabFlag] : c->fixed_table[off];
+  const std::vector<double2>* xr;
+  hcd el(int off, int conj, int param = 0) const {
+    const double2 v = (off & kXtabFlag) ? (param ? (*xr)[off & ~kXtabFlag] : (*xt)[off & ~kXtabFlag]) : tab[off];
     return hcd(v.x, conj ? -v.y : v.y);
   }
 };
@@ -1722,7 +1908,7 @@ void host_apply_fop(const HostLowering& L, const FOp& f, std::vector<hcd>& v) {
     std::vector<hcd> M(size_t(d) * d);
     for (int r = 0; r < d; ++r)
       for (int q = 0; q < d; ++q) {
-        const double2 x = L.c->fixed_table[f.mat_off + r + q * d];
+        const double2 x = L.tab[f.mat_off + r + q * d];
         hcd e(x.x, x.y);
         if (f.mode == MAT_CONJ) e = std::conj(e);
         M[r + q * d] = e;
@@ -1776,10 +1962,10 @@ void host_apply_fop(const HostLowering& L, const FOp& f, std::vector<hcd>& v) {
         mt = ts.real();
         sn = ts.imag();
       } else {
-        m00 = L.el(f.off[0], f.conj);
-        m10 = L.el(f.off[1], f.conj);
-        m01 = L.el(f.off[2], f.conj);
-        m11 = L.el(f.off[3], f.conj);
+        m00 = L.el(f.off[0], f.conj, f.param);
+        m10 = L.el(f.off[1], f.conj, f.param);
+        m01 = L.el(f.off[2], f.conj, f.param);
+        m11 = L.el(f.off[3], f.conj, f.param);
         if (f.type == MOP_RROT) {
           m00 = m00.real(); m10 = m10.real(); m01 = m01.real(); m11 = m11.real();
         } else if (f.type == MOP_IROT) {
@@ -1805,7 +1991,7 @@ void host_apply_fop(const HostLowering& L, const FOp& f, std::vector<hcd>& v) {
     }
     case MOP_U2: {
       hcd u[16];
-      for (int e = 0; e < 16; ++e) u[e] = L.el(f.off[e], f.conj);
+      for (int e = 0; e < 16; ++e) u[e] = L.el(f.off[e], f.conj, f.param);
       const int b0 = f.tgt[0], b1 = f.tgt[1];
       for (int64_t i = 0; i < len; ++i) {
         if (bit(i, b0) || bit(i, b1)) continue;
@@ -1824,12 +2010,12 @@ void host_apply_fop(const HostLowering& L, const FOp& f, std::vector<hcd>& v) {
       for (int64_t i = 0; i < len; ++i) {
         int a = 0;
         for (int j = 0; j < f.nb; ++j) a |= bit(i, f.bits[j]) << j;
-        if ((f.active >> a) & 1) v[i] *= L.el(f.off[a], f.conj);
+        if ((f.active >> a) & 1) v[i] *= L.el(f.off[a], f.conj, f.param);
       }
       return;
     }
     case MOP_CPHASE: {
-      const hcd fac = f.neg ? hcd(-1, 0) : L.el(f.off[0], f.conj);
+      const hcd fac = f.neg ? hcd(-1, 0) : L.el(f.off[0], f.conj, f.param);
       for (int64_t i = 0; i < len; ++i)
         if (ctl_ok(i)) v[i] *= fac;
       return;
@@ -1848,7 +2034,7 @@ void host_apply_mop(const HostLowering& L, const Pass& p, const StageDesc& sd, c
   auto gbit_of_reg = [&](int k) { return tile ? p.bits[sd.reg[k]] : sd.reg[k]; };
   auto gbit_of_sel = [&](int sel) { return sel >= 64 ? sel - 64 : (tile ? p.bits[sel] : sel); };
   auto bit = [](int64_t i, int b) { return int((i >> b) & 1); };
-  auto el = [&](int e) { return L.el(m.off[e], m.conj); };
+  auto el = [&](int e) { return L.el(m.off[e], m.conj, m.param); };
   auto sel_ok = [&](int64_t i) {
     for (int j = 0; j < m.nsel; ++j)
       if (!bit(i, gbit_of_sel(m.sel[j]))) return false;
@@ -1939,17 +2125,27 @@ extern "C" int mb_lowering_check(const mb_op* ops, size_t nops, int n, int dm, i
   mb_circuit_s c;
   if (int rc = mb::circuit_compile_host(ops, nops, n, &c)) return rc;
   for (const mb::COp& op : c.ops)
-    if (op.parametric || op.k == 0) {
-      mb::set_error("lowering check: fixed gates and channels only");
+    if (op.k == 0) {
+      mb::set_error("lowering check: zero-qubit gates are not lowered");
       return MB_EUNSUPPORTED;
     }
+  // Bind the parametric instructions on the host (the code k_bind runs), each at its given value.
+  std::vector<double2> tab = c.fixed_table;
+  for (const mb::BindRec& rc : c.binds) mb::bind_record(rc, rc.value, tab.data(), tab.data());
   mb::Schedule S;
   S.N = N;
   S.dm = dm ? 1 : 0;
   S.t = std::min(tile_bits, N);
   S.R = reg_bits;
-  mb::build_fops(&c, n, S.dm, false, S.fops, 0, -1, &S.xtab);
+  mb::build_fops(&c, n, S.dm, false, S.fops, 0, -1, &S);
   mb::build_schedule(S, 1);
+  // this sample's fused products (what k_fuse writes after binding)
+  std::vector<double2> xrow(std::max(1, S.xrow));
+  for (const mb::FuseRec& r : S.frecs) {
+    double2 M[16];
+    mb::fuse_product(r, S.fcomps.data(), tab.data(), tab.data(), M);
+    for (int e = 0; e < r.d * r.d; ++e) xrow[r.out + e] = M[e];
+  }
   // random start vector
   std::vector<mb::hcd> v0(size_t(1) << N);
   uint64_t st = seed * 0x9E3779B97F4A7C15ull + 1;
@@ -1968,19 +2164,19 @@ extern "C" int mb_lowering_check(const mb_op* ops, size_t nops, int n, int dm, i
     if (op.kind == MB_OP_CHANNEL) {
       f.nb = 2 * op.k;
       for (int j = 0; j < op.k; ++j) { f.bits[j] = op.pos[j]; f.bits[j + op.k] = op.pos[j] + n; }
-      mb::host_apply_fop(mb::HostLowering{&c, &S.xtab}, f, ref);
+      mb::host_apply_fop(mb::HostLowering{tab.data(), &S.xtab, &xrow}, f, ref);
       continue;
     }
     f.nb = op.k;
     for (int j = 0; j < op.k; ++j) f.bits[j] = op.pos[j];
-    mb::host_apply_fop(mb::HostLowering{&c, &S.xtab}, f, ref);
+    mb::host_apply_fop(mb::HostLowering{tab.data(), &S.xtab, &xrow}, f, ref);
     if (dm) {
       for (int j = 0; j < op.k; ++j) f.bits[j] = op.pos[j] + n;
       f.mode = mb::MAT_CONJ;
-      mb::host_apply_fop(mb::HostLowering{&c, &S.xtab}, f, ref);
+      mb::host_apply_fop(mb::HostLowering{tab.data(), &S.xtab, &xrow}, f, ref);
     }
   }
-  const mb::HostLowering L{&c, &S.xtab};
+  const mb::HostLowering L{tab.data(), &S.xtab, &xrow};
   std::vector<mb::hcd> a = v0, b = v0, e = v0;
   for (const mb::FOp& f : S.fops) mb::host_apply_fop(L, f, a);
   for (const mb::Pass& p : S.passes)

@@ -227,15 +227,17 @@ __device__ __forceinline__ void cphase_dispatch(double2 (&a)[1 << R], int need, 
 
 // Runs micro-ops [0, nops) on the registers. HAS_U2 = false compiles a lean variant without
 // the 4x4 path (fewer live registers) for passes that hold no two-qubit dense gate.
+// xt0: the schedule's fixed derived entries; xb: this sample's row of per-sample entries.
 template <int R, bool HAS_U2>
 __device__ __forceinline__ void run_mops(double2 (&a)[1 << R], const MOp* __restrict__ mops, int nops,
                                          uint64_t lbase, const int* reg, uint64_t gbase,
-                                         const double2* __restrict__ tab, const double2* __restrict__ xt,
-                                         int64_t tstride, int b) {
+                                         const double2* __restrict__ tab, const double2* __restrict__ xt0,
+                                         const double2* __restrict__ xb, int64_t tstride, int b) {
   for (int q = 0; q < nops; ++q) {
     const MOp* __restrict__ op = mops + q;
     const int type = op->type, r0 = op->r0, nsel = op->nsel, conj = op->conj;
     const double2* m = tab + (op->param ? int64_t(b) * tstride : 0);
+    const double2* xt = op->param ? xb : xt0;
     if (type == MOP_LIFT) {
       const double2 ts = ldm(m, xt, op->off[0], 0);
       switch (r0) {
@@ -446,6 +448,8 @@ struct TileArgs {
   const MOp* mops;
   const double2* table;
   const double2* xtab;     // the schedule's derived coefficients (kXtabFlag offsets)
+  const double2* xtabs;    // per-sample derived entries, row b at xtabs + b * xrow
+  int64_t xrow;
   unsigned* err;
 };
 
@@ -460,6 +464,8 @@ struct RegArgs {
   const MOp* mops;
   const double2* table;
   const double2* xtab;
+  const double2* xtabs;
+  int64_t xrow;
 };
 
 }  // namespace mb

@@ -147,6 +147,14 @@ std::string tma_st(int nd) {
   return o.str();
 }
 
+// Shared-memory staging key of matrix element e of a micro-op: its table offset, with bit 30 set
+// for a per-sample derived entry (those live in their own row region, so their offsets can
+// coincide with fixed derived ones).
+constexpr int32_t kXrowKey = 1 << 30;
+inline int smat_key(const MOp& m, int e) {
+  return m.off[e] | ((m.param && (m.off[e] & kXtabFlag)) ? kXrowKey : 0);
+}
+
 // Generates the body of one register stage. Variables a0..a{2^R-1} hold the amplitudes; nm
 // maps logical register index j to the variable currently holding it (controlled-X on
 // register bits only permutes nm).
@@ -185,14 +193,15 @@ struct StageGen {
   std::string v(int j) const { return pre + std::to_string(nm[j]); }
   std::string ldm(const MOp& m, int e) const {
     if (smap) {
-      auto it = smap->find(m.off[e]);
+      auto it = smap->find(smat_key(m, e));
       if (it != smap->end()) {
         const std::string x = "smat[" + std::to_string(it->second) + "]";
         return m.conj ? "cj(" + x + ")" : x;
       }
     }
     if (m.off[e] & kXtabFlag)
-      return std::string(m.conj ? "ldc" : "ld") + "(xtab + " + std::to_string(m.off[e] & ~kXtabFlag) + ")";
+      return std::string(m.conj ? "ldc" : "ld") + "(" + (m.param ? "xb" : "xtab") + " + " +
+             std::to_string(m.off[e] & ~kXtabFlag) + ")";
     return std::string(m.conj ? "ldc" : "ld") + "(" + (m.param ? "tb" : "tab") + " + " + std::to_string(m.off[e]) + ")";
   }
 
@@ -462,20 +471,23 @@ struct SharedMats {
 // valid for single-sample schedules, where every thread reads sample 0's row.
 static SharedMats shared_mats(const Pass& p, bool with_params) {
   SharedMats sm;
-  auto add = [&](int off) {
-    if (sm.slot.count(off)) return;
-    sm.slot[off] = int(sm.offs.size());
-    sm.offs.push_back(off);
+  const MOp* cur = nullptr;
+  auto add = [&](int e) {
+    const int key = smat_key(*cur, e);
+    if (sm.slot.count(key)) return;
+    sm.slot[key] = int(sm.offs.size());
+    sm.offs.push_back(key);
   };
   for (const MOp& m : p.mops) {
     if (m.param && !with_params) continue;
+    cur = &m;
     switch (m.type) {
-      case MOP_U1: case MOP_CTRL: case MOP_RROT: case MOP_IROT: for (int e = 0; e < 4; ++e) add(m.off[e]); break;
-      case MOP_LIFT: add(m.off[0]); break;
-      case MOP_U2: for (int e = 0; e < 16; ++e) add(m.off[e]); break;
-      case MOP_DIAG: for (int e = 0; e < (1 << m.nsel); ++e) if ((m.active >> e) & 1) add(m.off[e]); break;
-      case MOP_CPHASE: if (!m.r1) add(m.off[0]); break;
-      case MOP_GRAD: for (int e = 0; e < (m.nsel == 1 ? 4 : 16); ++e) add(m.off[e]); break;
+      case MOP_U1: case MOP_CTRL: case MOP_RROT: case MOP_IROT: for (int e = 0; e < 4; ++e) add(e); break;
+      case MOP_LIFT: add(0); break;
+      case MOP_U2: for (int e = 0; e < 16; ++e) add(e); break;
+      case MOP_DIAG: for (int e = 0; e < (1 << m.nsel); ++e) if ((m.active >> e) & 1) add(e); break;
+      case MOP_CPHASE: if (!m.r1) add(0); break;
+      case MOP_GRAD: for (int e = 0; e < (m.nsel == 1 ? 4 : 16); ++e) add(e); break;
       default: break;
     }
   }
@@ -496,8 +508,9 @@ static std::string shared_mats_fill(const SharedMats& sm) {
   if (sm.offs.empty()) return "";
   std::ostringstream o;
   o << "  __shared__ double2 smat[" << sm.offs.size() << "];\n  for (u32 i = threadIdx.x; i < " << sm.offs.size()
-    << "u; i += blockDim.x) { const int mo = k_moffs[i]; smat[i] = (mo & " << kXtabFlag << ") ? __ldg(xtab + (mo & "
-    << (kXtabFlag - 1) << ")) : __ldg(tab + mo); }\n";
+    << "u; i += blockDim.x) { const int mo = k_moffs[i]; smat[i] = (mo & " << kXrowKey << ") ? __ldg(xtabs + (mo & "
+    << (kXtabFlag - 1) << ")) : (mo & " << kXtabFlag << ") ? __ldg(xtab + (mo & " << (kXtabFlag - 1)
+    << ")) : __ldg(tab + mo); }\n";
   return o.str();
 }
 
@@ -510,7 +523,8 @@ std::string jit_tile_source(const Pass& p, int R, int N, bool stage_params, int 
   o << kPrelude << shared_mats_decl(smats);
   o << "extern \"C\" __global__ void __launch_bounds__(" << threads << ", " << std::max(1, ctas)
     << ") mbk_tile(const __grid_constant__ TMap tmap, "
-    << "const double2* __restrict__ tab, const double2* __restrict__ xtab, long long tstride, long long tps, "
+    << "const double2* __restrict__ tab, const double2* __restrict__ xtab, const double2* __restrict__ xtabs, "
+    << "long long xrow, long long tstride, long long tps, "
     << "long long ntiles, u32* err) {\n";
   o << "  extern __shared__ unsigned char smem_raw[];\n  __shared__ __align__(8) u64 bar[2];\n  __shared__ int s_abort;\n";
   o << shared_mats_fill(smats);
@@ -570,6 +584,7 @@ std::string jit_tile_source(const Pass& p, int R, int N, bool stage_params, int 
   }
   o << geom("tile", "");
   o << "    const double2* tb = tab + (long long)b * tstride;\n    (void)tb;\n";
+  o << "    const double2* xb = xtabs + (long long)b * xrow;\n    (void)xb;\n";
   o << "    double2* tl = bufs[cur];\n";
   o << "    if (!mbar_wait(&bar[cur], cur ? ph1 : ph0)) { atomicOr(err, 1u); s_abort = 1; }\n";
   o << "    if (cur) ph1 ^= 1u; else ph0 ^= 1u;\n    __syncthreads();\n    if (s_abort) break;\n";
@@ -607,7 +622,7 @@ static void emit_grad(std::ostringstream& o, const MOp& m, const StageGen& gy, c
   const std::string tabn = m.param ? "tb" : "tab";
   auto L = [&](int e) {
     if (gy.smap) {
-      auto it = gy.smap->find(m.off[e]);
+      auto it = gy.smap->find(smat_key(m, e));
       if (it != gy.smap->end()) return "smat[" + std::to_string(it->second) + "]";
     }
     return "ld(" + tabn + " + " + std::to_string(m.off[e]) + ")";
@@ -683,6 +698,7 @@ std::string jit_adjoint_source(const Pass& p, int R, int N, bool stage_params, i
     << "long long ntiles, u32* err, double* gpart, u32* gcount, double* gout, const int* __restrict__ gslot) {\n";
   // reverse sweeps use no derived coefficients (their gates stay in the circuit's table)
   o << "  const double2* __restrict__ xtab = nullptr; (void)xtab;\n";
+  o << "  const double2* __restrict__ xtabs = nullptr; (void)xtabs;\n";
   o << "  extern __shared__ unsigned char smem_raw[];\n  __shared__ __align__(8) u64 bar[2];\n  __shared__ int s_abort;\n"
     << "  __shared__ bool lastcta;\n";
   o << shared_mats_fill(smats);
@@ -739,6 +755,7 @@ std::string jit_adjoint_source(const Pass& p, int R, int N, bool stage_params, i
     << subst(ld, "n_", "&tmd", "dbuf[cur ^ 1]", "&bar[cur ^ 1]") << "\n    }\n";
   o << geom("tile", "");
   o << "    const double2* tb = tab + (long long)b * tstride;\n    (void)tb; (void)gb;\n";
+  o << "    const double2* xb = xtabs; (void)xb;\n";
   o << "    double2* ty = ybuf[cur]; double2* td = dbuf[cur];\n";
   o << "    if (!mbar_wait(&bar[cur], cur ? ph1 : ph0)) { atomicOr(err, 1u); s_abort = 1; }\n";
   o << "    if (cur) ph1 ^= 1u; else ph0 ^= 1u;\n    __syncthreads();\n    if (s_abort) break;\n";
@@ -809,7 +826,8 @@ std::string jit_reg_source(const Pass& p, int N, bool stage_params) {
   const SharedMats smats = shared_mats(p, stage_params);
   o << kPrelude << shared_mats_decl(smats);
   o << "extern \"C\" __global__ void __launch_bounds__(128) mbk_reg(double2* __restrict__ v, const double2* __restrict__ tab, "
-    << "const double2* __restrict__ xtab, long long tstride, long long groups, int nsamples) {\n";
+    << "const double2* __restrict__ xtab, const double2* __restrict__ xtabs, long long xrow, long long tstride, "
+    << "long long groups, int nsamples) {\n";
   if (!smats.offs.empty()) o << shared_mats_fill(smats) << "  __syncthreads();\n";
   o << "  const long long total = groups * nsamples;\n";
   o << "  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < total; g += (long long)gridDim.x * blockDim.x) {\n";
@@ -821,6 +839,7 @@ std::string jit_reg_source(const Pass& p, int N, bool stage_params) {
   o << "    const u64 gb = 0ull; (void)gb;\n";
   o << "    double2* vs = v + ((long long)b << " << N << ");\n";
   o << "    const double2* tb = tab + (long long)b * tstride; (void)tb;\n";
+  o << "    const double2* xb = xtabs + (long long)b * xrow; (void)xb;\n";
   int reg[kMaxRegBits];
   for (int k = 0; k < R; ++k) reg[k] = p.bits[k];
   for (int j = 0; j < A; ++j) o << "    double2 a" << j << " = vs[lb | " << reg_off_const(j, R, reg) << "];\n";
@@ -871,12 +890,14 @@ int jit_prepare(std::vector<std::string>& sources, std::vector<CUfunction>& out,
   return MB_OK;
 }
 
-int jit_launch_tile(CUfunction fn, const CUtensorMap* map, const double2* tab, const double2* xtab, int64_t tstride,
-                    int64_t tps, int64_t ntiles, unsigned* err, int threads, size_t shm, int grid, cudaStream_t st) {
+int jit_launch_tile(CUfunction fn, const CUtensorMap* map, const double2* tab, const double2* xtab, const double2* xtabs,
+                    int64_t xrow, int64_t tstride, int64_t tps, int64_t ntiles, unsigned* err, int threads, size_t shm,
+                    int grid, cudaStream_t st) {
   Drv& d = drv();
   if (d.setattr(fn, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, int(shm)) != CUDA_SUCCESS) return MB_EDEVICE;
   long long ts = tstride, tp = tps, nt = ntiles;
-  void* params[] = {(void*)map, (void*)&tab, (void*)&xtab, &ts, &tp, &nt, &err};
+  long long xr = xrow;
+  void* params[] = {(void*)map, (void*)&tab, (void*)&xtab, (void*)&xtabs, &xr, &ts, &tp, &nt, &err};
   if (d.launch(fn, grid, 1, 1, threads, 1, 1, unsigned(shm), (CUstream)st, params, nullptr) != CUDA_SUCCESS) {
     set_error("JIT tile launch failed");
     return MB_EDEVICE;
@@ -884,12 +905,13 @@ int jit_launch_tile(CUfunction fn, const CUtensorMap* map, const double2* tab, c
   return MB_OK;
 }
 
-int jit_launch_reg(CUfunction fn, double2* v, const double2* tab, const double2* xtab, int64_t tstride, int64_t groups,
-                   int nsamples, int grid, cudaStream_t st) {
+int jit_launch_reg(CUfunction fn, double2* v, const double2* tab, const double2* xtab, const double2* xtabs,
+                   int64_t xrow, int64_t tstride, int64_t groups, int nsamples, int grid, cudaStream_t st) {
   Drv& d = drv();
   long long ts = tstride, gr = groups;
   int ns = nsamples;
-  void* params[] = {&v, (void*)&tab, (void*)&xtab, &ts, &gr, &ns};
+  long long xr = xrow;
+  void* params[] = {&v, (void*)&tab, (void*)&xtab, (void*)&xtabs, &xr, &ts, &gr, &ns};
   if (d.launch(fn, grid, 1, 1, 128, 1, 1, 0, (CUstream)st, params, nullptr) != CUDA_SUCCESS) {
     set_error("JIT sweep launch failed");
     return MB_EDEVICE;

@@ -140,3 +140,33 @@ def test_lowering_reference_recorded_circuit():
     c = mq.QCircuit([mq.QuantumGate(g.positions, g.mat()) for g in W.cpu_scan_circuit(case["angles_by_layer"]).flat()])
     ea, eb = lowering_errors(c, 15, t=11, R=3)
     assert ea <= 1e-12 and eb <= 1e-12, (ea, eb)
+
+
+# Parametric families are bound on the host with the code the device binder runs, so the host
+# check also covers the per-sample fusion of single-qubit runs: RX, RY, RZ on one qubit become
+# one 2x2 per sample, and on density matrices a gate's two halves with the channels after it
+# become one 4x4 superoperator per sample.
+@pytest.mark.parametrize("t,R", [(8, 3), (11, 3), (12, 4)])
+def test_lowering_parametric_hardware_efficient(t, R):
+    n, depth = 12, 3
+    c = W.hea_circuit(n, depth, W.hea_angles(n, depth, W.rng_for(40)))
+    ea, eb = lowering_errors(c, n, t=t, R=R)
+    assert ea <= 1e-12 and eb <= 1e-12, (ea, eb)
+
+
+@pytest.mark.parametrize("t,R", [(8, 3), (10, 4)])
+def test_lowering_noisy_density_hardware_efficient(t, R):
+    n, depth = 5, 2
+    c = W.hea_circuit(n, depth, W.hea_angles(n, depth, W.rng_for(41)), noise=(0.01, 0.02))
+    ea, eb = lowering_errors(c, n, dm=True, t=t, R=R)
+    assert ea <= 1e-12 and eb <= 1e-12, (ea, eb)
+
+
+def test_lowering_reference_recorded_circuit_families():
+    import json
+    import os
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "cpu_scan_circuits.json")
+    with open(path) as f:
+        case = json.load(f)["cases"]["n15-d20"]
+    ea, eb = lowering_errors(W.cpu_scan_circuit(case["angles_by_layer"]), 15, t=11, R=3)
+    assert ea <= 1e-12 and eb <= 1e-12, (ea, eb)
