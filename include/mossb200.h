@@ -209,8 +209,15 @@ MB_API int mb_graph_free(mb_graph g);
 /* ---- tuning: tile bits t (10..12) and register bits R (3..5) per register size ---------- */
 MB_API int mb_tuning_set(int nbits, int tile_bits, int reg_bits);
 MB_API int mb_tuning_get(int nbits, int* tile_bits, int* reg_bits);
-/* Times the fused execution of c on s for each candidate (t, R) and records the fastest for
- * s's register size; best_ms receives its time per apply. */
+/* Fusion width per register size: 1 (default) multiplies every run of operations on one qubit
+ * into one matrix at bind time (2x2 on pure states; on density matrices both gate halves with
+ * the channels after them as one 4x4), 0 applies every gate as its own micro-op. */
+MB_API int mb_tuning_set_fusion(int nbits, int fusion);
+MB_API int mb_tuning_get_fusion(int nbits, int* fusion);
+/* Times the fused execution of c on s for each candidate (t, R, fusion width) and records the
+ * fastest for s's register size; best_ms receives its time per apply. Sizes that run on
+ * specialised kernels try the current (t, R) with and without fusion, so tuning them costs one
+ * extra set of kernel compilations. */
 MB_API int mb_autotune(mb_circuit c, mb_state s, const double* theta, size_t ntheta, int flags, int* best_t,
                        int* best_r, double* best_ms);
 

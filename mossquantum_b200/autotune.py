@@ -1,5 +1,7 @@
-"""Autotuner for the fused passes: tile bits t (shared-memory tile of 2^t amplitudes) and
-register bits R (2^R amplitudes per thread, the width of one fused register stage).
+"""Autotuner for the fused passes: tile bits t (shared-memory tile of 2^t amplitudes), register
+bits R (2^R amplitudes per thread, the width of one fused register stage) and the fusion width
+(1: every run of operations on one qubit is multiplied into one matrix at bind time; 0: every
+gate is its own micro-op).
 
 ``autotune`` times every candidate on the caller's circuit and state (``mb_autotune``) and
 records the fastest for that register size; ``save``/``load`` persist the table as JSON so a
@@ -39,6 +41,16 @@ def get(nbits):
     return t.value, r.value
 
 
+def get_fusion(nbits):
+    f = ctypes.c_int()
+    N.check(N.lib().mb_tuning_get_fusion(int(nbits), ctypes.byref(f)))
+    return f.value
+
+
+def set_fusion(nbits, fusion):
+    N.check(N.lib().mb_tuning_set_fusion(int(nbits), int(fusion)), "mb_tuning_set_fusion")
+
+
 def set(nbits, tile_bits, reg_bits):  # noqa: A001 - mirrors mb_tuning_set
     N.check(N.lib().mb_tuning_set(int(nbits), int(tile_bits), int(reg_bits)), "mb_tuning_set")
 
@@ -47,7 +59,7 @@ def save(table_bits, path=None):
     path = path or default_path()
     os.makedirs(os.path.dirname(path), exist_ok=True)
     with open(path, "w") as f:
-        json.dump({str(n): list(get(n)) for n in table_bits}, f, indent=1)
+        json.dump({str(n): list(get(n)) + [get_fusion(n)] for n in table_bits}, f, indent=1)
     return path
 
 
@@ -57,6 +69,8 @@ def load(path=None):
         return {}
     with open(path) as f:
         table = json.load(f)
-    for n, (t, r) in table.items():
-        set(int(n), t, r)
+    for n, v in table.items():
+        set(int(n), v[0], v[1])
+        if len(v) > 2:
+            set_fusion(int(n), v[2])
     return {int(n): tuple(v) for n, v in table.items()}

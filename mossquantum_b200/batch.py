@@ -25,7 +25,7 @@ class BatchPlan:
     """groups: {n: (template circuit for n qubits, samples B_n)}; observable_for(n) gives the
     observable evaluated on every sample of size n. kind: "pure" or "density"."""
 
-    def __init__(self, groups, observable_for, kind="pure", autotune=False, autotune_max_bits=17):
+    def __init__(self, groups, observable_for, kind="pure", autotune=False, autotune_max_bits=24):
         self.kind = kind
         self.tuned = {}
         self.groups = []
@@ -46,15 +46,17 @@ class BatchPlan:
         self.results = buf
         self.graph = None
         if autotune:
-            # Tile and register widths per register size, timed on each group's own batch;
-            # sizes above autotune_max_bits keep the defaults (their candidates would each
-            # need specialised kernels compiled first).
-            from .autotune import autotune as tune
+            # Tile width, register width and fusion width per register size, timed on each
+            # group's own batch with random angles (sizes on specialised kernels try a short
+            # list, one compilation per candidate); sizes above autotune_max_bits keep defaults.
+            from .autotune import autotune as tune, get_fusion
+            rng = np.random.default_rng(0)
             for g in self.groups:
                 bits = 2 * g["n"] if kind == "density" else g["n"]
                 if 8 <= bits <= autotune_max_bits:
-                    th = np.zeros((g["B"], g["circuit"].nparameters()))
-                    self.tuned[bits] = tune(g["circuit"], g["state"], th)
+                    th = rng.uniform(0, 2 * np.pi, size=(g["B"], g["circuit"].nparameters()))
+                    t, r, ms = tune(g["circuit"], g["state"], th)
+                    self.tuned[bits] = (t, r, get_fusion(bits), ms)
         # Eager warm-up with zero parameters: builds schedules, kernels and reduction plans.
         self._stage({g["n"]: np.zeros((g["B"], g["circuit"].nparameters())) for g in self.groups})
         self._record_body()

@@ -1315,10 +1315,12 @@ static int plain_fop_launch(mb_circuit c, const FOp& f, double2* v, int64_t elem
 // the defaults (the autotuner sets them per register size).
 struct Tuning {
   int t = 12, R = 4;
+  int fuse = 1;   // fusion width: 1 = single-qubit runs fused at bind time, 0 = one micro-op per gate
 };
 
 std::mutex g_tune_mu;
 std::map<int, std::pair<int, int>> g_tuning;  // register bits -> (tile bits, register bits)
+std::map<int, int> g_fusion;                   // register bits -> fusion width
 
 // Specialised kernels are used from MB_JIT_MIN_BITS register bits on (default 18); MB_JIT=0
 // disables them. Small states keep the interpreter kernels (no compile latency).
@@ -1347,6 +1349,8 @@ static Tuning tuning_for(int N) {
       tu.t = it->second.first;
       tu.R = it->second.second;
     }
+    auto fi = g_fusion.find(N);
+    if (fi != g_fusion.end()) tu.fuse = fi->second;
   }
   if (const char* e = getenv("MB_TILE_BITS")) tu.t = std::max(8, std::min(12, atoi(e)));
   if (const char* e = getenv("MB_REG_BITS")) tu.R = std::max(3, std::min(5, atoi(e)));
@@ -1357,6 +1361,8 @@ static Tuning tuning_for(int N) {
 }  // namespace
 
 static void prepare_jit(Schedule* S);
+
+bool jit_sizes(int nbits) { return want_jit(nbits) && jit_available(); }
 
 int get_schedule_ex(mb_circuit c, int n, int dm, int adjoint, int lo, int hi, int nsamples, Schedule** out) {
   const int N = dm ? 2 * n : n;
@@ -1373,6 +1379,7 @@ int get_schedule_ex(mb_circuit c, int n, int dm, int adjoint, int lo, int hi, in
   }
   for (Schedule* s : c->scheds)
     if (s->N == N && s->dm == dm && !s->dagger && s->t == tu.t && s->R == tu.R && s->nsamples == nsamples &&
+        (adjoint || s->fuse == (tu.fuse != 0)) &&
         s->lo == lo && s->hi == hi && s->adjoint == adjoint) {
       *out = s;
       return MB_OK;
@@ -1390,6 +1397,7 @@ int get_schedule_ex(mb_circuit c, int n, int dm, int adjoint, int lo, int hi, in
   S->lo = lo;
   S->hi = hi;
   S->adjoint = adjoint;
+  S->fuse = tu.fuse != 0;
   if (adjoint) {
     if (dm || !build_adjoint_fops(c, lo, hi, S->fops)) {
       set_error("the fused adjoint supports pure-state circuits with 1- and 2-qubit parameters");
@@ -1790,6 +1798,22 @@ extern "C" int mb_tuning_set(int nbits, int tile_bits, int reg_bits) {
   }
   std::lock_guard<std::mutex> lk(mb::g_tune_mu);
   mb::g_tuning[nbits] = {tile_bits, reg_bits};
+  return MB_OK;
+}
+
+extern "C" int mb_tuning_set_fusion(int nbits, int fusion) {
+  if (nbits < 1 || nbits > 40 || fusion < 0 || fusion > 1) {
+    mb::set_error("fusion width out of range (0 or 1)");
+    return MB_EINVAL;
+  }
+  std::lock_guard<std::mutex> lk(mb::g_tune_mu);
+  mb::g_fusion[nbits] = fusion;
+  return MB_OK;
+}
+
+extern "C" int mb_tuning_get_fusion(int nbits, int* fusion) {
+  if (!fusion) return MB_EINVAL;
+  *fusion = mb::tuning_for(nbits).fuse;
   return MB_OK;
 }
 

@@ -131,6 +131,7 @@ int observable_apply(mb_observable o, const double2* in, double2* out, int n, in
 
 // fused.cu
 int apply_fused(mb_circuit c, mb_state s, int64_t mrow_stride);
+bool jit_sizes(int nbits);  // register sizes that run on the specialised (NVRTC) kernels
 int get_schedule_ex(mb_circuit c, int n, int dm, int adjoint, int lo, int hi, int nsamples, Schedule** out);
 int run_schedule(mb_circuit c, Schedule* S, double2* v, int nsamples, int64_t mstride);
 int run_adjoint_schedule(mb_circuit c, Schedule* S, double2* y, double2* d, double* d_grad);

@@ -5,6 +5,7 @@
 // experiments.jl). Here a caller runs a sequence once eagerly (building schedules,
 // specialised kernels and reduction plans), records the same sequence into a CUDA graph and
 // replays it with new parameters: one graph launch per evaluation of a whole batch.
+#include <array>
 #include <cstring>
 #include <vector>
 
@@ -128,11 +129,18 @@ extern "C" int mb_autotune(mb_circuit c, mb_state s, const double* theta, size_t
   if (!c || !s || !best_t || !best_r || !best_ms) return MB_EINVAL;
   const int dm = s->kind == MB_DENSITY || s->kind == MB_BATCH_DENSITY;
   const int N = dm ? 2 * s->n : s->n;
-  int t0 = 0, r0 = 0;
+  int t0 = 0, r0 = 0, f0 = 1;
   mb_tuning_get(N, &t0, &r0);
-  const int cand[][2] = {{12, 4}, {11, 4}, {10, 4}, {12, 3}, {11, 3}, {10, 3}};
+  mb_tuning_get_fusion(N, &f0);
+  std::vector<std::array<int, 3>> cand;
+  if (jit_sizes(N)) {
+    for (int f : {1, 0}) cand.push_back({t0, r0, f});
+  } else {
+    for (int f : {1, 0})
+      for (auto tr : {std::array<int, 2>{12, 4}, {11, 4}, {10, 4}, {12, 3}, {11, 3}, {10, 3}}) cand.push_back({tr[0], tr[1], f});
+  }
   double best = 1e300;
-  int bt = t0, br = r0;
+  int bt = t0, br = r0, bf = f0;
   cudaEvent_t a, b;
   MB_CHECK_CUDA(cudaEventCreate(&a));
   MB_CHECK_CUDA(cudaEventCreate(&b));
@@ -140,6 +148,7 @@ extern "C" int mb_autotune(mb_circuit c, mb_state s, const double* theta, size_t
   for (auto& cd : cand) {
     if (cd[0] > N) continue;
     if ((rc = mb_tuning_set(N, cd[0], cd[1]))) break;
+    if ((rc = mb_tuning_set_fusion(N, cd[2]))) break;
     // warm-up builds the schedule and its kernels; then two timed applies
     if ((rc = mb_apply(c, s, theta, ntheta, flags & ~MB_APPLY_PLAIN))) {
       rc = MB_OK;  // a width this circuit cannot use (e.g. no specialised kernels): skip it
@@ -158,12 +167,14 @@ extern "C" int mb_autotune(mb_circuit c, mb_state s, const double* theta, size_t
       best = ms / 2;
       bt = cd[0];
       br = cd[1];
+      bf = cd[2];
     }
     if (rc) break;
   }
   cudaEventDestroy(a);
   cudaEventDestroy(b);
   mb_tuning_set(N, bt, br);
+  mb_tuning_set_fusion(N, bf);
   *best_t = bt;
   *best_r = br;
   *best_ms = best;
