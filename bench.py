@@ -582,7 +582,8 @@ def serve_measure(requests, rate, plain=True, seed_stream=0, log_prefix="serve")
     out = {"rate_req_per_s": "saturating" if rate is None else rate, "requests": len(reqs),
            "server": {"p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "evals_per_s": st["evals_per_s"],
                       "wall_evals_per_s": len(reqs) / span, "iterations": st["iterations"],
-                      "peak_hbm_bytes": st["peak_bytes"], "warmup_s": warm_s},
+                      "peak_hbm_bytes": st["peak_bytes"], "warmup_s": warm_s,
+                      "jit_compile_ms_in_run": st["jit_compile_ms"], "jit_compiles_in_run": st["jit_compiles"]},
            "gpu_launches": launches, "clocks": clk.summary(),
            "h2d_bytes": int(sum(8 * r[5].size for r in reqs)),
            "d2h_bytes": int(sum(16 + (8 * r[5].size if r[4] else 0) for r in reqs))}

@@ -322,6 +322,8 @@ typedef struct mb_server_stats {
   size_t bytes_in_use, peak_bytes, budget_bytes;
   double p50_ms, p99_ms;    /* latency percentiles of the completed requests                   */
   double evals_per_s;       /* completed requests / (last completion - first submission)       */
+  double jit_compile_ms;    /* specialised-kernel compile time spent since start / stats reset  */
+  uint64_t jit_compiles;    /* kernels compiled since start / stats reset                       */
 } mb_server_stats;
 
 typedef struct mb_server_s* mb_server;

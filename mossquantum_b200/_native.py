@@ -76,7 +76,8 @@ class MbServerStats(ctypes.Structure):
     _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64), ("failed", ctypes.c_uint64),
                 ("iterations", ctypes.c_uint64), ("active", ctypes.c_int), ("pending", ctypes.c_int),
                 ("bytes_in_use", ctypes.c_size_t), ("peak_bytes", ctypes.c_size_t), ("budget_bytes", ctypes.c_size_t),
-                ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double), ("evals_per_s", ctypes.c_double)]
+                ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double), ("evals_per_s", ctypes.c_double),
+                ("jit_compile_ms", ctypes.c_double), ("jit_compiles", ctypes.c_uint64)]
 
 
 class MbKernelStat(ctypes.Structure):

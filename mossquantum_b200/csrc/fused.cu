@@ -1572,8 +1572,12 @@ static void prepare_jit(Schedule* S) {
     if (getenv("MB_JIT_VERBOSE")) fprintf(stderr, "mossb200: JIT disabled for this schedule: %s\n", err.c_str());
     return;
   }
-  for (size_t i = 0; i < small_who.size(); ++i) small_who[i]->jit_fn = fns[i];
+  for (size_t i = 0; i < small_who.size(); ++i) {
+    small_who[i]->jit_fn = fns[i];
+    if (fns[i]) jit_retain((void*)fns[i]);
+  }
   S->jit = 1;
+  if (!g_ctx.capturing) jit_trim();
 }
 
 int run_schedule(mb_circuit c, Schedule* S, double2* v, int nsamples, int64_t mstride) {
@@ -1763,6 +1767,8 @@ int apply_fused(mb_circuit c, mb_state s, int64_t mrow_stride) {
 
 void release_schedules(mb_circuit c) {
   for (Schedule* s : c->scheds) {
+    for (const Pass& p : s->passes)
+      if (p.jit_fn) jit_release(p.jit_fn);
     dev_free(s->d_stages);
     dev_free(s->d_mops);
     dev_free(s->d_gslots);

@@ -74,6 +74,7 @@ struct Drv {
   CUresult (*launch)(CUfunction, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned, CUstream,
                      void**, void**) = nullptr;
   CUresult (*setattr)(CUfunction, CUfunction_attribute, int) = nullptr;
+  CUresult (*unload)(CUmodule) = nullptr;
   bool ok = false;
 };
 
@@ -88,12 +89,27 @@ Drv& drv() {
   if (cudaGetDriverEntryPoint("cuModuleGetFunction", &p, cudaEnableDefault, &q) == cudaSuccess && p) d.getfn = (decltype(d.getfn))p;
   if (cudaGetDriverEntryPoint("cuLaunchKernel", &p, cudaEnableDefault, &q) == cudaSuccess && p) d.launch = (decltype(d.launch))p;
   if (cudaGetDriverEntryPoint("cuFuncSetAttribute", &p, cudaEnableDefault, &q) == cudaSuccess && p) d.setattr = (decltype(d.setattr))p;
+  if (cudaGetDriverEntryPoint("cuModuleUnload", &p, cudaEnableDefault, &q) == cudaSuccess && p) d.unload = (decltype(d.unload))p;
   d.ok = d.load && d.getfn && d.launch && d.setattr;
   return d;
 }
 
+// Compiled kernels by source text. Schedules that use a kernel hold a reference
+// (jit_retain / jit_release); jit_trim unloads the least recently used unreferenced modules
+// while more than MB_JIT_CACHE_MAX (default 1024) are loaded, so a long-running process that
+// meets ever new circuit shapes keeps a bounded set of modules.
+struct CacheEnt {
+  CUmodule mod = nullptr;
+  CUfunction fn = nullptr;
+  int refs = 0;
+  uint64_t last = 0;
+};
 std::mutex g_jit_mu;
-std::map<std::string, CUfunction> g_cache;
+std::map<std::string, CacheEnt> g_cache;
+std::map<CUfunction, std::string> g_by_fn;
+uint64_t g_tick = 0;
+double g_compile_s = 0.0;     // cumulative NVRTC compile + module load time
+uint64_t g_compiles = 0;
 
 const char* kPrelude = R"PRE(
 typedef unsigned long long u64;
@@ -393,7 +409,10 @@ CUfunction compile_kernel(const std::string& src, std::string* err) {
   {
     std::lock_guard<std::mutex> lk(g_jit_mu);
     auto it = g_cache.find(src);
-    if (it != g_cache.end()) return it->second;
+    if (it != g_cache.end()) {
+      it->second.last = ++g_tick;
+      return it->second.fn;
+    }
   }
   Nvrtc& n = nvrtc();
   Drv& d = drv();
@@ -451,13 +470,69 @@ CUfunction compile_kernel(const std::string& src, std::string* err) {
     return nullptr;
   }
   std::lock_guard<std::mutex> lk(g_jit_mu);
-  g_cache[src] = fn;
+  auto it = g_cache.find(src);
+  if (it != g_cache.end()) {  // another thread compiled the same source meanwhile
+    if (d.unload) d.unload(mod);
+    it->second.last = ++g_tick;
+    return it->second.fn;
+  }
+  CacheEnt& e = g_cache[src];
+  e.mod = mod;
+  e.fn = fn;
+  e.last = ++g_tick;
+  g_by_fn[fn] = src;
+  g_compile_s += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  ++g_compiles;
   return fn;
 }
 
 }  // namespace
 
 bool jit_available() { return nvrtc().ok && drv().ok; }
+
+void jit_retain(void* fn) {
+  std::lock_guard<std::mutex> lk(g_jit_mu);
+  auto it = g_by_fn.find((CUfunction)fn);
+  if (it != g_by_fn.end()) ++g_cache[it->second].refs;
+}
+
+void jit_release(void* fn) {
+  std::lock_guard<std::mutex> lk(g_jit_mu);
+  auto it = g_by_fn.find((CUfunction)fn);
+  if (it != g_by_fn.end()) {
+    CacheEnt& e = g_cache[it->second];
+    if (e.refs > 0) --e.refs;
+  }
+}
+
+void jit_trim() {
+  size_t cap = 1024;
+  if (const char* e = getenv("MB_JIT_CACHE_MAX")) cap = size_t(std::max(16, atoi(e)));
+  Drv& d = drv();
+  std::lock_guard<std::mutex> lk(g_jit_mu);
+  bool synced = false;
+  while (g_cache.size() > cap && d.unload) {
+    auto victim = g_cache.end();
+    for (auto it = g_cache.begin(); it != g_cache.end(); ++it)
+      if (it->second.refs == 0 && (victim == g_cache.end() || it->second.last < victim->second.last)) victim = it;
+    if (victim == g_cache.end()) break;  // everything loaded is in use
+    if (!synced) {
+      // a released schedule's kernels may still be running: finish all work before unloading
+      cudaDeviceSynchronize();
+      synced = true;
+    }
+    d.unload(victim->second.mod);
+    g_by_fn.erase(victim->second.fn);
+    g_cache.erase(victim);
+  }
+}
+
+void jit_stats(double* compile_ms, uint64_t* compiles, size_t* modules) {
+  std::lock_guard<std::mutex> lk(g_jit_mu);
+  if (compile_ms) *compile_ms = g_compile_s * 1e3;
+  if (compiles) *compiles = g_compiles;
+  if (modules) *modules = g_cache.size();
+}
 
 // Matrix elements of a pass that are the same for every sample (fixed gates and channels): the
 // kernel copies them from the table into shared memory once per CTA, so the gate loops read
@@ -874,8 +949,12 @@ int jit_prepare(std::vector<std::string>& sources, std::vector<CUfunction>& out,
         if (budget_s > 0 && elapsed() > budget_s) {
           std::lock_guard<std::mutex> lk(g_jit_mu);
           auto it = g_cache.find(sources[i]);
-          if (it != g_cache.end()) out[i] = it->second;
-          else skipped[i] = 1;
+          if (it != g_cache.end()) {
+            out[i] = it->second.fn;
+            it->second.last = ++g_tick;
+          } else {
+            skipped[i] = 1;
+          }
           continue;
         }
         out[i] = compile_kernel(sources[i], &errs[i]);

@@ -9,6 +9,13 @@
 
 namespace mb {
 bool jit_available();
+// Reference counts of the compiled kernels a schedule uses; jit_trim unloads unreferenced
+// modules beyond the cache cap (MB_JIT_CACHE_MAX).
+void jit_retain(void* fn);
+void jit_release(void* fn);
+void jit_trim();
+// Cumulative compile time (NVRTC and module load), compilations, modules loaded.
+void jit_stats(double* compile_ms, uint64_t* compiles, size_t* modules);
 // ctas: CTAs per SM the kernel is compiled for (its launch bounds; the launch uses the same).
 std::string jit_tile_source(const Pass& p, int R, int N, bool stage_params, int ctas = 1);
 std::string jit_reg_source(const Pass& p, int N, bool stage_params);

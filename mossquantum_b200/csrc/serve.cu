@@ -32,6 +32,7 @@
 #include <vector>
 
 #include "internal.h"
+#include "jit.h"
 
 using namespace mb;
 
@@ -105,6 +106,8 @@ struct mb_server_s {
   std::vector<double> lat;                         // qmu
   uint64_t submitted = 0, completed = 0, failed = 0, iterations = 0;
   double t_first = -1, t_last = 0;
+  double jit_ms0 = 0;         // compile counters at start / last stats reset
+  uint64_t jit_n0 = 0;
   int n_active = 0, n_pending = 0;                 // qmu (mirrors of loop-owned counts)
   // loop-owned
   std::deque<Req*> pending;
@@ -636,6 +639,7 @@ extern "C" int mb_server_start(const mb_server_config* cfg, mb_server* out) {
   if (int rc = check_init()) return rc;
   if (!out) return MB_EINVAL;
   std::unique_ptr<mb_server_s> S(new mb_server_s());
+  jit_stats(&S->jit_ms0, &S->jit_n0, nullptr);
   const size_t left = g_ctx.budget > g_ctx.used ? g_ctx.budget - g_ctx.used : 0;
   S->budget = (cfg && cfg->hbm_budget_bytes) ? cfg->hbm_budget_bytes : size_t(double(left) * 0.95);
   if (S->budget > left) {
@@ -798,6 +802,11 @@ extern "C" int mb_server_stats_get(mb_server S, mb_server_stats* o) {
     const double span = S->t_last - S->t_first;
     o->evals_per_s = span > 0 ? double(S->completed) / (span / 1e3) : 0.0;
   }
+  double ms = 0;
+  uint64_t nc = 0;
+  jit_stats(&ms, &nc, nullptr);
+  o->jit_compile_ms = ms - S->jit_ms0;
+  o->jit_compiles = nc - S->jit_n0;
   return MB_OK;
 }
 
@@ -807,6 +816,7 @@ extern "C" int mb_server_stats_reset(mb_server S) {
   S->lat.clear();
   S->submitted = S->completed = S->failed = S->iterations = 0;
   S->t_first = -1;
+  jit_stats(&S->jit_ms0, &S->jit_n0, nullptr);
   S->t_last = 0;
   S->peak = S->used;
   return MB_OK;
