@@ -300,6 +300,20 @@ def batch_measure(steps=3, warmup=2, per_size=3, dm_samples=4):
     ms_step = (pure_ms + dm_ms) / steps
     launches = N.launch_count() - l0
     evals = 512 + 64
+    # The sizes below the specialised-kernel threshold (10..17 qubits) replayed alone: what
+    # launching all sizes' passes together could save at most (their kernels are short and
+    # leave most SMs idle).
+    small = {n: groups[n] for n in groups if n < 18}
+    plan_small = BatchPlan(small, W.xxz)
+    th_small = {n: th[n] for n in small}
+    plan_small.run(th_small)
+    start.record(stream)
+    for _ in range(steps):
+        plan_small.run(th_small)
+    end.record(stream)
+    end.synchronize()
+    small_ms = start.elapsed_time(end) / steps
+    plan_small.close()
     # plain per-call path: stratified sample
     plain_s = {}
     for n in sorted(counts):
@@ -319,7 +333,8 @@ def batch_measure(steps=3, warmup=2, per_size=3, dm_samples=4):
     plain_total = sum(plain_s[n] * counts[n] for n in counts) + 64 * dm_plain
     log(f"batch: {ms_step:.1f} ms per step, plain per-call {plain_total * 1e3:.0f} ms per batch")
     return {"evals_per_s": evals / (ms_step / 1e3), "ms_per_step": ms_step, "pure_ms_per_step": pure_ms / steps,
-            "density_ms_per_step": dm_ms / steps, "evals_per_step": evals, "steps": steps, "warmup": warmup,
+            "density_ms_per_step": dm_ms / steps, "small_sizes_ms_per_step": small_ms,
+            "evals_per_step": evals, "steps": steps, "warmup": warmup,
             "sizes": counts, "plan_build_s": prep_s,
             "autotuned": {str(k): list(v) for k, v in {**plan.tuned, **plan_dm.tuned}.items()},
             "plain_per_call": {"evals_per_s": evals / plain_total, "seconds_per_batch": plain_total,
@@ -341,6 +356,7 @@ def batch_workload(args):
             "config": {"workload": "512 pure (n=10..22, HEA depth 8) + 64 density (n=10, noisy) <XXZ>",
                        "sizes": r["sizes"], "plan_build_s": r["plan_build_s"], "autotuned": r["autotuned"]},
             "pure_ms_per_step": r["pure_ms_per_step"], "density_ms_per_step": r["density_ms_per_step"],
+            "small_sizes_ms_per_step": r["small_sizes_ms_per_step"],
             "plain_per_call": r["plain_per_call"], "speedup_vs_plain": r["speedup_vs_plain"],
             "e2e": {"value": r["e2e"]["evals_per_s"], "unit": "evals/s",
                     "h2d_bytes_per_step": r["e2e"]["h2d_bytes_per_step"],
