@@ -692,7 +692,10 @@ std::string jit_tile_source(const Pass& p, int R, int N, bool stage_params, int 
 
 // Gradient accumulation of one MOP_GRAD op: thread sum of Re<y|D|delta> over its register
 // amplitudes, reduced across the warp and added to the warp's shared-memory slot.
-static void emit_grad(std::ostringstream& o, const MOp& m, const StageGen& gy, const StageGen& gd, int R, int nw) {
+// Emits this thread's partial sum of one gradient micro-op into variable `name` (declared by
+// the caller); the warp reduction of a stage's sums runs once, in emit_grad_reduce.
+static void emit_grad(std::ostringstream& o, const MOp& m, const StageGen& gy, const StageGen& gd, int R,
+                      const std::string& name) {
   const int A = 1 << R;
   const std::string tabn = m.param ? "tb" : "tab";
   auto L = [&](int e) {
@@ -754,8 +757,35 @@ static void emit_grad(std::ostringstream& o, const MOp& m, const StageGen& gy, c
         o << "  }\n";
       }
   }
-  o << "  for (int off = 16; off > 0; off >>= 1) gs += __shfl_xor_sync(0xffffffffu, gs, off);\n";
-  o << "  if ((tx & 31u) == 0u) gw[" << m.active << " * " << nw << " + (tx >> 5)] += gs;\n}\n";
+  o << "  " << name << " = gs;\n}\n";
+}
+
+// Sums k partial sums (consecutive accumulators acc0, acc0+1, ...) over the warp in one
+// butterfly: at step s the lanes with lane bit s set keep the upper half of their values and
+// send the lower half, so k values take (k - 1) + (5 - log2 k) shuffles instead of 5k. Lane L
+// then holds the sum of value j = sum_s bit_s(L) * k / 2^(s+1); lanes below k add it to the
+// warp's slot of accumulator acc0 + j.
+static void emit_grad_reduce(std::ostringstream& o, const std::vector<std::string>& names, int acc0, int nw) {
+  const int kreal = int(names.size());
+  int k = 1, m = 0;
+  while (k < kreal) k <<= 1, ++m;
+  if (m > 5) return;  // callers chunk to 32
+  o << "{ const u32 ln = tx & 31u;\n";
+  for (int i = 0; i < k; ++i) o << "  double v" << i << " = " << (i < kreal ? names[i] : std::string("0.0")) << ";\n";
+  int cur = k;
+  for (int st = 0; st < m; ++st) {
+    const int half = cur >> 1;
+    o << "  { const bool up = (ln >> " << st << ") & 1u;\n";
+    for (int i = 0; i < half; ++i)
+      o << "    { const double keep = up ? v" << (i + half) << " : v" << i << ", send = up ? v" << i << " : v"
+        << (i + half) << "; v" << i << " = keep + __shfl_xor_sync(0xffffffffu, send, " << (1 << st) << "); }\n";
+    o << "  }\n";
+    cur = half;
+  }
+  for (int st = m; st < 5; ++st) o << "  v0 += __shfl_xor_sync(0xffffffffu, v0, " << (1 << st) << ");\n";
+  o << "  if (ln < " << k << "u) { u32 j = 0u;";
+  for (int st = 0; st < m; ++st) o << " j += ((ln >> " << st << ") & 1u) * " << (k >> (st + 1)) << "u;";
+  o << " if (j < " << kreal << "u) gw[(" << acc0 << "u + j) * " << nw << "u + (tx >> 5)] += v0; }\n}\n";
 }
 
 std::string jit_adjoint_source(const Pass& p, int R, int N, bool stage_params, int ctas) {
@@ -848,15 +878,29 @@ std::string jit_adjoint_source(const Pass& p, int R, int N, bool stage_params, i
     StageGen gd{R, sd.reg, o, false, std::vector<int>(A), "d"};
     gy.smap = gd.smap = &smats.slot;
     for (int j = 0; j < A; ++j) gy.nm[j] = gd.nm[j] = j;
+    // gradient partial sums of this stage, reduced together in chunks (2 with 16 amplitudes per
+    // thread, 8 with 8: few enough live sums to stay in registers)
+    const int gchunk = R >= 4 ? 2 : 8;
+    std::vector<std::string> gnames;
+    int gacc0 = -1, gcount = 0;
     for (int q = 0; q < sd.nops; ++q) {
       const MOp& m = p.mops[sd.op0 + q];
       if (m.type == MOP_GRAD || m.type == MOP_GRADP) {
-        emit_grad(o, m, gy, gd, R, nw);
+        if (int(gnames.size()) == gchunk || (gacc0 >= 0 && int(m.active) != gacc0 + int(gnames.size()))) {
+          emit_grad_reduce(o, gnames, gacc0, nw);
+          gnames.clear();
+        }
+        if (gnames.empty()) gacc0 = int(m.active);
+        const std::string name = "gp" + std::to_string(gcount++);
+        o << "      double " << name << ";\n";
+        emit_grad(o, m, gy, gd, R, name);
+        gnames.push_back(name);
       } else {
         gy.emit(m);
         gd.emit(m);
       }
     }
+    if (!gnames.empty()) emit_grad_reduce(o, gnames, gacc0, nw);
     for (int j = 0; j < A; ++j)
       o << "      ty[swz(lb | " << reg_off_const(j, R, sd.reg) << ")] = " << gy.v(j) << "; td[swz(lb | "
         << reg_off_const(j, R, sd.reg) << ")] = " << gd.v(j) << ";\n";
