@@ -69,7 +69,7 @@ class Pool {
       std::lock_guard<std::mutex> lk(mu_);
       job_ = &f;
       tasks_ = tasks;
-      next_.store(1);
+      next_ = 1;          // task 0 runs on the calling thread
       pending_ = tasks - 1;
       ++gen_;
     }
@@ -78,6 +78,7 @@ class Pool {
     std::unique_lock<std::mutex> lk(mu_);
     done_cv_.wait(lk, [&] { return pending_ == 0; });
     job_ = nullptr;
+    tasks_ = 0;
   }
 
  private:
@@ -93,26 +94,21 @@ class Pool {
     stop_ = false;
     for (int i = 0; i < n; ++i) workers_.emplace_back([this] { loop(); });
   }
+  // A task index and the job it belongs to are taken in one critical section, so a worker that
+  // wakes late can never pair a finished job with the next job's counter.
   void loop() {
-    uint64_t seen;
-    {
-      std::lock_guard<std::mutex> lk(mu_);
-      seen = gen_;
-    }
+    std::unique_lock<std::mutex> lk(mu_);
+    uint64_t seen = gen_;
     for (;;) {
-      const std::function<void(int64_t)>* job;
-      int64_t tasks;
-      {
-        std::unique_lock<std::mutex> lk(mu_);
-        cv_.wait(lk, [&] { return gen_ != seen; });
-        seen = gen_;
-        if (stop_) return;
-        job = job_;
-        tasks = tasks_;
-      }
-      for (int64_t p = next_.fetch_add(1); p < tasks; p = next_.fetch_add(1)) {
+      cv_.wait(lk, [&] { return gen_ != seen || (job_ && next_ < tasks_); });
+      seen = gen_;
+      if (stop_) return;
+      while (job_ && next_ < tasks_) {
+        const int64_t p = next_++;
+        const std::function<void(int64_t)>* job = job_;
+        lk.unlock();
         (*job)(p);
-        std::lock_guard<std::mutex> lk(mu_);
+        lk.lock();
         if (--pending_ == 0) done_cv_.notify_one();
       }
     }
@@ -121,8 +117,7 @@ class Pool {
   std::mutex mu_, run_mu_;
   std::condition_variable cv_, done_cv_;
   const std::function<void(int64_t)>* job_ = nullptr;
-  int64_t tasks_ = 0, pending_ = 0;
-  std::atomic<int64_t> next_{0};
+  int64_t tasks_ = 0, pending_ = 0, next_ = 0;
   uint64_t gen_ = 0;
   bool stop_ = false;
 };
