@@ -1370,9 +1370,11 @@ int get_schedule_ex(mb_circuit c, int n, int dm, int adjoint, int lo, int hi, in
   Tuning tu = tuning_for(N);
   if (adjoint) {
     // y and delta tiles, double-buffered: MB_ADJOINT_TILE_BITS (8..11) and the register width of
-    // the dual-state passes MB_ADJOINT_REG_BITS (3..4)
-    tu.t = std::min(tu.t, 11);
-    tu.R = 4;
+    // the dual-state passes MB_ADJOINT_REG_BITS (3..4). Default 2^10-amplitude tiles, 8
+    // amplitudes per thread, 3 CTAs per SM: the fastest point of a sweep on the 24-qubit,
+    // 1152-angle gradient (47.8 ms against 60.2 ms at 2^11 tiles, 16 amplitudes, 1 CTA).
+    tu.t = std::min(tu.t, 10);
+    tu.R = 3;
     if (const char* e = getenv("MB_ADJOINT_TILE_BITS")) tu.t = std::max(8, std::min(11, atoi(e)));
     if (const char* e = getenv("MB_ADJOINT_REG_BITS")) tu.R = std::max(3, std::min(4, atoi(e)));
     tu.t = std::min(tu.t, N);
@@ -1514,11 +1516,11 @@ static int tile_ctas(int t) {
 }
 
 // CTAs per SM of a dual-state adjoint pass: what shared memory holds of four double-buffered
-// tiles plus the gradient slots (allowing 8 KB), capped at MB_ADJOINT_CTAS (default 1); the
+// tiles plus the gradient slots (allowing 8 KB), capped at MB_ADJOINT_CTAS (default 3); the
 // kernel's launch bounds ask the compiler to fit that many CTAs in the register file.
 static int adjoint_ctas(int t) {
   const size_t shm = (size_t(64) << t) + 1024 + 8 * 1024;
-  int cap = 1;
+  int cap = 3;
   if (const char* e = getenv("MB_ADJOINT_CTAS")) cap = std::max(1, std::min(4, atoi(e)));  // gpart holds 4 per SM
   return std::max(1, std::min(cap, int((227 * 1024) / (shm + 256))));
 }
