@@ -422,10 +422,30 @@ def _case_setup(name, mq, W):
         tensor = name == "dmma"
         return (f"K5 {'FP64 tensor cores' if tensor else 'on K0 (CUDA cores)'}: {len(gates)} random dense 5-qubit "
                 f"gates in brickwork, n={n}"), lambda: mq.apply_(c, s, plain=True, tensor=tensor)
+    if name in ("batch_pure", "batch_pure_small"):
+        # the uneven batch's pure part (512 states of 10..22 qubits, HEA depth 8, per-sample
+        # angles), applied eagerly group by group; _small keeps the sizes below 18 qubits
+        rng2 = W.rng_for(2)
+        sizes = rng2.integers(10, 23, size=512)
+        counts = {int(n): int((sizes == n).sum()) for n in np.unique(sizes)}
+        if name == "batch_pure_small":
+            counts = {n: B for n, B in counts.items() if n < 18}
+        groups = []
+        for n, B in sorted(counts.items()):
+            c = W.hea_circuit(n, 8)
+            th = np.random.default_rng(n).uniform(0, 2 * np.pi, size=(B, c.nparameters()))
+            groups.append((c, mq.BatchStateVector(n, B), th))
+
+        def step():
+            for c, st, th in groups:
+                st.set_zero()
+                mq.apply_(c, st, theta=th)
+        return f"uneven batch, pure part: {sum(counts.values())} states, sizes {min(counts)}..{max(counts)}", step
     raise ValueError(f"unknown kernel case {name}")
 
 
-KERNEL_CASES = ("dense1_low", "dense1_high", "tile", "density", "pauli", "adjoint", "marginal", "dmma", "dense5")
+KERNEL_CASES = ("dense1_low", "dense1_high", "tile", "density", "pauli", "adjoint", "marginal", "dmma", "dense5",
+                "batch_pure", "batch_pure_small")
 
 
 def kernel_workload(args):

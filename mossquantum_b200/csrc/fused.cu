@@ -1597,6 +1597,7 @@ int run_schedule(mb_circuit c, Schedule* S, double2* v, int nsamples, int64_t ms
   if (!S->frecs.empty()) {
     const int rows = mstride ? nsamples : 1;
     const int64_t work = int64_t(S->frecs.size()) * rows;
+    ProfScope ps("k_fuse", 0.0, st);
     k_fuse<<<unsigned((work + 127) / 128), 128, 0, st>>>(S->d_frecs, int(S->frecs.size()), S->d_fcomps, c->d_table,
                                                           mstride, xs, S->xrow, rows);
     MB_LAUNCHED();

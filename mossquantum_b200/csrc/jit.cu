@@ -182,6 +182,7 @@ struct StageGen {
   std::vector<int> nm;
   std::string pre = "a";  // variable prefix
   const std::map<int, int>* smap = nullptr;  // table offset -> slot of the pass's shared-memory copy
+  const std::map<int, int>* pmap = nullptr;  // per-sample entry -> slot of the tile's shared copy (spar)
 
   // Selector classification: register bit k (>= 0), or -1 with a runtime expression.
   int regbit(int sel) const {
@@ -212,6 +213,13 @@ struct StageGen {
       auto it = smap->find(smat_key(m, e));
       if (it != smap->end()) {
         const std::string x = "smat[" + std::to_string(it->second) + "]";
+        return m.conj ? "cj(" + x + ")" : x;
+      }
+    }
+    if (pmap && m.param) {
+      auto it = pmap->find(smat_key(m, e));
+      if (it != pmap->end()) {
+        const std::string x = "spar[" + std::to_string(it->second) + "]";
         return m.conj ? "cj(" + x + ")" : x;
       }
     }
@@ -570,6 +578,34 @@ static SharedMats shared_mats(const Pass& p, bool with_params) {
   return sm;
 }
 
+// Per-sample matrix elements of a multi-sample pass (parametric gates, fused per-sample
+// products): every tile belongs to one sample, so the tile's elements are copied into shared
+// memory once per tile and the stages read them from there. At most 1024 entries (16 KB).
+static SharedMats per_sample_mats(const Pass& p) {
+  SharedMats sm;
+  const MOp* cur = nullptr;
+  auto add = [&](int e) {
+    const int key = smat_key(*cur, e);
+    if (sm.slot.count(key)) return;
+    sm.slot[key] = int(sm.offs.size());
+    sm.offs.push_back(key);
+  };
+  for (const MOp& m : p.mops) {
+    if (!m.param) continue;
+    cur = &m;
+    switch (m.type) {
+      case MOP_U1: case MOP_CTRL: case MOP_RROT: case MOP_IROT: for (int e = 0; e < 4; ++e) add(e); break;
+      case MOP_LIFT: add(0); break;
+      case MOP_U2: for (int e = 0; e < 16; ++e) add(e); break;
+      case MOP_DIAG: for (int e = 0; e < (1 << m.nsel); ++e) if ((m.active >> e) & 1) add(e); break;
+      case MOP_CPHASE: if (!m.r1) add(0); break;
+      default: break;
+    }
+  }
+  if (sm.offs.size() > 1024) sm = SharedMats();
+  return sm;
+}
+
 // File-scope table of the offsets and the in-kernel copy (run before the kernel's first barrier).
 static std::string shared_mats_decl(const SharedMats& sm) {
   if (sm.offs.empty()) return "";
@@ -595,7 +631,13 @@ std::string jit_tile_source(const Pass& p, int R, int N, bool stage_params, int 
   const int threads = 1 << (p.t - R);
   const TmaGeom& g = p.geom;
   const SharedMats smats = shared_mats(p, stage_params);
+  const SharedMats pmats = stage_params ? SharedMats() : per_sample_mats(p);
   o << kPrelude << shared_mats_decl(smats);
+  if (!pmats.offs.empty()) {
+    o << "__constant__ int k_poffs[" << pmats.offs.size() << "] = {";
+    for (size_t i = 0; i < pmats.offs.size(); ++i) o << (i ? "," : "") << pmats.offs[i];
+    o << "};\n";
+  }
   o << "extern \"C\" __global__ void __launch_bounds__(" << threads << ", " << std::max(1, ctas)
     << ") mbk_tile(const __grid_constant__ TMap tmap, "
     << "const double2* __restrict__ tab, const double2* __restrict__ xtab, const double2* __restrict__ xtabs, "
@@ -603,6 +645,7 @@ std::string jit_tile_source(const Pass& p, int R, int N, bool stage_params, int 
     << "long long ntiles, u32* err) {\n";
   o << "  extern __shared__ unsigned char smem_raw[];\n  __shared__ __align__(8) u64 bar[2];\n  __shared__ int s_abort;\n";
   o << shared_mats_fill(smats);
+  if (!pmats.offs.empty()) o << "  __shared__ double2 spar[" << pmats.offs.size() << "];\n";
   o << "  double2* buf0 = (double2*)(((unsigned long long)smem_raw + 1023ull) & ~1023ull);\n";
   o << "  double2* bufs[2] = {buf0, buf0 + " << (1 << p.t) << "};\n";
   o << "  const u32 tx = threadIdx.x;\n";
@@ -660,6 +703,11 @@ std::string jit_tile_source(const Pass& p, int R, int N, bool stage_params, int 
   o << geom("tile", "");
   o << "    const double2* tb = tab + (long long)b * tstride;\n    (void)tb;\n";
   o << "    const double2* xb = xtabs + (long long)b * xrow;\n    (void)xb;\n";
+  if (!pmats.offs.empty()) {
+    // this tile's per-sample elements (the previous tile's stages ended with a barrier)
+    o << "    for (u32 i = tx; i < " << pmats.offs.size() << "u; i += blockDim.x) { const int mo = k_poffs[i]; "
+      << "spar[i] = (mo & " << kXrowKey << ") ? __ldg(xb + (mo & " << (kXtabFlag - 1) << ")) : __ldg(tb + mo); }\n";
+  }
   o << "    double2* tl = bufs[cur];\n";
   o << "    if (!mbar_wait(&bar[cur], cur ? ph1 : ph0)) { atomicOr(err, 1u); s_abort = 1; }\n";
   o << "    if (cur) ph1 ^= 1u; else ph0 ^= 1u;\n    __syncthreads();\n    if (s_abort) break;\n";
@@ -673,6 +721,7 @@ std::string jit_tile_source(const Pass& p, int R, int N, bool stage_params, int 
     for (int j = 0; j < A; ++j) o << "      a" << j << " = tl[swz(lb | " << reg_off_const(j, R, sd.reg) << ")];\n";
     StageGen sg{R, sd.reg, o, false, std::vector<int>(A)};
     sg.smap = &smats.slot;
+    if (!pmats.offs.empty()) sg.pmap = &pmats.slot;
     for (int j = 0; j < A; ++j) sg.nm[j] = j;
     for (int q = 0; q < sd.nops; ++q) sg.emit(p.mops[sd.op0 + q]);
     for (int j = 0; j < A; ++j) o << "      tl[swz(lb | " << reg_off_const(j, R, sd.reg) << ")] = " << sg.v(j) << ";\n";
