@@ -258,6 +258,82 @@ extern "C" int mb_adjoint(mb_circuit c, mb_observable o, mb_state init, const do
     }
   }
 
+  // Fused path for density matrices (density initial states, or pure ones promoted because the
+  // circuit has channels): dual-state passes that reverse single-qubit channels with their
+  // inverses. Segments end at checkpoint_every and wherever the product of the channels'
+  // ||S^-1||_2 would pass 100, so the rounding error of the uncomputed y stays bounded; y is
+  // reset to the segment's checkpoint after each reversed segment. Shared parameters with
+  // uniform sample weights (the gradient sums over the samples and is scaled once).
+  bool uniform_w = true;
+  for (int b = 1; b < B; ++b) uniform_w = uniform_w && w[b] == w[0];
+  if (is_dm && uniform_w && 2 * n >= 8 && nops_all > 0 && !(plain_env && atoi(plain_env))) {
+    std::vector<int> cuts = {0};
+    bool ok = true;
+    double growth = 1.0;
+    int seg_start = 0;
+    for (int i = 0; i < nops_all && ok; ++i) {
+      const double gr = reverse_growth(c, c->ops[i]);
+      if (!std::isfinite(gr)) {
+        ok = false;
+        break;
+      }
+      const bool by_k = checkpoint_every > 0 && i - seg_start >= checkpoint_every;
+      if (i > seg_start && (by_k || growth * gr > 100.0)) {
+        cuts.push_back(i);
+        seg_start = i;
+        growth = 1.0;
+      }
+      growth *= gr;
+    }
+    cuts.push_back(nops_all);
+    const int Sd = int(cuts.size()) - 1;
+    std::vector<Schedule*> adj(Sd, nullptr), fwd(Sd, nullptr);
+    for (int s2 = 0; s2 < Sd && ok; ++s2)
+      ok = adjoint_prepare(c, n, cuts[s2], cuts[s2 + 1], &adj[s2], 1, B) == MB_OK &&
+           get_schedule_ex(c, n, 1, 0, cuts[s2], cuts[s2 + 1], B, &fwd[s2]) == MB_OK;
+    if (ok) {
+      std::vector<std::unique_ptr<Buf>> ck(Sd);
+      for (int s2 = 0; s2 < Sd; ++s2) {
+        if (s2 > 0 || Sd > 1) {
+          ck[s2].reset(new Buf());
+          if ((rc = ck[s2]->alloc(sbytes))) return rc;
+          MB_CHECK_CUDA(cudaMemcpyAsync(ck[s2]->p, y.p, sbytes, cudaMemcpyDeviceToDevice, st));
+        }
+        if ((rc = run_schedule(c, fwd[s2], y.p, B, 0))) return rc;
+      }
+      mb_state_s view;
+      view.kind = init->kind >= MB_BATCH_PURE ? MB_BATCH_DENSITY : MB_DENSITY;
+      view.n = n;
+      view.batch = B;
+      view.dim = int64_t(1) << n;
+      view.elems = elems;
+      view.d = y.p;
+      if ((rc = expect_keys(o, &view))) return rc;
+      std::vector<double2> r(B);
+      MB_CHECK_CUDA(cudaMemcpyAsync(r.data(), g_ctx.results, sizeof(double2) * B, cudaMemcpyDeviceToHost, st));
+      // seed: z H' applied to the identity, the dense matrix H per sample (expectation.jl:69-73)
+      {
+        Buf ident;
+        if ((rc = ident.alloc(sbytes))) return rc;
+        if ((rc = launch_identity_density(ident.p, n, B, st))) return rc;
+        if ((rc = observable_apply(o, ident.p, delta.p, n, 1, B))) return rc;
+        MB_CHECK_CUDA(cudaStreamSynchronize(st));
+      }
+      double v = 0;
+      for (int b = 0; b < B; ++b) v += w[b] * r[b].x;
+      *value = v;
+      for (int s2 = Sd - 1; s2 >= 0; --s2) {
+        if ((rc = run_adjoint_schedule(c, adj[s2], y.p, delta.p, d_g))) return rc;
+        if (s2 > 0 && ck[s2]) MB_CHECK_CUDA(cudaMemcpyAsync(y.p, ck[s2]->p, sbytes, cudaMemcpyDeviceToDevice, st));
+      }
+      std::vector<double> gh(std::max(1, c->nslots));
+      if (c->nslots) MB_CHECK_CUDA(cudaMemcpyAsync(gh.data(), d_g, sizeof(double) * c->nslots, cudaMemcpyDeviceToHost, st));
+      MB_CHECK_CUDA(cudaStreamSynchronize(st));
+      for (int q = 0; q < c->nslots; ++q) grad[q] = w[0] * gh[q];
+      return MB_OK;
+    }
+  }
+
   // Segments of k instructions; checkpoint where a segment holds a channel or k was given.
   const int nops = int(c->ops.size());
   int k = checkpoint_every;

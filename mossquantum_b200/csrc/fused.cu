@@ -198,6 +198,7 @@ struct FOp {
   bool neg = false;           // MOP_CPHASE with factor -1 (a sign flip)
   int slot = -1;              // MOP_GRAD / MOP_GRADP: parameter slot
   int pauli = 0;              // MOP_GRADP: generator code (1 X, 2 Y, 3 Z, 4 PHASE)
+  int only = 0;               // reverse sweeps: 0 both states, 1 y only, 2 delta only
   // plain fallback
   int cls = CLS_DENSE;
   int mat_off = 0, mode = MAT_PLAIN;
@@ -759,41 +760,155 @@ static void build_fops(mb_circuit c, int n, int dm, bool dagger, std::vector<FOp
 
 // Reverse sweep of a pure-state circuit range: U' of every gate in reverse order, each active
 // parameter followed by its gradient accumulator (generator D in ordered form at gen_off).
-static bool build_adjoint_fops(mb_circuit c, int lo, int hi, std::vector<FOp>& out) {
+// Inverse of a 4x4 complex matrix (column-major) by Gauss-Jordan elimination with partial
+// pivoting; false when singular.
+static bool invert4(const cd* M, cd* inv) {
+  cd a[4][8];
+  for (int r = 0; r < 4; ++r)
+    for (int c2 = 0; c2 < 4; ++c2) {
+      a[r][c2] = M[r + 4 * c2];
+      a[r][c2 + 4] = r == c2 ? cd(1, 0) : cd(0, 0);
+    }
+  for (int col = 0; col < 4; ++col) {
+    int piv = col;
+    for (int r = col + 1; r < 4; ++r)
+      if (std::abs(a[r][col]) > std::abs(a[piv][col])) piv = r;
+    if (!(std::abs(a[piv][col]) > 1e-300)) return false;
+    if (piv != col)
+      for (int k = 0; k < 8; ++k) std::swap(a[piv][k], a[col][k]);
+    const cd d = a[col][col];
+    for (int k = 0; k < 8; ++k) a[col][k] /= d;
+    for (int r = 0; r < 4; ++r)
+      if (r != col) {
+        const cd f = a[r][col];
+        for (int k = 0; k < 8; ++k) a[r][k] -= f * a[col][k];
+      }
+  }
+  for (int r = 0; r < 4; ++r)
+    for (int c2 = 0; c2 < 4; ++c2) inv[r + 4 * c2] = a[r][c2 + 4];
+  return true;
+}
+
+// Spectral norm of a 4x4 complex matrix (power iteration on A'A).
+static double norm2_4(const cd* A) {
+  cd v[4] = {1, 0.5, 0.25, 0.125};
+  double s = 0;
+  for (int it = 0; it < 100; ++it) {
+    cd w[4], u[4];
+    for (int r = 0; r < 4; ++r) {
+      w[r] = 0;
+      for (int k = 0; k < 4; ++k) w[r] += A[r + 4 * k] * v[k];
+    }
+    for (int r = 0; r < 4; ++r) {
+      u[r] = 0;
+      for (int k = 0; k < 4; ++k) u[r] += std::conj(A[k + 4 * r]) * w[k];
+    }
+    double nu = 0;
+    for (int r = 0; r < 4; ++r) nu += std::norm(u[r]);
+    nu = std::sqrt(nu);
+    if (!(nu > 0)) return 0;
+    for (int r = 0; r < 4; ++r) v[r] = u[r] / nu;
+    s = std::sqrt(nu);
+  }
+  return s;
+}
+
+// Growth of rounding errors in y when the reverse sweep uncomputes through instruction op:
+// 1 for gates (unitary), ||S^-1||_2 for a single-qubit channel, infinity when it cannot be
+// inverted.
+double growth_of(mb_circuit c, const COp& op) {
+  if (op.kind != MB_OP_CHANNEL) return 1.0;
+  if (op.k != 1) return INFINITY;
+  cd S[16], inv[16];
+  for (int e = 0; e < 16; ++e) S[e] = cd(c->fixed_table[op.mat_off + e].x, c->fixed_table[op.mat_off + e].y);
+  if (!invert4(S, inv)) return INFINITY;
+  return norm2_4(inv);
+}
+
+// Gradient micro-op of one active parameter on the bits of `shift` (0: pure state or the row
+// bits; n: the column bits of a density matrix, where the generator enters conjugated).
+static FOp grad_fop(const COp& op, int shift) {
+  FOp g;
+  g.type = MOP_GRAD;
+  g.nb = op.k;
+  for (int j = 0; j < op.k; ++j) g.bits[j] = op.pos[j] + shift;
+  g.ntgt = op.k;
+  for (int j = 0; j < op.k; ++j) g.tgt[j] = g.bits[j];
+  const int d = 1 << op.k;
+  for (int r = 0; r < d; ++r)
+    for (int cc = 0; cc < d; ++cc) g.off[r + d * cc] = op.gen_off + r + d * cc;
+  g.param = op.parametric ? 1 : 0;
+  g.conj = shift ? 1 : 0;
+  g.slot = op.slot;
+  if (op.k == 1 && op.parametric) {
+    // Rotation families have constant generators (k_bind's family_matrix): no table reads
+    // and four multiply-adds per pair instead of a 2x2 apply and a dot product. On column bits
+    // conj((i/2)X) = -(i/2)X, conj((i/2)Y) = (i/2)Y, conj((i/2)Z) = -(i/2)Z, conj(diag(0,-i))
+    // = -diag(0,-i).
+    const int code = op.family == MB_FAM_RX ? 1 : op.family == MB_FAM_RY ? 2 : op.family == MB_FAM_RZ ? 3
+                     : op.family == MB_FAM_PHASE ? 4 : 0;
+    if (code) {
+      g.type = MOP_GRADP;
+      g.pauli = code;
+      g.neg = ((op.flags & MB_OPF_ADJOINT) != 0) != (shift != 0 && code != 2);
+      g.conj = 0;
+    }
+  }
+  finalize_masks(g);
+  g.nd = g.all;
+  return g;
+}
+
+// Reverse sweep of a circuit range: U' of every gate in reverse order (on a density matrix: on
+// the row bits and conj(U)' on the column bits), each active parameter followed by its gradient
+// accumulator (generator D in ordered form at gen_off; density matrices: D on the row bits and
+// conj(D) on the column bits, _density_gate_gradient!, circuit.jl:155-172). A single-qubit
+// channel S updates delta with S' and uncomputes y with S^-1 (inverted here; the caller bounds
+// the error growth with reverse_growth). Returns false when the range has an instruction the
+// passes cannot reverse.
+static bool build_adjoint_fops(mb_circuit c, int lo, int hi, std::vector<FOp>& out, int dm = 0, int n = 0,
+                               std::vector<double2>* xt = nullptr) {
   out.clear();
   for (int oi = hi - 1; oi >= lo; --oi) {
     const COp& op = c->ops[oi];
+    if (op.kind == MB_OP_CHANNEL) {
+      if (!dm || op.k != 1 || !xt) return false;
+      cd S[16], inv[16];
+      for (int e = 0; e < 16; ++e) S[e] = cd(c->fixed_table[op.mat_off + e].x, c->fixed_table[op.mat_off + e].y);
+      if (!invert4(S, inv)) return false;
+      FOp d;
+      d.type = MOP_U2;
+      d.nb = 2;
+      d.bits[0] = d.tgt[0] = op.pos[0];
+      d.bits[1] = d.tgt[1] = op.pos[0] + n;
+      d.ntgt = 2;
+      d.cls = CLS_DENSE;
+      for (int r = 0; r < 4; ++r)
+        for (int cc = 0; cc < 4; ++cc) d.off[r + 4 * cc] = op.mat_off + cc + 4 * r;  // S' = conj(S^T)
+      d.conj = 1;
+      d.only = 2;
+      finalize_masks(d);
+      FOp y = d;
+      y.conj = 0;
+      y.only = 1;
+      for (int e = 0; e < 16; ++e) y.off[e] = xtab_push(xt, make_double2(inv[e].real(), inv[e].imag()));
+      out.push_back(d);
+      out.push_back(y);
+      continue;
+    }
     if (op.kind != MB_OP_GATE) return false;
     FOp u = gate_fop(c, op, 0, 0, true);
     mark_unfusable_masks(u);
     out.push_back(u);
+    if (dm) {
+      FOp uc = gate_fop(c, op, n, 1, true);
+      mark_unfusable_masks(uc);
+      out.push_back(uc);
+    }
     if (op.gen_off >= 0) {
       if (op.k > 2) return false;
-      FOp g;
-      g.type = MOP_GRAD;
-      g.nb = op.k;
-      for (int j = 0; j < op.k; ++j) g.bits[j] = op.pos[j];
-      g.ntgt = op.k;
-      for (int j = 0; j < op.k; ++j) g.tgt[j] = g.bits[j];
-      const int d = 1 << op.k;
-      for (int r = 0; r < d; ++r)
-        for (int cc = 0; cc < d; ++cc) g.off[r + d * cc] = op.gen_off + r + d * cc;
-      g.param = op.parametric ? 1 : 0;
-      g.slot = op.slot;
-      if (op.k == 1 && op.parametric) {
-        // Rotation families have constant generators (k_bind's family_matrix): no table reads
-        // and four multiply-adds per pair instead of a 2x2 apply and a dot product.
-        const int code = op.family == MB_FAM_RX ? 1 : op.family == MB_FAM_RY ? 2 : op.family == MB_FAM_RZ ? 3
-                         : op.family == MB_FAM_PHASE ? 4 : 0;
-        if (code) {
-          g.type = MOP_GRADP;
-          g.pauli = code;
-          g.neg = (op.flags & MB_OPF_ADJOINT) != 0;
-        }
-      }
-      finalize_masks(g);
-      g.nd = g.all;
-      out.push_back(g);
+      out.push_back(grad_fop(op, 0));
+      if (dm) out.push_back(grad_fop(op, n));
     }
   }
   return true;
@@ -951,6 +1066,7 @@ static void plan_stages(const std::vector<FOp>& fops, const std::vector<int>& op
         m.type = int16_t(f.type);
         m.conj = int16_t(f.conj);
         m.param = int16_t(f.param);
+        m.only = int16_t(f.only);
         std::memcpy(m.off, f.off, sizeof(m.off));
         auto regidx = [&](int gbit) {
           for (int k = 0; k < R; ++k)
@@ -1362,6 +1478,8 @@ static Tuning tuning_for(int N) {
 
 static void prepare_jit(Schedule* S);
 
+double reverse_growth(mb_circuit c, const COp& op) { return growth_of(c, op); }
+
 bool jit_sizes(int nbits) { return want_jit(nbits) && jit_available(); }
 
 int get_schedule_ex(mb_circuit c, int n, int dm, int adjoint, int lo, int hi, int nsamples, Schedule** out) {
@@ -1401,8 +1519,8 @@ int get_schedule_ex(mb_circuit c, int n, int dm, int adjoint, int lo, int hi, in
   S->adjoint = adjoint;
   S->fuse = tu.fuse != 0;
   if (adjoint) {
-    if (dm || !build_adjoint_fops(c, lo, hi, S->fops)) {
-      set_error("the fused adjoint supports pure-state circuits with 1- and 2-qubit parameters");
+    if (!build_adjoint_fops(c, lo, hi, S->fops, dm, n, &S->xtab)) {
+      set_error("the fused adjoint supports circuits with 1- and 2-qubit parameters and single-qubit channels");
       return MB_EUNSUPPORTED;
     }
   } else {
@@ -1518,9 +1636,9 @@ static int tile_ctas(int t) {
 // CTAs per SM of a dual-state adjoint pass: what shared memory holds of four double-buffered
 // tiles plus the gradient slots (allowing 8 KB), capped at MB_ADJOINT_CTAS (default 3); the
 // kernel's launch bounds ask the compiler to fit that many CTAs in the register file.
-static int adjoint_ctas(int t) {
+static int adjoint_ctas(int t, int dm = 0) {
   const size_t shm = (size_t(64) << t) + 1024 + 8 * 1024;
-  int cap = 3;
+  int cap = dm ? 2 : 3;  // density passes hold 4x4 channel operators for both states: 2 CTAs keep them unspilled
   if (const char* e = getenv("MB_ADJOINT_CTAS")) cap = std::max(1, std::min(4, atoi(e)));  // gpart holds 4 per SM
   return std::max(1, std::min(cap, int((227 * 1024) / (shm + 256))));
 }
@@ -1537,7 +1655,7 @@ static void prepare_jit(Schedule* S) {
   for (Pass& p : S->passes) {
     if (p.kind == PASS_TILE && !S->adjoint) p.ctas = tile_ctas(p.t);
     if (p.kind == PASS_TILE && S->adjoint) {
-      p.ctas = adjoint_ctas(p.t);
+      p.ctas = adjoint_ctas(p.t, S->dm);
       src.push_back(jit_adjoint_source(p, S->R, S->N, single, p.ctas));
     }
     else if (p.kind == PASS_TILE) src.push_back(jit_tile_source(p, S->R, S->N, single, p.ctas));
@@ -1691,7 +1809,8 @@ int run_schedule(mb_circuit c, Schedule* S, double2* v, int nsamples, int64_t ms
 }
 
 // Reverse sweep over an adjoint schedule: U' on y and delta in every pass, gradient
-// contributions added into d_grad (one entry per parameter slot).
+// contributions added into d_grad (one entry per parameter slot), summed over the schedule's
+// samples (stored back to back; they share the parameters).
 int run_adjoint_schedule(mb_circuit c, Schedule* S, double2* y, double2* d, double* d_grad) {
   cudaStream_t st = g_ctx.stream;
   const int N = S->N;
@@ -1716,23 +1835,25 @@ int run_adjoint_schedule(mb_circuit c, Schedule* S, double2* y, double2* d, doub
     return rc;
   }
   cudaMemsetAsync(gcount, 0, sizeof(unsigned), st);
+  const int B = S->nsamples;
   for (const Pass& p : S->passes) {
     if (p.kind == PASS_PLAIN) {
-      if ((rc = plain_fop_launch(c, S->fops[p.plain_fop], y, elems, 1, 0, st))) break;
-      if ((rc = plain_fop_launch(c, S->fops[p.plain_fop], d, elems, 1, 0, st))) break;
+      const FOp& f = S->fops[p.plain_fop];
+      if (f.only != 2 && (rc = plain_fop_launch(c, f, y, elems, B, 0, st))) break;
+      if (f.only != 1 && (rc = plain_fop_launch(c, f, d, elems, B, 0, st))) break;
       continue;
     }
     CUtensorMap my, md;
-    if ((rc = make_tmap(p, y, N, 1, &my)) || (rc = make_tmap(p, d, N, 1, &md))) break;
+    if ((rc = make_tmap(p, y, N, B, &my)) || (rc = make_tmap(p, d, N, B, &md))) break;
     const int threads = 1 << (p.t - S->R);
     const int nw = std::max(1, threads / 32);
     const size_t shm = (size_t(64) << p.t) + 1024 + sizeof(double) * std::max<size_t>(1, p.grad_slots.size() * nw);
     const int per_sm = std::max(1, int((227 * 1024) / (shm + 256)));
-    const int64_t ntiles = int64_t(1) << (N - p.t);
+    const int64_t tps = int64_t(1) << (N - p.t), ntiles = tps * B;
     const int grid = int(std::min<int64_t>(ntiles, int64_t(g_ctx.sm_count) * std::min(per_sm, std::max(1, p.ctas))));
-    ProfScope ps("k_adjoint_pass_jit", 64.0 * double(elems), st, pass_flops_per_amp(p, true) * double(elems));
-    rc = jit_launch_adjoint((CUfunction)p.jit_fn, &my, &md, c->d_table, 0, ntiles, ntiles, g_ctx.flags + 2, gpart, gcount,
-                            d_grad, S->d_gslots + p.grad_off, threads, shm, grid, st);
+    ProfScope ps("k_adjoint_pass_jit", 64.0 * double(elems) * B, st, pass_flops_per_amp(p, true) * double(elems) * B);
+    rc = jit_launch_adjoint((CUfunction)p.jit_fn, &my, &md, c->d_table, 0, tps, ntiles, g_ctx.flags + 2, gpart, gcount,
+                            d_grad, S->d_gslots + p.grad_off, S->d_xtab, threads, shm, grid, st);
     ++launch_counter();
     if (rc) break;
   }
@@ -1743,9 +1864,9 @@ int run_adjoint_schedule(mb_circuit c, Schedule* S, double2* y, double2* d, doub
 
 // Adjoint schedule for instructions [lo, hi) with its specialised kernels compiled; fails
 // (MB_EUNSUPPORTED) when the range cannot run fused.
-int adjoint_prepare(mb_circuit c, int n, int lo, int hi, Schedule** out) {
+int adjoint_prepare(mb_circuit c, int n, int lo, int hi, Schedule** out, int dm, int nsamples) {
   Schedule* S = nullptr;
-  int rc = get_schedule_ex(c, n, 0, 1, lo, hi, 1, &S);
+  int rc = get_schedule_ex(c, n, dm, 1, lo, hi, nsamples, &S);
   if (rc) return rc;
   prepare_jit(S);
   if (S->jit != 1 || (1 << (S->t - S->R)) < 32) {
@@ -1859,19 +1980,21 @@ extern "C" int mb_schedule_info(const mb_op* ops, size_t nops, int n, int dm, in
     // Development aid: the specialised kernel source of every pass (compiled offline to read
     // register and spill counts); with MB_JIT_DUMP_ADJOINT the dual-state passes of the
     // circuit's reverse sweep (pure states) as well.
-    if (getenv("MB_JIT_DUMP_ADJOINT") && !dm) {
+    if (getenv("MB_JIT_DUMP_ADJOINT")) {
       mb::Schedule A;
       A.N = N;
-      A.t = std::min(std::min(tile_bits, 11), N);
-      A.R = 4;
+      A.dm = dm ? 1 : 0;
+      A.nsamples = nsamples;
+      A.t = std::min(std::min(tile_bits, 10), N);
+      A.R = 3;
       if (const char* e = getenv("MB_ADJOINT_REG_BITS")) A.R = std::max(3, std::min(4, atoi(e)));
       A.adjoint = 1;
-      if (mb::build_adjoint_fops(&c, 0, int(c.ops.size()), A.fops)) {
-        mb::build_schedule(A, 1, false);
+      if (mb::build_adjoint_fops(&c, 0, int(c.ops.size()), A.fops, A.dm, n, &A.xtab)) {
+        mb::build_schedule(A, nsamples, false);
         int j = 0;
         for (mb::Pass& ps : A.passes) {
           if (ps.kind != mb::PASS_TILE) continue;
-          const std::string src = mb::jit_adjoint_source(ps, A.R, N, true, mb::adjoint_ctas(ps.t));
+          const std::string src = mb::jit_adjoint_source(ps, A.R, N, nsamples == 1, mb::adjoint_ctas(ps.t, A.dm));
           char path[512];
           snprintf(path, sizeof(path), "%s/adj_%03d.cu", dir, j++);
           if (FILE* f = fopen(path, "w")) {

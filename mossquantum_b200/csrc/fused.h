@@ -39,6 +39,7 @@ struct MOp {
   uint32_t active;   // MOP_DIAG: local indices whose factor is applied
   int16_t conj;      // read the matrix conjugated (density-matrix column pass)
   int16_t param;     // per-sample matrix row (parametric gate with per-sample theta)
+  int16_t only;      // reverse sweeps: 0 both states, 1 y only, 2 delta only
   int32_t off[16];   // matrix elements (double2 offsets in a sample's matrix table)
 };
 

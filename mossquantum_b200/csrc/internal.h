@@ -135,7 +135,12 @@ bool jit_sizes(int nbits);  // register sizes that run on the specialised (NVRTC
 int get_schedule_ex(mb_circuit c, int n, int dm, int adjoint, int lo, int hi, int nsamples, Schedule** out);
 int run_schedule(mb_circuit c, Schedule* S, double2* v, int nsamples, int64_t mstride);
 int run_adjoint_schedule(mb_circuit c, Schedule* S, double2* y, double2* d, double* d_grad);
-int adjoint_prepare(mb_circuit c, int n, int lo, int hi, Schedule** out);
+// dm: the range runs on density matrices (single-qubit channels reversed with their inverses);
+// nsamples: samples stored back to back that share the parameters.
+int adjoint_prepare(mb_circuit c, int n, int lo, int hi, Schedule** out, int dm = 0, int nsamples = 1);
+// Growth factor of rounding errors in y when a reverse sweep uncomputes through op (1 for
+// gates, ||S^-1||_2 for a single-qubit channel, infinity if it cannot be inverted).
+double reverse_growth(mb_circuit c, const COp& op);
 void release_schedules(mb_circuit c);
 
 // adjoint.cu: single-sample reverse sweeps of one circuit application (serving loop)

@@ -747,12 +747,16 @@ static void emit_grad(std::ostringstream& o, const MOp& m, const StageGen& gy, c
                       const std::string& name) {
   const int A = 1 << R;
   const std::string tabn = m.param ? "tb" : "tab";
+  // generator entries, conjugated for the column bits of a density matrix
   auto L = [&](int e) {
     if (gy.smap) {
       auto it = gy.smap->find(smat_key(m, e));
-      if (it != gy.smap->end()) return "smat[" + std::to_string(it->second) + "]";
+      if (it != gy.smap->end()) {
+        const std::string x = "smat[" + std::to_string(it->second) + "]";
+        return m.conj ? "cj(" + x + ")" : x;
+      }
     }
-    return "ld(" + tabn + " + " + std::to_string(m.off[e]) + ")";
+    return std::string(m.conj ? "ldc" : "ld") + "(" + tabn + " + " + std::to_string(m.off[e]) + ")";
   };
   o << "{ double gs = 0.0;\n";
   if (m.type == MOP_GRADP) {
@@ -849,9 +853,8 @@ std::string jit_adjoint_source(const Pass& p, int R, int N, bool stage_params, i
   o << "extern \"C\" __global__ void __launch_bounds__(" << threads << ", " << std::max(1, ctas)
     << ") mbk_adj(const __grid_constant__ TMap tmy, "
     << "const __grid_constant__ TMap tmd, const double2* __restrict__ tab, long long tstride, long long tps, "
-    << "long long ntiles, u32* err, double* gpart, u32* gcount, double* gout, const int* __restrict__ gslot) {\n";
-  // reverse sweeps use no derived coefficients (their gates stay in the circuit's table)
-  o << "  const double2* __restrict__ xtab = nullptr; (void)xtab;\n";
+    << "long long ntiles, u32* err, double* gpart, u32* gcount, double* gout, const int* __restrict__ gslot, "
+    << "const double2* __restrict__ xtab) {\n";
   o << "  const double2* __restrict__ xtabs = nullptr; (void)xtabs;\n";
   o << "  extern __shared__ unsigned char smem_raw[];\n  __shared__ __align__(8) u64 bar[2];\n  __shared__ int s_abort;\n"
     << "  __shared__ bool lastcta;\n";
@@ -945,8 +948,8 @@ std::string jit_adjoint_source(const Pass& p, int R, int N, bool stage_params, i
         emit_grad(o, m, gy, gd, R, name);
         gnames.push_back(name);
       } else {
-        gy.emit(m);
-        gd.emit(m);
+        if (m.only != 2) gy.emit(m);   // channels: S^-1 on y only, S' on delta only
+        if (m.only != 1) gd.emit(m);
       }
     }
     if (!gnames.empty()) emit_grad_reduce(o, gnames, gacc0, nw);
@@ -976,11 +979,12 @@ std::string jit_adjoint_source(const Pass& p, int R, int N, bool stage_params, i
 
 int jit_launch_adjoint(CUfunction fn, const CUtensorMap* my, const CUtensorMap* md, const double2* tab, int64_t tstride,
                        int64_t tps, int64_t ntiles, unsigned* err, double* gpart, unsigned* gcount, double* gout,
-                       const int* gslot, int threads, size_t shm, int grid, cudaStream_t st) {
+                       const int* gslot, const double2* xtab, int threads, size_t shm, int grid, cudaStream_t st) {
   Drv& d = drv();
   if (d.setattr(fn, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, int(shm)) != CUDA_SUCCESS) return MB_EDEVICE;
   long long ts = tstride, tp = tps, nt = ntiles;
-  void* params[] = {(void*)my, (void*)md, (void*)&tab, &ts, &tp, &nt, &err, &gpart, &gcount, &gout, (void*)&gslot};
+  void* params[] = {(void*)my, (void*)md, (void*)&tab, &ts, &tp, &nt, &err, &gpart, &gcount, &gout, (void*)&gslot,
+                    (void*)&xtab};
   if (d.launch(fn, grid, 1, 1, threads, 1, 1, unsigned(shm), (CUstream)st, params, nullptr) != CUDA_SUCCESS) {
     set_error("JIT adjoint launch failed");
     return MB_EDEVICE;

@@ -30,7 +30,7 @@ int jit_launch_tile(CUfunction fn, const CUtensorMap* map, const double2* tab, c
 std::string jit_adjoint_source(const Pass& p, int R, int N, bool stage_params, int ctas = 1);
 int jit_launch_adjoint(CUfunction fn, const CUtensorMap* my, const CUtensorMap* md, const double2* tab, int64_t tstride,
                        int64_t tps, int64_t ntiles, unsigned* err, double* gpart, unsigned* gcount, double* gout,
-                       const int* gslot, int threads, size_t shm, int grid, cudaStream_t st);
+                       const int* gslot, const double2* xtab, int threads, size_t shm, int grid, cudaStream_t st);
 int jit_launch_reg(CUfunction fn, double2* v, const double2* tab, const double2* xtab, const double2* xtabs,
                    int64_t xrow, int64_t tstride, int64_t groups, int nsamples, int grid, cudaStream_t st);
 }  // namespace mb

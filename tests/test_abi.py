@@ -43,3 +43,17 @@ def test_init_without_gpu_reports_device_error():
     assert rc == N.MB_EDEVICE
     with pytest.raises(N.BackendError):
         N.check(rc)
+
+
+def test_no_undefined_internal_symbols():
+    """A library function declared in one file and (by mistake) defined with internal linkage in
+    another links into the shared library as an undefined symbol and fails only when loaded:
+    none of the library's own symbols may be undefined."""
+    import shutil
+    import subprocess
+    if not shutil.which("nm"):
+        pytest.skip("nm not available")
+    path = os.path.join(ROOT, "mossquantum_b200", "libmossb200.so")
+    out = subprocess.run(["nm", "-D", "-C", "--undefined-only", path], capture_output=True, text=True).stdout
+    bad = [ln for ln in out.splitlines() if "mb::" in ln or " mb_" in ln]
+    assert not bad, bad
