@@ -117,6 +117,22 @@ static int forward_range_dm(mb_circuit c, int n, int lo, int hi, double2* z) {
 int reverse_dm_single(mb_circuit c, int n, const double2* ckpt, double2* delta, double* d_grad,
                       double2* const* scratch) {
   const int k = int(c->ops.size());
+  // Fused: the state after c, recomputed from the checkpoint with the fused passes, then one
+  // dual-state reverse that uncomputes y through the channels' inverses (when their error
+  // growth over c stays within 100).
+  {
+    double growth = 1.0;
+    for (const COp& op : c->ops) growth *= reverse_growth(c, op);
+    const char* plain_env = getenv("MB_ADJOINT_PLAIN");
+    Schedule *adj = nullptr, *fwd = nullptr;
+    if (k > 0 && 2 * n >= 8 && growth <= 100.0 && !(plain_env && atoi(plain_env)) &&
+        adjoint_prepare(c, n, 0, k, &adj, 1, 1) == MB_OK && get_schedule_ex(c, n, 1, 0, 0, k, 1, &fwd) == MB_OK) {
+      const size_t sbytes = sizeof(double2) * (size_t(1) << (2 * n));
+      MB_CHECK_CUDA(cudaMemcpyAsync(scratch[0], ckpt, sbytes, cudaMemcpyDeviceToDevice, g_ctx.stream));
+      if (int rc = run_schedule(c, fwd, scratch[0], 1, 0)) return rc;
+      return run_adjoint_schedule(c, adj, scratch[0], delta, d_grad);
+    }
+  }
   int m = 1, nscratch = 1;
   dm_reverse_plan(c, &m, &nscratch);
   const int nseg = std::max(1, (k + m - 1) / m);
