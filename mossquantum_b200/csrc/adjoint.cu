@@ -11,6 +11,11 @@
 // Circuits with channels run on density matrices throughout (a pure initial state is
 // promoted first, DensityMatrix(psi), execution/channels.jl:19); this gives the same
 // parameter gradient as promoting at the first channel.
+// Fused paths: pure states (one sample) and density matrices (samples with shared parameters)
+// run the reverse as dual-state passes (y and Δ tiles together, gradients accumulated in the
+// pass). On density matrices a single-qubit channel is reversed by S' on Δ and S^-1 on y (the
+// input is uncomputed instead of recomputed); segments keep the product of ||S^-1||_2 within
+// 100 and y is reset to the segment's checkpoint after each, which bounds the rounding error.
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
