@@ -1,17 +1,18 @@
-// K4: fused Pauli-string expectation <psi|H|psi> (bit masks, phases and warp shuffles).
+// K4: fused Pauli-string expectation <psi|H|psi> and the adjoint seed H psi.
 //
 // The reference evaluates one dense local matrix per site key, one state pass per key
 // (src/observables/expectation.jl:12-33, backends/cpu/expectations/threaded.jl). Here every
 // term is decomposed into Pauli strings P = i^{#Y} X^x Z^z with a complex coefficient, and
 // the strings are grouped by their flip mask x. For amplitude index j,
 //   <psi|P|psi> = sum_j conj(psi_j) * i^{#Y} (-1)^{|(j^x)&z|} psi_{j^x}.
-// One pass gives each warp 32 consecutive low indices (lanes = bits 0..4) and each thread
-// 2^R amplitudes on R higher "register" bits. A group whose flip mask lies in those bits
-// finds its partner amplitude in the thread's registers (mirrored in shared memory for the
-// runtime flip) and a warp shuffle across lanes, so one read of the state evaluates every
-// such group; the diagonal group (x = 0: all Z/ZZ terms) needs no partner. Groups with flip
-// bits elsewhere run in further passes with other register bits; TFIM on n qubits takes
-// ceil((n-5)/5) passes instead of 2n-1.
+// A pass reads the state once in tiles of 1024 amplitudes: the five lane bits 0..4 times five
+// "register" bits chosen for the pass, staged in shared memory, so every group whose flip mask
+// lies in those ten local bits finds its partner amplitude in the tile. The sign of a string
+// splits into a tile-base part and a local part: strings whose Z mask avoids the local bits
+// give one constant per tile, strings inside the local bits are tabulated once per pass over
+// the 1024 local indices, and only strings that straddle both are evaluated per amplitude (a
+// couple per pass for nearest-neighbour Hamiltonians). TFIM on n qubits takes ceil((n-5)/5)
+// passes instead of 2n-1 key passes.
 #include <algorithm>
 #include <cmath>
 #include <complex>
@@ -24,19 +25,26 @@
 namespace mb {
 
 typedef std::complex<double> cdd;
-constexpr int kPR = 5;  // register bits per thread
-constexpr int kPThreads = 64;   // 64 x 32 mirrored amplitudes = 32 KiB of shared memory
+constexpr int kPR = 5;                    // register bits per pass
+constexpr int kPLocal = 5 + kPR;          // local bits of a tile (lanes + registers)
+constexpr int kPTile = 1 << kPLocal;      // 1024 amplitudes, 16 KiB of shared memory
+constexpr int kPThreads = 256;
+constexpr int kPPerThread = kPTile / kPThreads;
+constexpr int kPMaxGroups = 128;          // groups per pass (per-tile constants in shared memory)
 
 struct PString {
   uint64_t z;
   double2 c;  // coefficient including i^{#Y}
 };
 
+// One flip-mask group of one pass; its strings are stored in the program's own order:
+// [k0, k0 + nk) constant per tile, [v0, v0 + nv) straddling, the rest tabulated at `tab`.
 struct PGroup {
-  uint64_t x;  // flip mask (global bits)
-  int xlow;    // flip bits among lanes (bits 0..4)
-  int xreg;    // flip bits among the register bits (register index space)
-  int s0, ns;  // strings [s0, s0 + ns)
+  uint64_t x;   // flip mask (global bits, all among the pass's local bits)
+  int xl;       // flip mask as a local index (bits 0..4 lanes, 5..9 registers)
+  int k0, nk;
+  int v0, nv;
+  int tab;      // offset of the group's 1024-entry table, or -1
 };
 
 struct PPassArgs {
@@ -45,7 +53,8 @@ struct PPassArgs {
   int g0, ngroups;
   const PGroup* groups;
   const PString* strings;
-  int64_t threads_per_sample;
+  const double2* tables;
+  int64_t tiles_per_sample;
 };
 
 struct PauliProgram {
@@ -53,6 +62,7 @@ struct PauliProgram {
   std::vector<PPassArgs> passes;
   PGroup* d_groups = nullptr;
   PString* d_strings = nullptr;
+  double2* d_tables = nullptr;
 };
 
 struct PauliData {
@@ -63,18 +73,62 @@ struct PauliData {
 
 namespace {
 
-__device__ __forceinline__ double2 warp_sum2(double2 x) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    x.x += __shfl_down_sync(0xffffffffu, x.x, o);
-    x.y += __shfl_down_sync(0xffffffffu, x.y, o);
+// Global bits of local index l: lane bits as they are, register bit k at reg[k].
+__host__ __device__ __forceinline__ uint64_t local_bits(int l, const int* reg) {
+  uint64_t o = uint64_t(l & 31);
+  for (int k = 0; k < kPR; ++k)
+    if ((l >> (5 + k)) & 1) o |= uint64_t(1) << reg[k];
+  return o;
+}
+
+// Tile base: tile index T with zeros inserted at the lane bits and the register bits.
+__device__ __forceinline__ uint64_t tile_base(int64_t T, const int* reg) {
+  uint64_t base = uint64_t(T) << 5;
+  for (int k = 0; k < kPR; ++k) {
+    const int p = reg[k];
+    base = ((base >> p) << (p + 1)) | (base & ((uint64_t(1) << p) - 1));
   }
-  return x;
+  return base;
+}
+
+// Loads a tile into shared memory (each warp reads 32 consecutive amplitudes) and computes the
+// per-tile constants of the pass's groups.
+__device__ __forceinline__ void stage_tile(const double2* __restrict__ vs, uint64_t base, const uint64_t* loc,
+                                           const PPassArgs& a, double2* tile, double2* kconst) {
+#pragma unroll
+  for (int k = 0; k < kPPerThread; ++k) tile[threadIdx.x + k * kPThreads] = vs[base | loc[k]];
+  for (int gi = threadIdx.x; gi < a.ngroups; gi += kPThreads) {
+    const PGroup g = a.groups[a.g0 + gi];
+    double2 kc = cz();
+    for (int s = g.k0; s < g.k0 + g.nk; ++s) {
+      const PString ps = a.strings[s];
+      const bool odd = __popcll(base & ps.z) & 1;
+      kc.x += odd ? -ps.c.x : ps.c.x;
+      kc.y += odd ? -ps.c.y : ps.c.y;
+    }
+    kconst[gi] = kc;
+  }
+}
+
+// Factor of group g at local index l (tile base `base`, local bits `lb`).
+__device__ __forceinline__ double2 group_factor(const PGroup& g, const PPassArgs& a, const double2* kconst, int gi,
+                                                int l, uint64_t base, uint64_t lb) {
+  double2 f = kconst[gi];
+  if (g.tab >= 0) f = cadd(f, __ldg(a.tables + g.tab + l));
+  const uint64_t k_idx = (base | lb) ^ g.x;
+  for (int s = g.v0; s < g.v0 + g.nv; ++s) {
+    const PString ps = a.strings[s];
+    const bool odd = __popcll(k_idx & ps.z) & 1;
+    f.x += odd ? -ps.c.x : ps.c.x;
+    f.y += odd ? -ps.c.y : ps.c.y;
+  }
+  return f;
 }
 
 __global__ void __launch_bounds__(kPThreads) k_pauli_pass(const double2* __restrict__ v, const PPassArgs a,
                                                          double2* partials, unsigned* counters, double2* out) {
-  __shared__ double2 mirror[1 << kPR][kPThreads];
+  __shared__ double2 tile[kPTile];
+  __shared__ double2 kconst[kPMaxGroups];
   __shared__ double2 wp[kPThreads / 32];
   __shared__ bool last;
   const int b = blockIdx.y, G = gridDim.x;
@@ -82,58 +136,33 @@ __global__ void __launch_bounds__(kPThreads) k_pauli_pass(const double2* __restr
   int reg[kPR];
 #pragma unroll
   for (int k = 0; k < kPR; ++k) reg[k] = a.reg[k];
+  uint64_t loc[kPPerThread];
+#pragma unroll
+  for (int k = 0; k < kPPerThread; ++k) loc[k] = local_bits(threadIdx.x + k * kPThreads, reg);
   double2 acc = cz();
-  // Every lane of a warp iterates the same number of times (the per-sample thread count is
-  // a multiple of 32), so the shuffles below always see a full warp.
-  for (int64_t t0 = int64_t(blockIdx.x) * blockDim.x; t0 < a.threads_per_sample; t0 += int64_t(G) * blockDim.x) {
-    const int64_t t = t0 + threadIdx.x;
-    if (t >= a.threads_per_sample) break;  // whole warps leave together (count is a multiple of 32)
-    uint64_t base = uint64_t(t);
+  for (int64_t T = blockIdx.x; T < a.tiles_per_sample; T += G) {
+    const uint64_t base = tile_base(T, reg);
+    stage_tile(vs, base, loc, a, tile, kconst);
+    __syncthreads();
 #pragma unroll
-    for (int k = 0; k < kPR; ++k) {
-      const int p = reg[k];
-      base = ((base >> p) << (p + 1)) | (base & ((uint64_t(1) << p) - 1));
-    }
-    double2 amp[1 << kPR];
-#pragma unroll
-    for (int j = 0; j < (1 << kPR); ++j) {
-      uint64_t o = 0;
-#pragma unroll
-      for (int k = 0; k < kPR; ++k)
-        if ((j >> k) & 1) o |= uint64_t(1) << reg[k];
-      amp[j] = vs[base | o];
-      mirror[j][threadIdx.x] = amp[j];
-    }
-    __syncwarp();
-    for (int gi = 0; gi < a.ngroups; ++gi) {
-      const PGroup g = a.groups[a.g0 + gi];
-#pragma unroll
-      for (int j = 0; j < (1 << kPR); ++j) {
-        uint64_t o = 0;
-#pragma unroll
-        for (int k = 0; k < kPR; ++k)
-          if ((j >> k) & 1) o |= uint64_t(1) << reg[k];
-        const uint64_t k_idx = (base | o) ^ g.x;  // index of the partner amplitude
-        double2 p = g.xreg ? mirror[j ^ g.xreg][threadIdx.x] : amp[j];
-        if (g.xlow) {
-          p.x = __shfl_xor_sync(0xffffffffu, p.x, g.xlow);
-          p.y = __shfl_xor_sync(0xffffffffu, p.y, g.xlow);
-        }
-        double2 f = cz();
-        for (int s = 0; s < g.ns; ++s) {
-          const PString ps = a.strings[g.s0 + s];
-          const bool odd = __popcll(k_idx & ps.z) & 1;
-          f.x += odd ? -ps.c.x : ps.c.x;
-          f.y += odd ? -ps.c.y : ps.c.y;
-        }
+    for (int k = 0; k < kPPerThread; ++k) {
+      const int l = threadIdx.x + k * kPThreads;
+      const double2 amp = tile[l];
+      for (int gi = 0; gi < a.ngroups; ++gi) {
+        const PGroup g = a.groups[a.g0 + gi];
+        const double2 p = tile[l ^ g.xl];
+        const double2 f = group_factor(g, a, kconst, gi, l, base, loc[k]);
         // conj(psi_j) * psi_{j^x} * f
-        const double2 cp = make_double2(amp[j].x * p.x + amp[j].y * p.y, amp[j].x * p.y - amp[j].y * p.x);
+        const double2 cp = make_double2(amp.x * p.x + amp.y * p.y, amp.x * p.y - amp.y * p.x);
         acc = cfma(f, cp, acc);
       }
     }
-    __syncwarp();
+    __syncthreads();
   }
-  acc = warp_sum2(acc);
+  for (int o = 16; o > 0; o >>= 1) {
+    acc.x += __shfl_down_sync(0xffffffffu, acc.x, o);
+    acc.y += __shfl_down_sync(0xffffffffu, acc.y, o);
+  }
   if ((threadIdx.x & 31) == 0) wp[threadIdx.x >> 5] = acc;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -153,59 +182,36 @@ __global__ void __launch_bounds__(kPThreads) k_pauli_pass(const double2* __restr
 }
 
 // Seed variant: out (+)= scale * H psi, with (P psi)_j = i^{#Y} (-1)^{|(j^x)&z|} psi_{j^x}.
-// Same pass structure as k_pauli_pass; each pass adds the groups it holds.
+// Same tiles; the first pass writes, later passes add the groups they hold.
 __global__ void __launch_bounds__(kPThreads) k_pauli_apply(const double2* __restrict__ v, double2* __restrict__ out,
                                                           const PPassArgs a, double scale, int first) {
-  __shared__ double2 mirror[1 << kPR][kPThreads];
+  __shared__ double2 tile[kPTile];
+  __shared__ double2 kconst[kPMaxGroups];
   const int b = blockIdx.y, G = gridDim.x;
   const double2* vs = v + (int64_t(b) << a.n);
   double2* os = out + (int64_t(b) << a.n);
   int reg[kPR];
 #pragma unroll
   for (int k = 0; k < kPR; ++k) reg[k] = a.reg[k];
-  for (int64_t t0 = int64_t(blockIdx.x) * blockDim.x; t0 < a.threads_per_sample; t0 += int64_t(G) * blockDim.x) {
-    const int64_t t = t0 + threadIdx.x;
-    if (t >= a.threads_per_sample) break;
-    uint64_t base = uint64_t(t);
+  uint64_t loc[kPPerThread];
 #pragma unroll
-    for (int k = 0; k < kPR; ++k) {
-      const int p = reg[k];
-      base = ((base >> p) << (p + 1)) | (base & ((uint64_t(1) << p) - 1));
-    }
+  for (int k = 0; k < kPPerThread; ++k) loc[k] = local_bits(threadIdx.x + k * kPThreads, reg);
+  for (int64_t T = blockIdx.x; T < a.tiles_per_sample; T += G) {
+    const uint64_t base = tile_base(T, reg);
+    stage_tile(vs, base, loc, a, tile, kconst);
+    __syncthreads();
 #pragma unroll
-    for (int j = 0; j < (1 << kPR); ++j) {
-      uint64_t o = 0;
-#pragma unroll
-      for (int k = 0; k < kPR; ++k)
-        if ((j >> k) & 1) o |= uint64_t(1) << reg[k];
-      mirror[j][threadIdx.x] = vs[base | o];
-    }
-#pragma unroll
-    for (int j = 0; j < (1 << kPR); ++j) {
-      uint64_t o = 0;
-#pragma unroll
-      for (int k = 0; k < kPR; ++k)
-        if ((j >> k) & 1) o |= uint64_t(1) << reg[k];
-      double2 r = first ? cz() : os[base | o];
+    for (int k = 0; k < kPPerThread; ++k) {
+      const int l = threadIdx.x + k * kPThreads;
+      double2 r = first ? cz() : os[base | loc[k]];
       for (int gi = 0; gi < a.ngroups; ++gi) {
         const PGroup g = a.groups[a.g0 + gi];
-        double2 p = mirror[j ^ g.xreg][threadIdx.x];
-        if (g.xlow) {
-          p.x = __shfl_xor_sync(0xffffffffu, p.x, g.xlow);
-          p.y = __shfl_xor_sync(0xffffffffu, p.y, g.xlow);
-        }
-        const uint64_t k_idx = (base | o) ^ g.x;
-        double2 f = cz();
-        for (int s = 0; s < g.ns; ++s) {
-          const PString ps = a.strings[g.s0 + s];
-          const bool odd = __popcll(k_idx & ps.z) & 1;
-          f.x += odd ? -ps.c.x : ps.c.x;
-          f.y += odd ? -ps.c.y : ps.c.y;
-        }
-        r = cfma(cscale(f, scale), p, r);
+        const double2 f = group_factor(g, a, kconst, gi, l, base, loc[k]);
+        r = cfma(cscale(f, scale), tile[l ^ g.xl], r);
       }
-      os[base | o] = r;
+      os[base | loc[k]] = r;
     }
+    __syncthreads();
   }
 }
 
@@ -274,18 +280,21 @@ void pauli_free(mb_observable o) {
   for (PauliProgram* p : o->pauli->programs) {
     dev_free(p->d_groups);
     dev_free(p->d_strings);
+    dev_free(p->d_tables);
     delete p;
   }
   delete o->pauli;
   o->pauli = nullptr;
 }
 
-// Pass plan for an n-qubit state, or nullptr when the fused form does not apply (fewer
-// than 5 + R qubits, or a group flips more than R bits above the lane bits).
+// Pass plan for an n-qubit state, or nullptr when the fused form does not apply (fewer than
+// 10 qubits, or a group flips more than kPR bits above the lane bits). Each pass takes the
+// groups whose flip bits fit its local bits; per group the strings are ordered constant,
+// straddling, tabulated, and the tabulated ones are summed here over the 1024 local indices.
 static int pauli_program(mb_observable o, int n, PauliProgram** out) {
   *out = nullptr;
   PauliData* pd = o->pauli;
-  if (!pd || n < 5 + kPR) return MB_OK;
+  if (!pd || n < kPLocal) return MB_OK;
   for (PauliProgram* p : pd->programs)
     if (p->n == n) {
       *out = p;
@@ -294,12 +303,17 @@ static int pauli_program(mb_observable o, int n, PauliProgram** out) {
   std::vector<int> rem;
   for (size_t g = 0; g < pd->groups.size(); ++g) {
     const uint64_t hi = pd->groups[g].first & ~uint64_t(31);
-    if (__builtin_popcountll(hi) > kPR) return MB_OK;
+    if (__builtin_popcountll(hi) > kPR || (pd->groups[g].first >> n) != 0) return MB_OK;
+    const int s0 = pd->groups[g].second.first, ns = pd->groups[g].second.second;
+    for (int s = s0; s < s0 + ns; ++s)
+      if ((pd->strings[s].z >> n) != 0) return MB_OK;
     rem.push_back(int(g));
   }
   std::unique_ptr<PauliProgram> P(new PauliProgram());
   P->n = n;
   std::vector<PGroup> hg;
+  std::vector<PString> hs;
+  std::vector<double2> ht;
   while (!rem.empty() || P->passes.empty()) {
     uint64_t regm = 0;
     for (int g : rem) {
@@ -312,25 +326,52 @@ static int pauli_program(mb_observable o, int n, PauliProgram** out) {
     int k = 0;
     for (int q = 5; q < n; ++q)
       if ((regm >> q) & 1) pa.reg[k++] = q;
+    const uint64_t localm = uint64_t(31) | regm;
     pa.g0 = int(hg.size());
     std::vector<int> left;
     for (int g : rem) {
       const uint64_t x = pd->groups[g].first;
-      if ((x & ~uint64_t(31) & ~regm) != 0) {
+      if ((x & ~localm) != 0 || int(hg.size()) - pa.g0 >= kPMaxGroups) {
         left.push_back(g);
         continue;
       }
       PGroup G{};
       G.x = x;
-      G.xlow = int(x & 31);
+      G.xl = int(x & 31);
       for (int r = 0; r < kPR; ++r)
-        if ((x >> pa.reg[r]) & 1) G.xreg |= 1 << r;
-      G.s0 = pd->groups[g].second.first;
-      G.ns = pd->groups[g].second.second;
+        if ((x >> pa.reg[r]) & 1) G.xl |= 1 << (5 + r);
+      const int s0 = pd->groups[g].second.first, ns = pd->groups[g].second.second;
+      std::vector<PString> kc, st, tb;
+      for (int s = s0; s < s0 + ns; ++s) {
+        const PString& ps = pd->strings[s];
+        const uint64_t zl = ps.z & localm, zh = ps.z & ~localm;
+        (zl == 0 ? kc : (zh == 0 ? tb : st)).push_back(ps);
+      }
+      G.k0 = int(hs.size());
+      G.nk = int(kc.size());
+      hs.insert(hs.end(), kc.begin(), kc.end());
+      G.v0 = int(hs.size());
+      G.nv = int(st.size());
+      hs.insert(hs.end(), st.begin(), st.end());
+      G.tab = -1;
+      if (!tb.empty()) {
+        // sum over the strings inside the local bits, for every local index l
+        G.tab = int(ht.size());
+        for (int l = 0; l < kPTile; ++l) {
+          const uint64_t k_idx = local_bits(l, pa.reg) ^ x;
+          double2 f = cz();
+          for (const PString& ps : tb) {
+            const bool odd = __builtin_popcountll(k_idx & ps.z) & 1;
+            f.x += odd ? -ps.c.x : ps.c.x;
+            f.y += odd ? -ps.c.y : ps.c.y;
+          }
+          ht.push_back(f);
+        }
+      }
       hg.push_back(G);
     }
     pa.ngroups = int(hg.size()) - pa.g0;
-    pa.threads_per_sample = int64_t(1) << (n - kPR);
+    pa.tiles_per_sample = int64_t(1) << (n - kPLocal);
     P->passes.push_back(pa);
     rem.swap(left);
     if (pd->groups.empty()) break;
@@ -340,15 +381,21 @@ static int pauli_program(mb_observable o, int n, PauliProgram** out) {
     if ((rc = dev_alloc((void**)&P->d_groups, sizeof(PGroup) * hg.size()))) return rc;
     MB_CHECK_CUDA(cudaMemcpyAsync(P->d_groups, hg.data(), sizeof(PGroup) * hg.size(), cudaMemcpyHostToDevice, g_ctx.stream));
   }
-  if (!pd->strings.empty()) {
-    if ((rc = dev_alloc((void**)&P->d_strings, sizeof(PString) * pd->strings.size()))) return rc;
-    MB_CHECK_CUDA(cudaMemcpyAsync(P->d_strings, pd->strings.data(), sizeof(PString) * pd->strings.size(),
-                                  cudaMemcpyHostToDevice, g_ctx.stream));
+  if (!hs.empty()) {
+    if ((rc = dev_alloc((void**)&P->d_strings, sizeof(PString) * hs.size()))) return rc;
+    MB_CHECK_CUDA(cudaMemcpyAsync(P->d_strings, hs.data(), sizeof(PString) * hs.size(), cudaMemcpyHostToDevice,
+                                  g_ctx.stream));
+  }
+  if (!ht.empty()) {
+    if ((rc = dev_alloc((void**)&P->d_tables, sizeof(double2) * ht.size()))) return rc;
+    MB_CHECK_CUDA(cudaMemcpyAsync(P->d_tables, ht.data(), sizeof(double2) * ht.size(), cudaMemcpyHostToDevice,
+                                  g_ctx.stream));
   }
   MB_CHECK_CUDA(cudaStreamSynchronize(g_ctx.stream));
   for (PPassArgs& pa : P->passes) {
     pa.groups = P->d_groups;
     pa.strings = P->d_strings;
+    pa.tables = P->d_tables;
   }
   *out = P.get();
   pd->programs.push_back(P.release());
@@ -367,7 +414,7 @@ int expect_pauli(mb_observable o, mb_state s, double2* out) {
   if (g_ctx.capturing) {
     for (PauliProgram* q : o->pauli->programs)
       if (q->n == s->n) P = q;
-    if (!P && s->n >= 5 + kPR) {
+    if (!P && s->n >= kPLocal) {
       set_error("record the expectation once before capturing it (its pass plan is built lazily)");
       return MB_EUNSUPPORTED;
     }
@@ -380,10 +427,9 @@ int expect_pauli(mb_observable o, mb_state s, double2* out) {
   MB_CHECK_CUDA(cudaMemsetAsync(out, 0, sizeof(double2) * s->batch, st));
   for (const PPassArgs& pa : P->passes) {
     if (pa.ngroups == 0) continue;
-    const int64_t blocks = (pa.threads_per_sample + kPThreads - 1) / kPThreads;
     int64_t per = std::max<int64_t>(1, std::min<int64_t>(int64_t(g_ctx.sm_count) * 8 / s->batch + 1,
                                                       g_ctx.partials_cap / (s->batch + 1) - 1));
-    const int G = int(std::min<int64_t>(blocks, per));
+    const int G = int(std::min<int64_t>(pa.tiles_per_sample, per));
     if (int64_t(G) * s->batch > g_ctx.partials_cap || s->batch > g_ctx.ncounters) {
       set_error("reduction workspace too small for %d samples", s->batch);
       return MB_EUNSUPPORTED;
@@ -395,9 +441,6 @@ int expect_pauli(mb_observable o, mb_state s, double2* out) {
   return MB_OK;
 }
 
-}  // namespace mb
-
-namespace mb {
 // out = scale * H in for pure states (the adjoint seed 2H psi); false when the fused form
 // does not apply to this register size (the caller then uses the per-key kernels).
 int pauli_apply(mb_observable o, const double2* in, double2* out, int n, int nsamples, double scale, bool* done) {
@@ -409,8 +452,7 @@ int pauli_apply(mb_observable o, const double2* in, double2* out, int n, int nsa
   bool first = true;
   for (const PPassArgs& pa : P->passes) {
     if (pa.ngroups == 0) continue;
-    const int64_t blocks = (pa.threads_per_sample + kPThreads - 1) / kPThreads;
-    const int G = int(std::min<int64_t>(blocks, int64_t(g_ctx.sm_count) * 16));
+    const int G = int(std::min<int64_t>(pa.tiles_per_sample, int64_t(g_ctx.sm_count) * 16));
     ProfScope ps("k_pauli_apply", (first ? 32.0 : 48.0) * double(int64_t(1) << n) * nsamples, st);
     k_pauli_apply<<<dim3(G, nsamples), kPThreads, 0, st>>>(in, out, pa, scale, first ? 1 : 0);
     MB_LAUNCHED();
@@ -420,4 +462,5 @@ int pauli_apply(mb_observable o, const double2* in, double2* out, int n, int nsa
   *done = true;
   return MB_OK;
 }
+
 }  // namespace mb
