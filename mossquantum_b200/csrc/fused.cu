@@ -1263,6 +1263,9 @@ static std::vector<int> window(int lo, int len, int N) {
 static void build_schedule(Schedule& S, int nsamples, bool allow_reg = true) {
   const int N = S.N, t = std::min(S.t, N), R = S.R;
   const uint64_t full = N >= 64 ? ~uint64_t(0) : ((uint64_t(1) << N) - 1);
+  // MB_SCHED_ONE_WINDOW=1 restricts tile candidates to one window above bits 0..2 (for
+  // comparisons); by default a tile may hold two.
+  static const bool two_windows = !(getenv("MB_SCHED_ONE_WINDOW") && atoi(getenv("MB_SCHED_ONE_WINDOW")));
   std::vector<int> rem(S.fops.size());
   for (size_t i = 0; i < rem.size(); ++i) rem[i] = int(i);
   S.passes.clear();
@@ -1298,6 +1301,21 @@ static void build_schedule(Schedule& S, int nsamples, bool allow_reg = true) {
         }
         const int rlo = std::max(5, std::min(h0, N - R));
         if (allow_reg && N - 5 >= R) cands.push_back({PASS_REG, window(rlo, R, N)});
+        if (two_windows) {
+          // Bits 0..2 and two windows [a, a + w1), [b, b + w2) with w1 + w2 = t - 3: one pass
+          // can then continue a chain of gates at two places (the tail of one layer and the
+          // head of the next).
+          for (int w1 = 2; w1 <= w - 2; ++w1) {
+            const int w2 = w - w1;
+            for (int a = 3; a + w1 <= N; ++a)
+              for (int b = a + w1 + 1; b + w2 <= N; ++b) {
+                std::vector<int> bb = {0, 1, 2};
+                for (int q : window(a, w1, N)) bb.push_back(q);
+                for (int q : window(b, w2, N)) bb.push_back(q);
+                cands.push_back({PASS_TILE, bb});
+              }
+          }
+        }
         if (S.dm) {
           // Paired windows for density matrices: row bits [a, a+w1) and the matching column
           // bits [b, b+w2) (b = a + n), so a channel's supermatrix on (q, q+n) and both halves

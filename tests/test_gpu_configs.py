@@ -154,21 +154,26 @@ def test_reference_recorded_circuits(mq, O, name):
 
 @pytest.mark.parametrize("tile_bits", [11, 12])
 def test_long_range_gate_beyond_a_tile(mq, O, tile_bits):
-    """A dense 2-qubit gate on qubits 4 and 14 of a 14-qubit state lies farther apart than any
-    tile window: the fused forward runs it as a plain pass, and the fused adjoint refuses the
-    schedule so the gradient takes the plain reverse sweep."""
+    """A dense 3-qubit gate on qubits 4, 12 and 20 of a 20-qubit state needs three windows
+    above the lane bits, more than a tile holds: the fused forward runs it as a plain pass,
+    and the fused adjoint refuses the schedule so the gradient takes the plain reverse sweep.
+    A 2-qubit gate on qubits 4 and 18 fits two windows of one tile."""
     from mossquantum_b200 import _native as N
     from mossquantum_b200 import workloads as W
-    n = 14
+    n = 20
     rng = np.random.default_rng(14)
-    z = rng.normal(size=(4, 4)) + 1j * rng.normal(size=(4, 4))
+    z = rng.normal(size=(8, 8)) + 1j * rng.normal(size=(8, 8))
     u, _ = np.linalg.qr(z)
+    z2 = rng.normal(size=(4, 4)) + 1j * rng.normal(size=(4, 4))
+    u2, _ = np.linalg.qr(z2)
     gates = [mq.HGate(q) for q in range(1, n + 1)]
-    gates += [mq.QuantumGate((4, 14), u)]
+    gates += [mq.QuantumGate((4, 12, 20), u), mq.QuantumGate((4, 18), u2)]
     gates += [mq.RyGate(q, float(rng.uniform(0, 2 * np.pi)), isparas=True) for q in range(1, n + 1)]
     gates += [mq.CNOTGate(q, q + 1) for q in range(1, n)]
-    gates += [mq.QuantumGate((14, 4), u.conj().T)]
+    gates += [mq.QuantumGate((20, 4, 12), u.conj().T)]
     c = mq.QCircuit(gates)
+    from mossquantum_b200 import autotune
+    before = autotune.get(n)
     N.check(N.lib().mb_tuning_set(n, tile_bits, 4))
     try:
         s = mq.apply_(c, mq.StateVector(n))
@@ -181,4 +186,4 @@ def test_long_range_gate_beyond_a_tile(mq, O, tile_bits):
         assert abs(v - vr) <= 1e-11
         assert np.max(np.abs(g - gr)) <= 1e-10
     finally:
-        N.check(N.lib().mb_tuning_set(n, 12, 4))
+        autotune.set(n, *before)

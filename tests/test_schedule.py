@@ -2,7 +2,8 @@
 
 Every circuit must schedule in bounded time with every fused operation in exactly one pass:
 density-matrix channels on qubits farther apart than a tile window (paired row/column
-windows), 2-qubit gates between distant qubits (a plain pass), the 28-qubit U3 circuit and
+windows), 2-qubit gates between distant qubits (two windows of one tile), gates that need
+three windows (a plain pass), the 28-qubit U3 circuit and
 the uneven-batch circuits, across tile and register widths.
 """
 import ctypes
@@ -43,7 +44,8 @@ def test_noisy_density_circuits_schedule(n, t, R):
 
 def test_config_circuits_schedule():
     u = W.u3_brickwork(28, 20, W.u3_params(28, 20, W.rng_for(1, 0)))
-    assert schedule_info(u, 28) == (20, 20, 0, 0, 1)
+    assert schedule_info(u, 28) == (15, 15, 0, 0, 1)
+    assert schedule_info(u, 28, t=12, R=4) == (11, 11, 0, 0, 1)
     assert schedule_info(W.hea_circuit(10, 8, noise=(0.01, 0.02)), 10, dm=True, nsamples=64)[4] == 1
     for n in (10, 16, 22):
         assert schedule_info(W.hea_circuit(n, 8), n, nsamples=5)[4] == 1
@@ -53,10 +55,13 @@ def test_long_range_gates_get_plain_passes():
     rng = np.random.default_rng(3)
     n = 28
     q, _ = np.linalg.qr(rng.normal(size=(4, 4)) + 1j * rng.normal(size=(4, 4)))
+    u8, _ = np.linalg.qr(rng.normal(size=(8, 8)) + 1j * rng.normal(size=(8, 8)))
     gates = [mq.HGate(p) for p in range(1, n + 1)]
     # (1, 28) is bits 0 and 27: bit 0 is in every tile, so a window at the top holds it;
-    # (6, 26) and (4, 20) span more than any window and run as plain passes
-    gates += [mq.QuantumGate((6, 26), q), mq.QuantumGate((1, 28), q), mq.QuantumGate((4, 20), q), mq.RyGate(14, 0.3)]
+    # (6, 26) and (4, 20) fit two windows of one tile; the 3-qubit gates on bits (5, 15, 25)
+    # and (3, 11, 19) would need three windows and run as plain passes
+    gates += [mq.QuantumGate((6, 26), q), mq.QuantumGate((1, 28), q), mq.QuantumGate((4, 20), q), mq.RyGate(14, 0.3),
+              mq.QuantumGate((6, 16, 26), u8), mq.QuantumGate((4, 12, 20), u8)]
     npasses, ntile, nreg, nplain, complete = schedule_info(mq.QCircuit(gates), n)
     assert complete == 1 and nplain == 2
 
@@ -169,4 +174,19 @@ def test_lowering_reference_recorded_circuit_families():
     with open(path) as f:
         case = json.load(f)["cases"]["n15-d20"]
     ea, eb = lowering_errors(W.cpu_scan_circuit(case["angles_by_layer"]), 15, t=11, R=3)
+    assert ea <= 1e-12 and eb <= 1e-12, (ea, eb)
+
+
+# Tiles of bits 0..2 plus two windows let one pass continue a CNOT chain at two places (the
+# light cones of consecutive layers): the hardware-efficient ansatz on 20..24 qubits needs
+# about one pass per layer instead of three. The two-window passes must still lower exactly.
+def test_two_window_tiles_cut_passes():
+    assert schedule_info(W.hea_circuit(20, 8), 20, t=11, R=3, nsamples=32)[:2] == (8, 8)
+    c24 = W.hea_circuit(24, 16, W.hea_angles(24, 16, W.rng_for(3)))
+    assert schedule_info(c24, 24, t=10, R=3)[0] <= 27
+    n, depth = 17, 6
+    c = W.hea_circuit(n, depth, W.hea_angles(n, depth, W.rng_for(42)))
+    npasses = schedule_info(c, n, t=9, R=3)[0]
+    assert npasses <= 12, npasses
+    ea, eb = lowering_errors(c, n, t=9, R=3)
     assert ea <= 1e-12 and eb <= 1e-12, (ea, eb)
