@@ -1072,6 +1072,12 @@ extern "C" int mb_observable_apply(mb_observable o, mb_state in, mb_state out) {
   }
   if (int rc = validate_observable(o, in)) return rc;
   const int is_dm = in->kind == MB_DENSITY || in->kind == MB_BATCH_DENSITY;
+  if (!is_dm && o->pauli_ok && !g_ctx.capturing) {
+    // pure states from 10 qubits: Pauli-string passes over shared-memory tiles
+    bool done = false;
+    if (int rc = pauli_apply(o, in->d, out->d, in->n, in->batch, 1.0, &done)) return rc;
+    if (done) return MB_OK;
+  }
   return observable_apply(o, in->d, out->d, in->n, is_dm, in->batch);
 }
 

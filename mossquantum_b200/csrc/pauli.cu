@@ -45,6 +45,8 @@ struct PGroup {
   int k0, nk;
   int v0, nv;
   int tab;      // offset of the group's 1024-entry table, or -1
+  int herm;     // every string's coefficient without i^{#Y} is real (the group is Hermitian)
+  int hb;       // highest set bit of xl (flip groups)
 };
 
 struct PPassArgs {
@@ -92,15 +94,15 @@ __device__ __forceinline__ uint64_t tile_base(int64_t T, const int* reg) {
 }
 
 // Loads a tile into shared memory (each warp reads 32 consecutive amplitudes) and computes the
-// per-tile constants of the pass's groups.
+// per-tile constants of the pass's groups (descriptors already in shared memory).
 __device__ __forceinline__ void stage_tile(const double2* __restrict__ vs, uint64_t base, const uint64_t* loc,
-                                           const PPassArgs& a, double2* tile, double2* kconst) {
+                                           const PPassArgs& a, const PGroup* gd, double2* tile, double2* kconst) {
 #pragma unroll
   for (int k = 0; k < kPPerThread; ++k) tile[threadIdx.x + k * kPThreads] = vs[base | loc[k]];
   for (int gi = threadIdx.x; gi < a.ngroups; gi += kPThreads) {
-    const PGroup g = a.groups[a.g0 + gi];
+    const int k0 = gd[gi].k0, nk = gd[gi].nk;
     double2 kc = cz();
-    for (int s = g.k0; s < g.k0 + g.nk; ++s) {
+    for (int s = k0; s < k0 + nk; ++s) {
       const PString ps = a.strings[s];
       const bool odd = __popcll(base & ps.z) & 1;
       kc.x += odd ? -ps.c.x : ps.c.x;
@@ -111,24 +113,36 @@ __device__ __forceinline__ void stage_tile(const double2* __restrict__ vs, uint6
 }
 
 // Factor of group g at local index l (tile base `base`, local bits `lb`).
-__device__ __forceinline__ double2 group_factor(const PGroup& g, const PPassArgs& a, const double2* kconst, int gi,
-                                                int l, uint64_t base, uint64_t lb) {
-  double2 f = kconst[gi];
+__device__ __forceinline__ double2 group_factor(const PGroup& g, const PPassArgs& a, double2 kc, int l,
+                                                uint64_t base, uint64_t lb) {
+  double2 f = kc;
   if (g.tab >= 0) f = cadd(f, __ldg(a.tables + g.tab + l));
-  const uint64_t k_idx = (base | lb) ^ g.x;
-  for (int s = g.v0; s < g.v0 + g.nv; ++s) {
-    const PString ps = a.strings[s];
-    const bool odd = __popcll(k_idx & ps.z) & 1;
-    f.x += odd ? -ps.c.x : ps.c.x;
-    f.y += odd ? -ps.c.y : ps.c.y;
+  if (g.nv) {
+    const uint64_t k_idx = (base | lb) ^ g.x;
+    for (int s = g.v0; s < g.v0 + g.nv; ++s) {
+      const PString ps = a.strings[s];
+      const bool odd = __popcll(k_idx & ps.z) & 1;
+      f.x += odd ? -ps.c.x : ps.c.x;
+      f.y += odd ? -ps.c.y : ps.c.y;
+    }
   }
   return f;
 }
 
+__device__ __forceinline__ void load_groups(const PPassArgs& a, PGroup* gd) {
+  for (int gi = threadIdx.x; gi < a.ngroups; gi += kPThreads) gd[gi] = a.groups[a.g0 + gi];
+}
+
+// <psi|H|psi> over the groups of one pass. Groups are the outer loop (one descriptor read per
+// tile), the thread's amplitudes the inner one. A Hermitian flip group sums over pairs
+// (j, j^x) only: conj(psi_j) f(j) psi_{j^x} + conj(psi_{j^x}) f(j^x) psi_j equals
+// 2 Re(conj(psi_j) f(j) psi_{j^x}) because f(j^x) = conj(f(j)), so half the amplitudes of the
+// tile (local bit hb clear) carry the group.
 __global__ void __launch_bounds__(kPThreads) k_pauli_pass(const double2* __restrict__ v, const PPassArgs a,
                                                          double2* partials, unsigned* counters, double2* out) {
   __shared__ double2 tile[kPTile];
   __shared__ double2 kconst[kPMaxGroups];
+  __shared__ PGroup gd[kPMaxGroups];
   __shared__ double2 wp[kPThreads / 32];
   __shared__ bool last;
   const int b = blockIdx.y, G = gridDim.x;
@@ -139,22 +153,48 @@ __global__ void __launch_bounds__(kPThreads) k_pauli_pass(const double2* __restr
   uint64_t loc[kPPerThread];
 #pragma unroll
   for (int k = 0; k < kPPerThread; ++k) loc[k] = local_bits(threadIdx.x + k * kPThreads, reg);
+  load_groups(a, gd);
+  __syncthreads();
   double2 acc = cz();
   for (int64_t T = blockIdx.x; T < a.tiles_per_sample; T += G) {
     const uint64_t base = tile_base(T, reg);
-    stage_tile(vs, base, loc, a, tile, kconst);
+    stage_tile(vs, base, loc, a, gd, tile, kconst);
     __syncthreads();
+    for (int gi = 0; gi < a.ngroups; ++gi) {
+      const PGroup g = gd[gi];
+      const double2 kc = kconst[gi];
+      if (g.xl == 0) {
+        // diagonal group: f(j) |psi_j|^2
 #pragma unroll
-    for (int k = 0; k < kPPerThread; ++k) {
-      const int l = threadIdx.x + k * kPThreads;
-      const double2 amp = tile[l];
-      for (int gi = 0; gi < a.ngroups; ++gi) {
-        const PGroup g = a.groups[a.g0 + gi];
-        const double2 p = tile[l ^ g.xl];
-        const double2 f = group_factor(g, a, kconst, gi, l, base, loc[k]);
-        // conj(psi_j) * psi_{j^x} * f
-        const double2 cp = make_double2(amp.x * p.x + amp.y * p.y, amp.x * p.y - amp.y * p.x);
-        acc = cfma(f, cp, acc);
+        for (int k = 0; k < kPPerThread; ++k) {
+          const int l = threadIdx.x + k * kPThreads;
+          const double2 amp = tile[l];
+          const double2 f = group_factor(g, a, kc, l, base, loc[k]);
+          const double p2 = amp.x * amp.x + amp.y * amp.y;
+          acc.x = fma(f.x, p2, acc.x);
+          acc.y = fma(f.y, p2, acc.y);
+        }
+      } else if (g.herm) {
+        const int hb = g.hb;
+#pragma unroll
+        for (int k = 0; k < kPPerThread / 2; ++k) {
+          const int m = threadIdx.x + k * kPThreads;
+          const int l = ((m >> hb) << (hb + 1)) | (m & ((1 << hb) - 1));
+          const double2 amp = tile[l], p = tile[l ^ g.xl];
+          const double2 f = group_factor(g, a, kc, l, base, g.nv ? local_bits(l, reg) : 0);
+          // 2 Re(conj(amp) p f)
+          const double cr = amp.x * p.x + amp.y * p.y, ci = amp.x * p.y - amp.y * p.x;
+          acc.x = fma(2.0 * f.x, cr, fma(-2.0 * f.y, ci, acc.x));
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < kPPerThread; ++k) {
+          const int l = threadIdx.x + k * kPThreads;
+          const double2 amp = tile[l], p = tile[l ^ g.xl];
+          const double2 f = group_factor(g, a, kc, l, base, loc[k]);
+          const double2 cp = make_double2(amp.x * p.x + amp.y * p.y, amp.x * p.y - amp.y * p.x);
+          acc = cfma(f, cp, acc);
+        }
       }
     }
     __syncthreads();
@@ -187,6 +227,7 @@ __global__ void __launch_bounds__(kPThreads) k_pauli_apply(const double2* __rest
                                                           const PPassArgs a, double scale, int first) {
   __shared__ double2 tile[kPTile];
   __shared__ double2 kconst[kPMaxGroups];
+  __shared__ PGroup gd[kPMaxGroups];
   const int b = blockIdx.y, G = gridDim.x;
   const double2* vs = v + (int64_t(b) << a.n);
   double2* os = out + (int64_t(b) << a.n);
@@ -196,20 +237,28 @@ __global__ void __launch_bounds__(kPThreads) k_pauli_apply(const double2* __rest
   uint64_t loc[kPPerThread];
 #pragma unroll
   for (int k = 0; k < kPPerThread; ++k) loc[k] = local_bits(threadIdx.x + k * kPThreads, reg);
+  load_groups(a, gd);
+  __syncthreads();
   for (int64_t T = blockIdx.x; T < a.tiles_per_sample; T += G) {
     const uint64_t base = tile_base(T, reg);
-    stage_tile(vs, base, loc, a, tile, kconst);
+    stage_tile(vs, base, loc, a, gd, tile, kconst);
+    double2 r[kPPerThread];
+#pragma unroll
+    for (int k = 0; k < kPPerThread; ++k) r[k] = cz();
     __syncthreads();
+    for (int gi = 0; gi < a.ngroups; ++gi) {
+      const PGroup g = gd[gi];
+      const double2 kc = kconst[gi];
+#pragma unroll
+      for (int k = 0; k < kPPerThread; ++k) {
+        const int l = threadIdx.x + k * kPThreads;
+        r[k] = cfma(group_factor(g, a, kc, l, base, loc[k]), tile[l ^ g.xl], r[k]);
+      }
+    }
 #pragma unroll
     for (int k = 0; k < kPPerThread; ++k) {
-      const int l = threadIdx.x + k * kPThreads;
-      double2 r = first ? cz() : os[base | loc[k]];
-      for (int gi = 0; gi < a.ngroups; ++gi) {
-        const PGroup g = a.groups[a.g0 + gi];
-        const double2 f = group_factor(g, a, kconst, gi, l, base, loc[k]);
-        r = cfma(cscale(f, scale), tile[l ^ g.xl], r);
-      }
-      os[base | loc[k]] = r;
+      const double2 o = first ? cz() : os[base | loc[k]];
+      os[base | loc[k]] = make_double2(fma(scale, r[k].x, o.x), fma(scale, r[k].y, o.y));
     }
     __syncthreads();
   }
@@ -342,8 +391,13 @@ static int pauli_program(mb_observable o, int n, PauliProgram** out) {
         if ((x >> pa.reg[r]) & 1) G.xl |= 1 << (5 + r);
       const int s0 = pd->groups[g].second.first, ns = pd->groups[g].second.second;
       std::vector<PString> kc, st, tb;
+      G.herm = 1;
+      G.hb = G.xl ? 31 - __builtin_clz(unsigned(G.xl)) : 0;
       for (int s = s0; s < s0 + ns; ++s) {
         const PString& ps = pd->strings[s];
+        // coefficient without i^{#Y} (#Y = |x & z|) real: c * (-i)^{#Y} has no imaginary part
+        const int ny = __builtin_popcountll(x & ps.z) & 3;
+        if ((ny & 1) ? ps.c.x != 0.0 : ps.c.y != 0.0) G.herm = 0;
         const uint64_t zl = ps.z & localm, zh = ps.z & ~localm;
         (zl == 0 ? kc : (zh == 0 ? tb : st)).push_back(ps);
       }

@@ -66,6 +66,28 @@ def test_observable_action(mq, O):
     np.testing.assert_allclose(out, O.apply_observable(psi, n, H.specs()), atol=1e-12)
 
 
+@pytest.mark.parametrize("n", [10, 13])
+def test_pauli_passes_expectation_and_action(mq, O, n):
+    """From 10 qubits on, expectations and H psi run as Pauli-string passes over shared-memory
+    tiles (Hermitian flip groups summed over pairs j, j^x; others over every amplitude);
+    strings with flips on up to five bits above the lanes, and Z strings inside, outside and
+    across a tile's bits."""
+    rng = np.random.default_rng(100 + n)
+    psi = random_state(n, rng)
+    s = mq.StateVector(psi)
+    for herm in (True, False):
+        H = random_operator(mq, n, rng, herm)
+        assert abs(mq.expectation(H, s) - O.expect(psi, n, H.specs())) <= 1e-11
+        out = mq.apply_observable(H, mq.StateVector(psi)).to_numpy()
+        np.testing.assert_allclose(out, O.apply_observable(psi, n, H.specs()), atol=1e-12)
+    # one Hermitian term with a complex coefficient pair: X1 Y7 Z13-type strings and their sum
+    # with a non-Hermitian partner in the same flip group
+    terms = [mq.QubitsTerm([1, 7, n], ["X", "Y", "Z"], 0.7), mq.QubitsTerm([1, 7], ["X", "X"], 0.3),
+             mq.QubitsTerm([1, 7, 4], ["Y", "X", "Z"], 0.2j)]
+    H = mq.QubitsOperator(terms)
+    assert abs(mq.expectation(H, s) - O.expect(psi, n, H.specs())) <= 1e-11
+
+
 def test_probabilities(mq, O):
     n = 9
     rng = np.random.default_rng(3)
