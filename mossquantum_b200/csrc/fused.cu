@@ -928,6 +928,44 @@ static uint64_t mask_of(const std::vector<int>& b) {
   return m;
 }
 
+// The scheduler's view of one remaining op: its masks and weight, packed so that scoring a
+// candidate bit set scans a small contiguous array.
+struct SlimOp {
+  uint64_t nd, all;
+  float w;
+  int fits_any;
+};
+
+static float slim_weight(const FOp& f) { return f.type == MOP_DIAG ? 0.25f : (f.type == MOP_U2 ? 2.0f : 1.0f); }
+
+// Score of take_ops for `tmask` (same rule, no list).
+static double score_mask(const std::vector<SlimOp>& ops, uint64_t tmask, uint64_t full) {
+  uint64_t b_all = 0, b_nd = 0;
+  double sc = 0;
+  for (const SlimOp& f : ops) {
+    const bool fits = f.fits_any && (f.nd & ~tmask) == 0;
+    const bool comm = (f.nd & b_all) == 0 && (f.all & b_nd) == 0;
+    if (fits && comm) {
+      sc += f.w;
+    } else {
+      b_all |= f.all;
+      b_nd |= f.nd;
+      if ((b_nd & full) == full) break;
+    }
+  }
+  return sc;
+}
+
+// Packs the first (at most 8192) remaining ops, the ones take_ops looks at.
+static void slim_ops(const std::vector<FOp>& fops, const std::vector<int>& rem, std::vector<SlimOp>& out) {
+  const size_t lim = std::min<size_t>(rem.size(), 8192);
+  out.resize(lim);
+  for (size_t i = 0; i < lim; ++i) {
+    const FOp& f = fops[rem[i]];
+    out[i] = {f.nd, f.all, slim_weight(f), f.type != F_UNFUSABLE};
+  }
+}
+
 // Greedy take: ops that fit `tmask` and commute with every op skipped before them.
 static std::vector<int> take_ops(const std::vector<FOp>& fops, const std::vector<int>& rem, uint64_t tmask,
                                  uint64_t full, double* score) {
@@ -941,7 +979,7 @@ static std::vector<int> take_ops(const std::vector<FOp>& fops, const std::vector
     const bool comm = (f.nd & b_all) == 0 && (f.all & b_nd) == 0;
     if (fits && comm) {
       taken.push_back(rem[i]);
-      sc += f.type == MOP_DIAG ? 0.25 : (f.type == MOP_U2 ? 2.0 : 1.0);
+      sc += slim_weight(f);
     } else {
       b_all |= f.all;
       b_nd |= f.nd;
@@ -1281,6 +1319,7 @@ static void build_schedule(Schedule& S, int nsamples, bool allow_reg = true) {
       continue;
     }
     std::vector<Cand> cands;
+    std::vector<SlimOp> slim;
     cands.push_back({PASS_TILE, window(0, t, N)});
     if (N > t) {
       // first target bit not coverable by the low tile, in circuit order
@@ -1303,15 +1342,38 @@ static void build_schedule(Schedule& S, int nsamples, bool allow_reg = true) {
         if (allow_reg && N - 5 >= R) cands.push_back({PASS_REG, window(rlo, R, N)});
         if (two_windows) {
           // Bits 0..2 and two windows [a, a + w1), [b, b + w2) with w1 + w2 = t - 3: one pass
-          // can then continue a chain of gates at two places (the tail of one layer and the
-          // head of the next).
+          // can then continue a chain of gates at two places (the tail of one layer's light
+          // cone and the head of the next). Every single window of each width is scored with
+          // bits 0..2; the best six positions of width w1 are paired with the best six of
+          // width t - 3 - w1 (an exhaustive search over all pairs finds tiles of the same
+          // quality on the tested circuits at five times the cost).
+          if (slim.empty()) slim_ops(S.fops, rem, slim);
+          constexpr int kTop = 6;
+          std::vector<std::vector<std::pair<double, int>>> top(w + 1);
+          for (int ww = 2; ww <= w - 2; ++ww) {
+            std::vector<std::pair<double, int>> sc;
+            for (int a = 3; a + ww <= N; ++a) {
+              const uint64_t m = uint64_t(7) | (((uint64_t(1) << ww) - 1) << a);
+              sc.push_back({-score_mask(slim, m, full), a});
+            }
+            std::sort(sc.begin(), sc.end());
+            if (sc.size() > size_t(kTop)) sc.resize(kTop);
+            top[ww] = sc;
+          }
           for (int w1 = 2; w1 <= w - 2; ++w1) {
             const int w2 = w - w1;
-            for (int a = 3; a + w1 <= N; ++a)
-              for (int b = a + w1 + 1; b + w2 <= N; ++b) {
+            if (w1 > w2) break;  // pairs (w1, w2) and (w2, w1) give the same tiles
+            for (const auto& pa : top[w1])
+              for (const auto& pb : top[w2]) {
+                int a = pa.second, la = w1, b = pb.second, lb = w2;
+                if (a > b) {
+                  std::swap(a, b);
+                  std::swap(la, lb);
+                }
+                if (b < a + la + 1) continue;  // overlapping or touching: not two windows
                 std::vector<int> bb = {0, 1, 2};
-                for (int q : window(a, w1, N)) bb.push_back(q);
-                for (int q : window(b, w2, N)) bb.push_back(q);
+                for (int q : window(a, la, N)) bb.push_back(q);
+                for (int q : window(b, lb, N)) bb.push_back(q);
                 cands.push_back({PASS_TILE, bb});
               }
           }
@@ -1338,19 +1400,18 @@ static void build_schedule(Schedule& S, int nsamples, bool allow_reg = true) {
     int bi = -1;
     std::vector<int> best_taken;
     TmaGeom bg{};
+    if (slim.empty()) slim_ops(S.fops, rem, slim);
     for (size_t ci = 0; ci < cands.size(); ++ci) {
+      double sc = score_mask(slim, mask_of(cands[ci].bits), full);
+      if (cands[ci].kind == PASS_REG) sc *= 0.999;  // prefer the wider tile on ties
+      if (sc <= best) continue;
       TmaGeom g{};
       if (cands[ci].kind == PASS_TILE && !tile_geom(cands[ci].bits, N, nsamples, g)) continue;
-      double sc;
-      auto tk = take_ops(S.fops, rem, mask_of(cands[ci].bits), full, &sc);
-      if (cands[ci].kind == PASS_REG) sc *= 0.999;  // prefer the wider tile on ties
-      if (sc > best) {
-        best = sc;
-        bi = int(ci);
-        best_taken = tk;
-        bg = g;
-      }
+      best = sc;
+      bi = int(ci);
+      bg = g;
     }
+    if (bi >= 0) best_taken = take_ops(S.fops, rem, mask_of(cands[bi].bits), full, nullptr);
     if (bi < 0 || best_taken.empty()) {
       // No candidate holds the first op (its bits lie farther apart than any window): run it
       // by itself with the plain kernel, which always makes progress. The adjoint has no
