@@ -20,11 +20,14 @@
 #include <algorithm>
 #include <cmath>
 #include <complex>
+#include <functional>
 #include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
 #include <mutex>
+#include <string>
+#include <unordered_map>
 
 #include "fused_kernels.cuh"
 #include "family.cuh"
@@ -1722,6 +1725,68 @@ static int adjoint_ctas(int t, int dm = 0) {
   return std::max(1, std::min(cap, int((227 * 1024) / (shm + 256))));
 }
 
+// Generated kernel sources, memoised by everything the generators read: the pass (bits, TMA
+// geometry, register stages, micro-ops, gradient slots) and the kernel shape. Circuits that
+// differ only in matrix values (a fresh host circuit with new angles) lower to passes with the
+// same micro-ops and table offsets, so their schedules reuse the source text instead of
+// generating it again (about 3 ms for the 28-qubit U3 + CZ circuit's 700 KB).
+static std::string pass_key(const Pass& p, int gen, int R, int N, bool single, int ctas) {
+  std::string k;
+  auto put = [&](const void* d, size_t n) { k.append(static_cast<const char*>(d), n); };
+  auto put_i = [&](int64_t v) { put(&v, sizeof v); };
+  for (int64_t v : {int64_t(gen), int64_t(R), int64_t(N), int64_t(single), int64_t(ctas), int64_t(p.kind),
+                    int64_t(p.t), int64_t(p.has_u2)})
+    put_i(v);
+  put_i(int64_t(p.bits.size()));
+  for (int b : p.bits) put_i(b);
+  put_i(p.geom.ndims);
+  for (int d = 0; d < 5; ++d) {
+    put_i(p.geom.start[d]);
+    put_i(p.geom.bits[d]);
+    put_i(p.geom.boxb[d]);
+  }
+  put_i(int64_t(p.stages.size()));
+  for (const StageDesc& sd : p.stages) {
+    put_i(sd.op0);
+    put_i(sd.nops);
+    put_i(sd.nreg);
+    for (int r = 0; r < kMaxRegBits; ++r) put_i(sd.reg[r]);
+    put_i(sd.ntid);
+    for (int r = 0; r < 26; ++r) put_i(sd.tid[r]);
+  }
+  put_i(int64_t(p.mops.size()));
+  for (const MOp& m : p.mops) {
+    for (int64_t v : {int64_t(m.type), int64_t(m.r0), int64_t(m.r1), int64_t(m.nsel), int64_t(m.sel[0]),
+                      int64_t(m.sel[1]), int64_t(m.sel[2]), int64_t(m.sel[3]), int64_t(m.active), int64_t(m.conj),
+                      int64_t(m.param), int64_t(m.only)})
+      put_i(v);
+    put(m.off, sizeof m.off);
+  }
+  put_i(int64_t(p.grad_slots.size()));
+  for (int g : p.grad_slots) put_i(g);
+  return k;
+}
+
+static std::string memo_source(const std::string& key, const std::function<std::string()>& gen) {
+  static std::mutex mu;
+  static std::unordered_map<std::string, std::string> memo;
+  static size_t bytes = 0;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = memo.find(key);
+    if (it != memo.end()) return it->second;
+  }
+  std::string src = gen();
+  std::lock_guard<std::mutex> lk(mu);
+  if (bytes > (size_t(256) << 20)) {  // bound the memo at 256 MB of keys and sources
+    memo.clear();
+    bytes = 0;
+  }
+  bytes += key.size() + src.size();
+  memo.emplace(key, src);
+  return src;
+}
+
 static void prepare_jit(Schedule* S) {
   if (S->jit != 0) return;
   S->jit = -1;
@@ -1735,11 +1800,16 @@ static void prepare_jit(Schedule* S) {
     if (p.kind == PASS_TILE && !S->adjoint) p.ctas = tile_ctas(p.t);
     if (p.kind == PASS_TILE && S->adjoint) {
       p.ctas = adjoint_ctas(p.t, S->dm);
-      src.push_back(jit_adjoint_source(p, S->R, S->N, single, p.ctas));
+      src.push_back(memo_source(pass_key(p, 1, S->R, S->N, single, p.ctas),
+                                [&] { return jit_adjoint_source(p, S->R, S->N, single, p.ctas); }));
+    } else if (p.kind == PASS_TILE) {
+      src.push_back(memo_source(pass_key(p, 0, S->R, S->N, single, p.ctas),
+                                [&] { return jit_tile_source(p, S->R, S->N, single, p.ctas); }));
+    } else if (p.kind == PASS_REG) {
+      src.push_back(memo_source(pass_key(p, 2, S->R, S->N, single, 0), [&] { return jit_reg_source(p, S->N, single); }));
+    } else {
+      continue;
     }
-    else if (p.kind == PASS_TILE) src.push_back(jit_tile_source(p, S->R, S->N, single, p.ctas));
-    else if (p.kind == PASS_REG) src.push_back(jit_reg_source(p, S->N, single));
-    else continue;
     who.push_back(&p);
   }
   std::vector<CUfunction> fns;

@@ -72,3 +72,20 @@ def test_jit_density_and_batch(mq, O, jit_on):
     for b in range(B):
         ref = O.apply(c.copy().reset_parameters(thetas[b]).specs(), O.zero_state(n), n)
         assert np.max(np.abs(out[:, b] - ref)) <= 1e-12
+
+
+def test_jit_fresh_circuits_same_structure(mq, O, jit_on):
+    """Fresh host circuits with new fixed angles lower to passes with the same micro-ops, so
+    their schedules reuse the memoised kernel sources; every circuit still gets its own matrix
+    values (each result against the oracle)."""
+    from mossquantum_b200 import _native as N
+    from mossquantum_b200 import workloads as W
+    n, depth = 14, 6
+    for i in range(3):
+        c = W.u3_brickwork(n, depth, W.u3_params(n, depth, W.rng_for(77, i)))
+        N.profile(True)
+        s = mq.apply_(c, mq.StateVector(n))
+        assert used_jit(N)
+        N.profile(False)
+        ref = O.apply(c.specs(), O.zero_state(n), n)
+        assert np.max(np.abs(s.to_numpy() - ref)) <= 1e-12
