@@ -1579,13 +1579,26 @@ int get_schedule_ex(mb_circuit c, int n, int dm, int adjoint, int lo, int hi, in
     if (const char* e = getenv("MB_ADJOINT_REG_BITS")) tu.R = std::max(3, std::min(4, atoi(e)));
     tu.t = std::min(tu.t, N);
   }
+  // A forward schedule of a batch serves every batch up to its capacity (the passes are the
+  // same for all batches of more than one sample; only the per-sample rows of the derived
+  // table grow), so batches of varying size, as in the serving loop, share one schedule.
+  // Capacities are powers of two; adjoint schedules keep their exact batch.
+  int cap = nsamples;
+  if (!adjoint && nsamples > 1)
+    for (cap = 2; cap < nsamples; cap *= 2) {
+    }
+  auto fits = [&](const Schedule* s) {
+    if (adjoint || nsamples == 1) return s->nsamples == nsamples;
+    return s->nsamples > 1 && s->nsamples >= nsamples;
+  };
   for (Schedule* s : c->scheds)
-    if (s->N == N && s->dm == dm && !s->dagger && s->t == tu.t && s->R == tu.R && s->nsamples == nsamples &&
+    if (s->N == N && s->dm == dm && !s->dagger && s->t == tu.t && s->R == tu.R && fits(s) &&
         (adjoint || s->fuse == (tu.fuse != 0)) &&
         s->lo == lo && s->hi == hi && s->adjoint == adjoint) {
       *out = s;
       return MB_OK;
     }
+  nsamples = cap;
   if (g_ctx.capturing) {
     set_error("run this circuit once on a state of this shape before capturing it (schedules are built lazily)");
     return MB_EUNSUPPORTED;
