@@ -52,3 +52,20 @@ def test_empty_batch(mq):
     s = mq.BatchStateVector(3, 0)
     s = mq.apply_(mq.HGate(1), s)
     assert mq.expectation(mq.QubitsTerm([1], ["Z"]), s).shape == (0,)
+
+
+def test_batches_of_varying_size_share_schedules(mq, O):
+    """One circuit over batches of 3, 2, 5 and 4 samples with per-sample angles (the serving
+    loop's pattern): forward schedules serve every batch up to a power-of-two capacity, so the
+    later batches reuse earlier schedules and their per-sample rows; every sample still matches
+    the oracle."""
+    from mossquantum_b200 import workloads as W
+    n, depth = 12, 3
+    c = W.hea_circuit(n, depth)
+    rng = np.random.default_rng(31)
+    for B in (3, 2, 5, 4):
+        th = rng.uniform(0, 2 * np.pi, size=(B, c.nparameters()))
+        out = mq.apply_(c, mq.BatchStateVector(n, B), theta=th).to_numpy()
+        for b in range(B):
+            ref = O.apply(c.copy().reset_parameters(th[b]).specs(), O.zero_state(n), n)
+            assert np.max(np.abs(out[:, b] - ref)) <= 1e-12, (B, b)
