@@ -1537,7 +1537,10 @@ static bool want_jit(int N) {
 static Tuning tuning_for(int N) {
   Tuning tu;
   if (want_jit(N) && jit_available()) {
-    tu.t = 11;
+    // 2^10-amplitude tiles, 8 amplitudes per thread, 4 CTAs of 128 threads per SM: the fastest
+    // point of a sweep over (t, R, CTAs) on the 28-qubit U3 + CZ step (62.5 ms against 63.8 ms
+    // at 2^11 tiles with 2 CTAs of 256 threads, 67.7 ms at 2^12 with 1 CTA of 512)
+    tu.t = 10;
     tu.R = 3;
   }
   {
@@ -1719,11 +1722,11 @@ int get_schedule(mb_circuit c, int n, int dm, bool dagger, int nsamples, Schedul
 
 // CTAs per SM of a specialised tile pass: as many double-buffered tiles as shared memory holds
 // (allowing 4 KB for the pass's matrix copy; a larger copy only lowers the resident count),
-// capped at MB_TILE_CTAS (default 2). The kernel's launch bounds ask the compiler to fit that
+// capped at MB_TILE_CTAS (default 4 for tiles of at most 2^10 amplitudes, else 2). The kernel's launch bounds ask the compiler to fit that
 // many CTAs in the register file.
 static int tile_ctas(int t) {
   const size_t shm = (size_t(32) << t) + 1024 + 4 * 1024;
-  int cap = 2;
+  int cap = t <= 10 ? 4 : 2;
   if (const char* e = getenv("MB_TILE_CTAS")) cap = std::max(1, std::min(8, atoi(e)));
   return std::max(1, std::min(cap, int((227 * 1024) / (shm + 256))));
 }
