@@ -300,20 +300,22 @@ def batch_measure(steps=3, warmup=2, per_size=3, dm_samples=4):
     ms_step = (pure_ms + dm_ms) / steps
     launches = N.launch_count() - l0
     evals = 512 + 64
-    # The sizes below the specialised-kernel threshold (10..17 qubits) replayed alone: what
-    # launching all sizes' passes together could save at most (their kernels are short and
-    # leave most SMs idle).
+    # The sizes below 18 qubits replayed alone: in the batch they run in one persistent launch
+    # (a CTA per sample); beside it the same sizes with one launch per size and pass.
     small = {n: groups[n] for n in groups if n < 18}
-    plan_small = BatchPlan(small, W.xxz)
     th_small = {n: th[n] for n in small}
-    plan_small.run(th_small)
-    start.record(stream)
-    for _ in range(steps):
+    small_ms = {}
+    for persistent in (True, False):
+        plan_small = BatchPlan(small, W.xxz, persistent=persistent)
         plan_small.run(th_small)
-    end.record(stream)
-    end.synchronize()
-    small_ms = start.elapsed_time(end) / steps
-    plan_small.close()
+        start.record(stream)
+        for _ in range(steps):
+            plan_small.run(th_small)
+        end.record(stream)
+        end.synchronize()
+        small_ms[persistent] = start.elapsed_time(end) / steps
+        plan_small.close()
+    persistent_info = plan.persistent_info()
     # plain per-call path: stratified sample
     plain_s = {}
     for n in sorted(counts):
@@ -333,7 +335,10 @@ def batch_measure(steps=3, warmup=2, per_size=3, dm_samples=4):
     plain_total = sum(plain_s[n] * counts[n] for n in counts) + 64 * dm_plain
     log(f"batch: {ms_step:.1f} ms per step, plain per-call {plain_total * 1e3:.0f} ms per batch")
     return {"evals_per_s": evals / (ms_step / 1e3), "ms_per_step": ms_step, "pure_ms_per_step": pure_ms / steps,
-            "density_ms_per_step": dm_ms / steps, "small_sizes_ms_per_step": small_ms,
+            "density_ms_per_step": dm_ms / steps, "small_sizes_ms_per_step": small_ms[True],
+            "small_sizes_per_size_launches_ms_per_step": small_ms[False],
+            "persistent_launch": {"groups": persistent_info[0], "samples": persistent_info[2],
+                                  "groups_on_per_size_path": persistent_info[1]},
             "evals_per_step": evals, "steps": steps, "warmup": warmup,
             "sizes": counts, "plan_build_s": prep_s,
             "autotuned": {str(k): list(v) for k, v in {**plan.tuned, **plan_dm.tuned}.items()},
@@ -357,6 +362,8 @@ def batch_workload(args):
                        "sizes": r["sizes"], "plan_build_s": r["plan_build_s"], "autotuned": r["autotuned"]},
             "pure_ms_per_step": r["pure_ms_per_step"], "density_ms_per_step": r["density_ms_per_step"],
             "small_sizes_ms_per_step": r["small_sizes_ms_per_step"],
+            "small_sizes_per_size_launches_ms_per_step": r["small_sizes_per_size_launches_ms_per_step"],
+            "persistent_launch": r["persistent_launch"],
             "plain_per_call": r["plain_per_call"], "speedup_vs_plain": r["speedup_vs_plain"],
             "e2e": {"value": r["e2e"]["evals_per_s"], "unit": "evals/s",
                     "h2d_bytes_per_step": r["e2e"]["h2d_bytes_per_step"],

@@ -206,6 +206,23 @@ MB_API int mb_graph_end(mb_graph* out);
 MB_API int mb_graph_launch(mb_graph g);
 MB_API int mb_graph_free(mb_graph g);
 
+/* ---- uneven batches in one persistent launch ---------------------------------------------
+ * (batches of the reference hold one register size, src/states/batch_state_vector.jl; this is
+ * the B200 form of many sizes with per-sample parameters). A plan over groups (circuit g on
+ * state g: a pure batch of one register size, its parameters staged with mb_theta_upload, one
+ * row per sample) runs every group of 8..17 qubits in ONE persistent kernel: CTAs take whole
+ * samples from a work counter, largest first, and run all of the sample's tile passes (two
+ * small launches before it bind the parameter rows and form the fused single-qubit products
+ * of every group). Other groups (more qubits, density matrices, instructions a tile cannot
+ * hold) run through mb_apply's fused path after it. Circuits and states must outlive the
+ * plan. mb_uneven_apply may be recorded into a graph once it has run eagerly. */
+typedef struct mb_uneven_s* mb_uneven;
+#define MB_UNEVEN_ZERO 1  /* start every sample from |0...0> */
+MB_API int mb_uneven_create(const mb_circuit* circuits, const mb_state* states, int ngroups, mb_uneven* out);
+MB_API int mb_uneven_apply(mb_uneven u, int flags);
+MB_API int mb_uneven_info(mb_uneven u, int* persistent_groups, int* fallback_groups, int* samples);
+MB_API int mb_uneven_free(mb_uneven u);
+
 /* ---- tuning: tile bits t (10..12) and register bits R (3..5) per register size ---------- */
 MB_API int mb_tuning_set(int nbits, int tile_bits, int reg_bits);
 MB_API int mb_tuning_get(int nbits, int* tile_bits, int* reg_bits);

@@ -31,6 +31,7 @@ FAMILIES = {"MATRIX": 0, "RX": 1, "RY": 2, "RZ": 3, "PHASE": 4, "CRX": 5, "CRY":
             "CPHASE": 8, "CCPHASE": 9, "SELECT": 10}
 MB_OPF_ADJOINT = 1
 MB_APPLY_FUSED, MB_APPLY_PLAIN, MB_APPLY_PER_SAMPLE, MB_APPLY_DEVICE_THETA, MB_APPLY_TENSOR = 0, 1, 2, 4, 8
+MB_UNEVEN_ZERO = 1
 
 
 class BackendError(RuntimeError):
@@ -143,6 +144,10 @@ def load():
         "mb_graph_end": ([ctypes.POINTER(vp)], ctypes.c_int),
         "mb_graph_launch": ([vp], ctypes.c_int),
         "mb_graph_free": ([vp], ctypes.c_int),
+        "mb_uneven_create": ([ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.c_int, ctypes.POINTER(vp)], ctypes.c_int),
+        "mb_uneven_apply": ([vp, ctypes.c_int], ctypes.c_int),
+        "mb_uneven_info": ([vp, ip, ip, ip], ctypes.c_int),
+        "mb_uneven_free": ([vp], ctypes.c_int),
         "mb_tuning_set": ([ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
         "mb_tuning_get": ([ctypes.c_int, ip, ip], ctypes.c_int),
         "mb_tuning_set_fusion": ([ctypes.c_int, ctypes.c_int], ctypes.c_int),

@@ -2,11 +2,13 @@
 
 MOSSQuantum's batches share one register size and one parameter vector
 (src/states/batch_state_vector.jl, docs/architecture.md). A ``BatchPlan`` accepts samples
-of different qubit counts, each with its own parameters: samples are grouped by size into
-device batches, every group runs the fused pass kernels over all of its samples at once
-(one launch per pass, tiles of every sample in the same persistent grid), and the whole
-sequence (reset, parameter binding, passes, expectations) is recorded once into a CUDA graph.
-``run`` uploads the parameters and replays the graph: one launch for the entire batch.
+of different qubit counts, each with its own parameters. Pure samples of 8..17 qubits run in
+ONE persistent kernel launch (``mb_uneven_apply``): its CTAs take whole samples from a work
+counter, largest first, and run every tile pass of the sample's circuit, so no launch is
+spent per size or per pass. Larger samples and density matrices are grouped by size into
+device batches that run the fused pass kernels over all of their samples at once. The whole
+sequence (reset, parameter binding, passes, expectations) is recorded once into a CUDA graph;
+``run`` uploads the parameters and replays the graph.
 """
 from __future__ import annotations
 
@@ -25,7 +27,7 @@ class BatchPlan:
     """groups: {n: (template circuit for n qubits, samples B_n)}; observable_for(n) gives the
     observable evaluated on every sample of size n. kind: "pure" or "density"."""
 
-    def __init__(self, groups, observable_for, kind="pure", autotune=False, autotune_max_bits=24):
+    def __init__(self, groups, observable_for, kind="pure", autotune=False, autotune_max_bits=24, persistent=True):
         self.kind = kind
         self.tuned = {}
         self.groups = []
@@ -59,6 +61,13 @@ class BatchPlan:
                     self.tuned[bits] = (t, r, get_fusion(bits), ms)
         # Eager warm-up with zero parameters: builds schedules, kernels and reduction plans.
         self._stage({g["n"]: np.zeros((g["B"], g["circuit"].nparameters())) for g in self.groups})
+        self.uneven = None
+        if persistent and kind == "pure" and self.groups:
+            cs = (ctypes.c_void_p * len(self.groups))(*[g["compiled"].handle.value for g in self.groups])
+            ss = (ctypes.c_void_p * len(self.groups))(*[g["state"].handle.value for g in self.groups])
+            u = ctypes.c_void_p()
+            N.check(N.lib().mb_uneven_create(cs, ss, len(self.groups), ctypes.byref(u)), "mb_uneven_create")
+            self.uneven = u
         self._record_body()
         N.synchronize()
         self._capture()
@@ -74,11 +83,14 @@ class BatchPlan:
 
     def _record_body(self):
         L = N.lib()
+        if self.uneven is not None:
+            N.check(L.mb_uneven_apply(self.uneven, N.MB_UNEVEN_ZERO), "uneven apply (recorded)")
         for g in self.groups:
             st = g["state"]
-            N.check(L.mb_state_set_zero(st.handle))
-            N.check(L.mb_apply(g["compiled"].handle, st.handle, None, 0,
-                               N.MB_APPLY_DEVICE_THETA | N.MB_APPLY_PER_SAMPLE), "apply (recorded)")
+            if self.uneven is None:
+                N.check(L.mb_state_set_zero(st.handle))
+                N.check(L.mb_apply(g["compiled"].handle, st.handle, None, 0,
+                                   N.MB_APPLY_DEVICE_THETA | N.MB_APPLY_PER_SAMPLE), "apply (recorded)")
             out = ctypes.c_void_p(self.results.value + 16 * g["offset"])
             N.check(L.mb_expect_to_device(g["obs"].handle().handle, st.handle, out), "expectation (recorded)")
 
@@ -106,10 +118,21 @@ class BatchPlan:
         vals = host[0::2] + 1j * host[1::2]
         return {g["n"]: vals[g["offset"]:g["offset"] + g["B"]] for g in self.groups}
 
+    def persistent_info(self):
+        """(groups in the persistent launch, groups on the per-size path, samples in the launch)."""
+        if self.uneven is None:
+            return 0, len(self.groups), 0
+        a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        N.check(N.lib().mb_uneven_info(self.uneven, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+        return a.value, b.value, c.value
+
     def close(self):
         if self.graph is not None:
             N.lib().mb_graph_free(self.graph)
             self.graph = None
+        if getattr(self, "uneven", None) is not None:
+            N.lib().mb_uneven_free(self.uneven)
+            self.uneven = None
         if self.results:
             N.lib().mb_buffer_free(self.results)
             self.results = ctypes.c_void_p()

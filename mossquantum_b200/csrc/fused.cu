@@ -182,6 +182,145 @@ __global__ void k_fuse(const FuseRec* __restrict__ recs, int nrecs, const FuseCo
 // ---------------------------------------------------------------------------------------------
 // Host: fused ops
 // ---------------------------------------------------------------------------------------------
+// Persistent uneven batch: one launch over samples of different register sizes, each with its
+// own parameters. A CTA takes one sample at a time from a work counter (largest samples first)
+// and runs that sample's whole circuit: the |0..0> start and every tile pass of its size's
+// schedule, tile by tile. A sample is owned by one CTA, so the passes need no synchronisation
+// between CTAs; samples of at most 2^17 amplitudes (2 MiB) keep their passes in L2. Two
+// launches before it bind every sample's parameter row and form its fused single-qubit
+// products, for all sizes at once (the pass kernel reads the tables through the read-only
+// cache, so they are written before it starts).
+constexpr int kUnevenThreads = 128;
+constexpr int kUnevenMaxTile = 11;   // 2^11-amplitude tiles, 16 amplitudes per thread
+
+struct UnevenGroup {
+  int n;                      // amplitude bits of one sample
+  int B;                      // samples
+  int pass0, npasses;         // this size's passes in the plan's pass array
+  int64_t bind0, fuse0;       // first work item of this group in the bind and fuse launches
+  int nbinds, nslots;
+  const BindRec* binds;
+  const double* theta;        // nslots values per sample
+  int nrecs;
+  const FuseRec* recs;
+  const FuseComp* comps;
+  double2* states;            // samples back to back
+  double2* table;             // matrix table, one row of tstride entries per sample
+  int64_t tstride;
+  const double2* xtab;        // derived coefficients, then per-sample rows of xrow entries
+  double2* xtabs;
+  int64_t xrow;
+};
+
+struct UnevenPass {
+  int t, nstages;
+  int bits[16];
+  const StageDesc* stages;
+  const MOp* mops;
+};
+
+// Group of work item w (groups ordered by their first item).
+__device__ __forceinline__ int uneven_group_of(const UnevenGroup* g, int ng, int64_t w, bool fuse) {
+  int i = 0;
+  while (i + 1 < ng && (fuse ? g[i + 1].fuse0 : g[i + 1].bind0) <= w) ++i;
+  return i;
+}
+
+// Parameter binding of every sample of every group: item = (group, sample, bind record).
+__global__ void k_uneven_bind(const UnevenGroup* __restrict__ groups, int ng, int64_t total) {
+  const int64_t w = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (w >= total) return;
+  const UnevenGroup& G = groups[uneven_group_of(groups, ng, w, false)];
+  const int64_t r = w - G.bind0;
+  const int b = int(r / G.nbinds), q = int(r % G.nbinds);
+  const BindRec rc = G.binds[q];
+  const double th = rc.slot >= 0 ? G.theta[int64_t(b) * G.nslots + rc.slot] : rc.value;
+  bind_record(rc, th, G.table, G.table + int64_t(b) * G.tstride);
+}
+
+// Fused single-qubit products of every sample of every group: item = (group, sample, record).
+__global__ void k_uneven_fuse(const UnevenGroup* __restrict__ groups, int ng, int64_t total) {
+  const int64_t w = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (w >= total) return;
+  const UnevenGroup& G = groups[uneven_group_of(groups, ng, w, true)];
+  const int64_t r = w - G.fuse0;
+  const int b = int(r / G.nrecs), q = int(r % G.nrecs);
+  const FuseRec rec = G.recs[q];
+  double2 M[16];
+  fuse_product(rec, G.comps, G.table, G.table + int64_t(b) * G.tstride, M);
+  double2* out = G.xtabs + int64_t(b) * G.xrow + rec.out;
+  for (int e = 0; e < rec.d * rec.d; ++e) out[e] = M[e];
+}
+
+template <bool U2>
+__global__ void __launch_bounds__(kUnevenThreads, 2)
+    k_uneven(const UnevenGroup* __restrict__ groups, const UnevenPass* __restrict__ passes,
+             const int2* __restrict__ items, int nitems, unsigned* next, int zero_init) {
+  constexpr int R = 4;
+  extern __shared__ unsigned char smem_raw[];
+  double2* tl = reinterpret_cast<double2*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* loc = reinterpret_cast<uint64_t*>(tl + (1 << kUnevenMaxTile));
+  __shared__ int s_item;
+  const int tx = threadIdx.x;
+  for (;;) {
+    if (tx == 0) s_item = int(atomicAdd(next, 1u));
+    __syncthreads();
+    const int item = s_item;
+    __syncthreads();
+    if (item >= nitems) break;
+    const int2 it = items[item];
+    const UnevenGroup G = groups[it.x];
+    const int b = it.y;
+    const int64_t dim = int64_t(1) << G.n;
+    double2* v = G.states + int64_t(b) * dim;
+    const double2* xs = G.xtabs ? G.xtabs + int64_t(b) * G.xrow : nullptr;
+    if (zero_init)
+      for (int64_t j = tx; j < dim; j += kUnevenThreads) v[j] = make_double2(j == 0 ? 1.0 : 0.0, 0.0);
+    __syncthreads();
+    for (int pi = 0; pi < G.npasses; ++pi) {
+      const UnevenPass& P = passes[G.pass0 + pi];
+      const int t = P.t, T = 1 << t;
+      for (int l = tx; l < T; l += kUnevenThreads) {
+        uint64_t o = 0;
+        for (int q = 0; q < t; ++q) o |= uint64_t((l >> q) & 1) << P.bits[q];
+        loc[l] = o;
+      }
+      __syncthreads();
+      const int64_t ntiles = dim >> t;
+      for (int64_t tile = 0; tile < ntiles; ++tile) {
+        uint64_t base = uint64_t(tile);
+        for (int q = 0; q < t; ++q) {
+          const int p = P.bits[q];
+          base = ((base >> p) << (p + 1)) | (base & ((uint64_t(1) << p) - 1));
+        }
+        for (int l = tx; l < T; l += kUnevenThreads) tl[fk::swz(uint32_t(l))] = v[base | loc[l]];
+        __syncthreads();
+        for (int s = 0; s < P.nstages; ++s) {
+          const StageDesc& sd = P.stages[s];
+          int reg[kMaxRegBits];
+#pragma unroll
+          for (int k = 0; k < R; ++k) reg[k] = sd.reg[k];
+          const int vthreads = 1 << sd.ntid;
+          for (int vt = tx; vt < vthreads; vt += kUnevenThreads) {
+            uint32_t lbase = 0;
+            for (int q = 0; q < sd.ntid; ++q) lbase |= ((uint32_t(vt) >> q) & 1u) << sd.tid[q];
+            double2 a[1 << R];
+#pragma unroll
+            for (int j = 0; j < (1 << R); ++j) a[j] = tl[fk::swz(lbase | uint32_t(fk::reg_offset<R>(j, reg)))];
+            fk::run_mops<R, U2>(a, P.mops + sd.op0, sd.nops, lbase, reg, base, G.table, G.xtab, xs, G.tstride, b);
+#pragma unroll
+            for (int j = 0; j < (1 << R); ++j) tl[fk::swz(lbase | uint32_t(fk::reg_offset<R>(j, reg)))] = a[j];
+          }
+          __syncthreads();
+        }
+        for (int l = tx; l < T; l += kUnevenThreads) v[base | loc[l]] = tl[fk::swz(uint32_t(l))];
+        __syncthreads();
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
 enum { F_UNFUSABLE = -1 };
 
 }  // namespace
@@ -231,6 +370,7 @@ struct Schedule {
   int jit = 0;  // 0 not tried, 1 specialised kernels ready, -1 interpreter kernels
   bool dagger = false;
   bool unschedulable = false;  // an adjoint op that no pass can hold
+  bool tile_only = false;      // built without register passes
   std::vector<FOp> fops;
   std::vector<Pass> passes;
   StageDesc* d_stages = nullptr;
@@ -1567,10 +1707,17 @@ double reverse_growth(mb_circuit c, const COp& op) { return growth_of(c, op); }
 
 bool jit_sizes(int nbits) { return want_jit(nbits) && jit_available(); }
 
-int get_schedule_ex(mb_circuit c, int n, int dm, int adjoint, int lo, int hi, int nsamples, Schedule** out) {
+// force: a tile and register width to use instead of the tuning table's; tile_only: no
+// register passes (every pass a tile pass, for the persistent uneven-batch kernel).
+static int get_schedule_impl(mb_circuit c, int n, int dm, int adjoint, int lo, int hi, int nsamples,
+                             const Tuning* force, bool tile_only, Schedule** out) {
   const int N = dm ? 2 * n : n;
   if (hi < 0) hi = int(c->ops.size());
   Tuning tu = tuning_for(N);
+  if (force) {
+    tu.t = std::min(force->t, N);
+    tu.R = force->R;
+  }
   if (adjoint) {
     // y and delta tiles, double-buffered: MB_ADJOINT_TILE_BITS (8..11) and the register width of
     // the dual-state passes MB_ADJOINT_REG_BITS (3..4). Default 2^10-amplitude tiles, 8
@@ -1597,7 +1744,7 @@ int get_schedule_ex(mb_circuit c, int n, int dm, int adjoint, int lo, int hi, in
   for (Schedule* s : c->scheds)
     if (s->N == N && s->dm == dm && !s->dagger && s->t == tu.t && s->R == tu.R && fits(s) &&
         (adjoint || s->fuse == (tu.fuse != 0)) &&
-        s->lo == lo && s->hi == hi && s->adjoint == adjoint) {
+        s->lo == lo && s->hi == hi && s->adjoint == adjoint && s->tile_only == tile_only) {
       *out = s;
       return MB_OK;
     }
@@ -1624,7 +1771,8 @@ int get_schedule_ex(mb_circuit c, int n, int dm, int adjoint, int lo, int hi, in
   } else {
     build_fops(c, n, dm, false, S->fops, lo, hi, S.get());
   }
-  build_schedule(*S, nsamples, !adjoint);
+  S->tile_only = tile_only;
+  build_schedule(*S, nsamples, !adjoint && !tile_only);
   if (S->unschedulable) {
     set_error("the fused adjoint cannot place an instruction whose qubits are farther apart than a tile");
     return MB_EUNSUPPORTED;
@@ -1706,12 +1854,16 @@ int get_schedule_ex(mb_circuit c, int n, int dm, int adjoint, int lo, int hi, in
       dev_free(S->d_xtab);
       dev_free(S->d_frecs);
       dev_free(S->d_fcomps);
-      return get_schedule_ex(c, n, dm, adjoint, lo, hi, nsamples, out);
+      return get_schedule_impl(c, n, dm, adjoint, lo, hi, nsamples, force, tile_only, out);
     }
   }
   *out = S.get();
   c->scheds.push_back(S.release());
   return MB_OK;
+}
+
+int get_schedule_ex(mb_circuit c, int n, int dm, int adjoint, int lo, int hi, int nsamples, Schedule** out) {
+  return get_schedule_impl(c, n, dm, adjoint, lo, hi, nsamples, nullptr, false, out);
 }
 
 int get_schedule(mb_circuit c, int n, int dm, bool dagger, int nsamples, Schedule** out) {
@@ -2070,6 +2222,245 @@ void release_schedules(mb_circuit c) {
 }
 
 }  // namespace mb
+
+// ---- persistent uneven batch (host side) -------------------------------------------------------
+// Groups of pure states of 8..17 qubits whose schedules (2^min(11, n)-amplitude tiles, 4 register
+// bits, no register passes) hold every instruction run in one k_uneven launch; other groups
+// (larger or density states, plain passes) run through the ordinary per-group path.
+struct mb_uneven_s {
+  std::vector<mb_circuit> cs;
+  std::vector<mb_state> ss;
+  std::vector<int> pgroups;              // persistent groups (input indices), largest first
+  std::vector<int> fallback;             // the others
+  std::vector<mb::Schedule*> scheds;     // per persistent group
+  std::vector<mb::UnevenGroup> hgroups;  // descriptors as last uploaded
+  std::vector<mb::UnevenPass> hpasses;
+  mb::UnevenGroup* d_groups = nullptr;
+  mb::UnevenPass* d_passes = nullptr;
+  int2* d_items = nullptr;
+  unsigned* d_next = nullptr;
+  int nitems = 0;
+  int64_t nbind = 0, nfuse = 0;
+  bool u2 = false;
+  double bytes = 0, flops = 0;           // algorithmic bytes and flops of one launch
+};
+
+namespace mb {
+namespace {
+constexpr int kUnevenMaxBits = 17;
+
+// Descriptors from the circuits' current tables and parameters (their device buffers move
+// when a larger batch of parameters is staged).
+void uneven_descriptors(mb_uneven u, std::vector<UnevenGroup>& out) {
+  out.clear();
+  int pass0 = 0;
+  int64_t b0 = 0, f0 = 0;
+  for (size_t i = 0; i < u->pgroups.size(); ++i) {
+    mb_circuit c = u->cs[u->pgroups[i]];
+    mb_state s = u->ss[u->pgroups[i]];
+    Schedule* S = u->scheds[i];
+    UnevenGroup g{};
+    g.n = s->n;
+    g.B = s->batch;
+    g.pass0 = pass0;
+    g.npasses = int(S->passes.size());
+    pass0 += g.npasses;
+    g.bind0 = b0;
+    g.fuse0 = f0;
+    g.nbinds = int(c->binds.size());
+    g.nslots = c->nslots;
+    g.binds = c->d_binds;
+    g.theta = c->d_theta;
+    g.nrecs = int(S->frecs.size());
+    g.recs = S->d_frecs;
+    g.comps = S->d_fcomps;
+    g.states = s->d;
+    g.table = c->d_table;
+    g.tstride = c->table_elems;
+    g.xtab = S->d_xtab;
+    g.xtabs = S->d_xtab ? S->d_xtab + S->xtab.size() : nullptr;
+    g.xrow = S->xrow;
+    b0 += int64_t(g.nbinds) * g.B;
+    f0 += int64_t(g.nrecs) * g.B;
+    out.push_back(g);
+  }
+}
+
+bool same_descriptors(const std::vector<UnevenGroup>& a, const std::vector<UnevenGroup>& b) {
+  return a.size() == b.size() && (a.empty() || std::memcmp(a.data(), b.data(), sizeof(UnevenGroup) * a.size()) == 0);
+}
+
+void uneven_release(mb_uneven u) {
+  dev_free(u->d_groups);
+  dev_free(u->d_passes);
+  dev_free(u->d_items);
+  dev_free(u->d_next);
+  u->d_groups = nullptr;
+  u->d_passes = nullptr;
+  u->d_items = nullptr;
+  u->d_next = nullptr;
+}
+}  // namespace
+}  // namespace mb
+
+extern "C" int mb_uneven_create(const mb_circuit* circuits, const mb_state* states, int ngroups, mb_uneven* out) {
+  using namespace mb;
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (int rc = check_init()) return rc;
+  if (int rc = check_not_capturing("mb_uneven_create")) return rc;
+  if (!out || ngroups < 0 || (ngroups && (!circuits || !states))) return MB_EINVAL;
+  std::unique_ptr<mb_uneven_s> u(new mb_uneven_s());
+  for (int g = 0; g < ngroups; ++g) {
+    if (!circuits[g] || !states[g]) return MB_EINVAL;
+    if (int rc = validate_apply(circuits[g], states[g])) return rc;
+    u->cs.push_back(circuits[g]);
+    u->ss.push_back(states[g]);
+  }
+  std::vector<int> order(ngroups);
+  for (int g = 0; g < ngroups; ++g) order[g] = g;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return u->ss[a]->n > u->ss[b]->n; });
+  for (int g : order) {
+    mb_circuit c = u->cs[g];
+    mb_state s = u->ss[g];
+    bool ok = (s->kind == MB_PURE || s->kind == MB_BATCH_PURE) && s->n >= 8 && s->n <= kUnevenMaxBits &&
+              s->batch > 0;
+    for (const COp& op : c->ops)
+      if (op.kind == MB_OP_GATE && op.k == 0) ok = false;
+    Schedule* S = nullptr;
+    if (ok) {
+      Tuning f;
+      f.t = std::min(kUnevenMaxTile, s->n);
+      f.R = 4;
+      if (int rc = get_schedule_impl(c, s->n, 0, 0, 0, -1, s->batch, &f, true, &S)) return rc;
+      for (const Pass& p : S->passes) ok = ok && p.kind == PASS_TILE && p.t <= kUnevenMaxTile && p.t >= 4;
+      ok = ok && S->R == 4;
+    }
+    if (!ok) {
+      u->fallback.push_back(g);
+      continue;
+    }
+    u->pgroups.push_back(g);
+    u->scheds.push_back(S);
+    for (const Pass& p : S->passes) {
+      UnevenPass up{};
+      up.t = p.t;
+      up.nstages = int(p.stages.size());
+      for (int q = 0; q < p.t; ++q) up.bits[q] = p.bits[q];
+      up.stages = S->d_stages + p.stage_off;
+      up.mops = S->d_mops;
+      u->hpasses.push_back(up);
+      u->u2 = u->u2 || p.has_u2;
+      const double amps = double(int64_t(1) << s->n) * s->batch;
+      u->bytes += 32.0 * amps;
+      u->flops += pass_flops_per_amp(p, false) * amps;
+    }
+  }
+  std::vector<int2> items;
+  for (size_t i = 0; i < u->pgroups.size(); ++i)
+    for (int b = 0; b < u->ss[u->pgroups[i]]->batch; ++b) items.push_back(make_int2(int(i), b));
+  u->nitems = int(items.size());
+  int rc;
+  uneven_descriptors(u.get(), u->hgroups);
+  for (const UnevenGroup& g : u->hgroups) {
+    u->nbind += int64_t(g.nbinds) * g.B;
+    u->nfuse += int64_t(g.nrecs) * g.B;
+  }
+  if (!u->pgroups.empty()) {
+    if ((rc = dev_alloc((void**)&u->d_groups, sizeof(UnevenGroup) * u->hgroups.size())) ||
+        (rc = dev_alloc((void**)&u->d_passes, sizeof(UnevenPass) * std::max<size_t>(1, u->hpasses.size()))) ||
+        (rc = dev_alloc((void**)&u->d_items, sizeof(int2) * items.size())) ||
+        (rc = dev_alloc((void**)&u->d_next, sizeof(unsigned)))) {
+      uneven_release(u.get());
+      return rc;
+    }
+    cudaStream_t st = g_ctx.stream;
+    MB_CHECK_CUDA(cudaMemcpyAsync(u->d_groups, u->hgroups.data(), sizeof(UnevenGroup) * u->hgroups.size(),
+                                  cudaMemcpyHostToDevice, st));
+    if (!u->hpasses.empty())
+      MB_CHECK_CUDA(cudaMemcpyAsync(u->d_passes, u->hpasses.data(), sizeof(UnevenPass) * u->hpasses.size(),
+                                    cudaMemcpyHostToDevice, st));
+    MB_CHECK_CUDA(cudaMemcpyAsync(u->d_items, items.data(), sizeof(int2) * items.size(), cudaMemcpyHostToDevice, st));
+    MB_CHECK_CUDA(cudaStreamSynchronize(st));
+  }
+  *out = u.release();
+  return MB_OK;
+}
+
+extern "C" int mb_uneven_info(mb_uneven u, int* persistent_groups, int* fallback_groups, int* samples) {
+  std::lock_guard<std::recursive_mutex> lk(mb::g_mu);
+  if (!u) return MB_EINVAL;
+  if (persistent_groups) *persistent_groups = int(u->pgroups.size());
+  if (fallback_groups) *fallback_groups = int(u->fallback.size());
+  if (samples) *samples = u->nitems;
+  return MB_OK;
+}
+
+extern "C" int mb_uneven_apply(mb_uneven u, int flags) {
+  using namespace mb;
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (int rc = check_init()) return rc;
+  if (!u) return MB_EINVAL;
+  cudaStream_t st = g_ctx.stream;
+  const bool zero = flags & MB_UNEVEN_ZERO;
+  // every group's parameters must be staged on the device, one row per sample
+  for (size_t g = 0; g < u->cs.size(); ++g)
+    if (u->cs[g]->theta_rows != u->ss[g]->batch && u->ss[g]->batch > 0) {
+      set_error("mb_uneven_apply: group %zu has %d staged parameter rows for %d samples", g, u->cs[g]->theta_rows,
+                u->ss[g]->batch);
+      return MB_EINVAL;
+    }
+  if (!u->pgroups.empty()) {
+    std::vector<UnevenGroup> cur;
+    uneven_descriptors(u, cur);
+    if (!same_descriptors(cur, u->hgroups)) {
+      if (int rc = check_not_capturing("mb_uneven_apply after the circuits' parameter buffers moved")) return rc;
+      MB_CHECK_CUDA(cudaMemcpyAsync(u->d_groups, cur.data(), sizeof(UnevenGroup) * cur.size(), cudaMemcpyHostToDevice,
+                                    st));
+      MB_CHECK_CUDA(cudaStreamSynchronize(st));
+      u->hgroups = cur;
+    }
+    const int ng = int(u->hgroups.size());
+    if (u->nbind) {
+      ProfScope ps("k_uneven_bind", 0.0, st);
+      k_uneven_bind<<<unsigned((u->nbind + 127) / 128), 128, 0, st>>>(u->d_groups, ng, u->nbind);
+      MB_LAUNCHED();
+    }
+    if (u->nfuse) {
+      ProfScope ps("k_uneven_fuse", 0.0, st);
+      k_uneven_fuse<<<unsigned((u->nfuse + 127) / 128), 128, 0, st>>>(u->d_groups, ng, u->nfuse);
+      MB_LAUNCHED();
+    }
+    MB_CHECK_CUDA(cudaMemsetAsync(u->d_next, 0, sizeof(unsigned), st));
+    const size_t shm = (size_t(16) << kUnevenMaxTile) + (size_t(8) << kUnevenMaxTile) + 1024;
+    const int grid = std::min(u->nitems, g_ctx.sm_count * 2);
+    ProfScope ps("k_uneven", u->bytes, st, u->flops);
+    auto launch = [&](auto kern) {
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm));
+      kern<<<grid, kUnevenThreads, shm, st>>>(u->d_groups, u->d_passes, u->d_items, u->nitems, u->d_next, zero ? 1 : 0);
+    };
+    u->u2 ? launch(k_uneven<true>) : launch(k_uneven<false>);
+    MB_LAUNCHED();
+  }
+  for (int g : u->fallback) {
+    mb_circuit c = u->cs[g];
+    mb_state s = u->ss[g];
+    if (s->batch == 0) continue;
+    if (zero)
+      if (int rc = launch_set_basis(s->d, s->elems, s->batch, 0, st)) return rc;
+    if (int rc = bind_launch(c, s->batch)) return rc;
+    const int64_t stride = s->kind >= MB_BATCH_PURE ? c->table_elems : 0;
+    if (int rc = apply_fused(c, s, stride)) return rc;
+  }
+  return MB_OK;
+}
+
+extern "C" int mb_uneven_free(mb_uneven u) {
+  std::lock_guard<std::recursive_mutex> lk(mb::g_mu);
+  if (!u) return MB_OK;
+  if (mb::g_ctx.init) mb::uneven_release(u);
+  delete u;
+  return MB_OK;
+}
 
 extern "C" int mb_circuit_passes(mb_circuit c, int* npasses) {
   std::lock_guard<std::recursive_mutex> lk(mb::g_mu);

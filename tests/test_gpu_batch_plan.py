@@ -54,3 +54,42 @@ def test_autotune_keeps_results(mq, O):
     s = mq.apply_(c, mq.StateVector(n))
     ref = O.apply(c.specs(), O.zero_state(n), n)
     assert np.max(np.abs(s.to_numpy() - ref)) <= 1e-12
+
+
+def test_persistent_uneven_launch(mq, O):
+    """Pure samples of 8..17 qubits with per-sample angles run in one persistent launch (a CTA
+    per sample, all of its passes); a 6-qubit and an 18-qubit group take the per-size path
+    after it. Every sample's expectation and every 8- and 17-qubit amplitude against the oracle
+    run alone; the launch list holds exactly one k_uneven per replay."""
+    from mossquantum_b200 import _native as N
+    from mossquantum_b200 import workloads as W
+    from mossquantum_b200.batch import BatchPlan
+    sizes = {6: 2, 8: 3, 11: 2, 14: 2, 17: 2, 18: 1}
+    depth = 3
+    groups = {n: (W.hea_circuit(n, depth), B) for n, B in sizes.items()}
+    plan = BatchPlan(groups, W.xxz)
+    assert plan.persistent_info() == (4, 2, 9)
+    rng = np.random.default_rng(17)
+    thetas = {n: rng.uniform(0, 2 * np.pi, size=(B, groups[n][0].nparameters())) for n, B in sizes.items()}
+    res = plan.run(thetas)
+    for n, B in sizes.items():
+        for b in range(B):
+            c = groups[n][0].copy().reset_parameters(thetas[n][b])
+            psi = O.apply(c.specs(), O.zero_state(n), n)
+            assert abs(res[n][b] - O.expect(psi, n, W.xxz(n).specs())) <= 1e-11, (n, b)
+            if n in (8, 17):
+                g = [x for x in plan.groups if x["n"] == n][0]
+                got = g["state"].to_numpy()[:, b]
+                assert np.max(np.abs(got - psi)) <= 1e-12, (n, b)
+    # the recorded body run eagerly: one persistent launch for the four middle sizes
+    plan._stage(thetas)
+    N.profile(True)
+    try:
+        plan._record_body()
+        N.synchronize()
+        rep = N.profile_report()
+    finally:
+        N.profile(False)
+    assert rep["k_uneven"][0] == 1, rep
+    assert "k_tile_pass" not in rep, rep
+    plan.close()
