@@ -1174,6 +1174,25 @@ static void plan_stages(const std::vector<FOp>& fops, const std::vector<int>& op
       if ((gm >> g) & 1) m |= uint64_t(1) << loc[g];
     return m;
   };
+  // Warp bits: a stage of 2^(t-R) threads has t-R-5 warp-index bits. Local bits >= 6 that the
+  // fewest ops need in registers are kept as the warp bits of every stage that leaves them out
+  // of its registers, so consecutive such stages exchange amplitudes within each warp only
+  // (the specialised kernels then end those stages with __syncwarp instead of a CTA barrier).
+  const int nw = std::max(0, t - R - 5);
+  std::vector<int> wbits;
+  if (nw > 0 && t - 6 >= nw) {
+    std::vector<std::pair<int, int>> cnt;
+    for (int q = 6; q < t; ++q) {
+      int c = 0;
+      for (int idx : ops) c += int((lmask(fops[idx].nd) >> q) & 1);
+      cnt.push_back({c, -q});
+    }
+    std::sort(cnt.begin(), cnt.end());
+    for (int i = 0; i < nw; ++i) wbits.push_back(-cnt[i].second);
+    std::sort(wbits.begin(), wbits.end());
+  }
+  uint64_t wmask = 0;
+  for (int q : wbits) wmask |= uint64_t(1) << q;
   std::vector<int> rem = ops;
   while (!rem.empty()) {
     std::vector<int> regs;
@@ -1192,14 +1211,19 @@ static void plan_stages(const std::vector<FOp>& fops, const std::vector<int>& op
       }
       if (int(regs.size()) == R) break;
     }
-    // Fill the register set with bank-neutral high bits first.
+    // Fill the register set with bank-neutral high bits first, the warp bits last.
     for (int q = t - 1; q >= 0 && int(regs.size()) < R; --q)
-      if (!((rmask >> q) & 1) && q >= 6) {
+      if (!((rmask >> q) & 1) && q >= 6 && !((wmask >> q) & 1)) {
         regs.push_back(q);
         rmask |= uint64_t(1) << q;
       }
     for (int q = 0; q < t && int(regs.size()) < R; ++q)
-      if (!((rmask >> q) & 1)) {
+      if (!((rmask >> q) & 1) && !((wmask >> q) & 1)) {
+        regs.push_back(q);
+        rmask |= uint64_t(1) << q;
+      }
+    for (int q : wbits)
+      if (int(regs.size()) < R && !((rmask >> q) & 1)) {
         regs.push_back(q);
         rmask |= uint64_t(1) << q;
       }
@@ -1237,8 +1261,15 @@ static void plan_stages(const std::vector<FOp>& fops, const std::vector<int>& op
         tidb.push_back(q);
         used_res[q % 3] = true;
       }
+    // the other thread bits ascending; the warp bits last (the top thread-index bits) when this
+    // stage holds none of them in registers
+    const bool keep_w = !wbits.empty() && (rmask & wmask) == 0;
     for (int q = 0; q < t; ++q)
-      if (!((rmask >> q) & 1) && std::find(tidb.begin(), tidb.end(), q) == tidb.end()) tidb.push_back(q);
+      if (!((rmask >> q) & 1) && std::find(tidb.begin(), tidb.end(), q) == tidb.end() &&
+          !(keep_w && ((wmask >> q) & 1)))
+        tidb.push_back(q);
+    if (keep_w)
+      for (int q : wbits) tidb.push_back(q);
     sd.ntid = int(tidb.size());
     for (int q = 0; q < sd.ntid; ++q) sd.tid[q] = tidb[q];
     sd.op0 = int(p.mops.size());

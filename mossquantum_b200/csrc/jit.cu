@@ -625,6 +625,18 @@ static std::string shared_mats_fill(const SharedMats& sm) {
   return o.str();
 }
 
+// Barrier after register stage i: none after the last (the proxy fence and the CTA barrier
+// before the tile's store follow); __syncwarp when stage i+1 keeps the same warp-index bits
+// (every warp then reads back only what it wrote); else a CTA barrier.
+static const char* stage_sync(const Pass& p, size_t i) {
+  if (i + 1 == p.stages.size()) return "";
+  const StageDesc& a = p.stages[i];
+  const StageDesc& b = p.stages[i + 1];
+  bool same = a.ntid == b.ntid;
+  for (int q = 5; same && q < a.ntid; ++q) same = a.tid[q] == b.tid[q];
+  return same ? "      __syncwarp();\n" : "      __syncthreads();\n";
+}
+
 std::string jit_tile_source(const Pass& p, int R, int N, bool stage_params, int ctas) {
   std::ostringstream o;
   const int A = 1 << R;
@@ -714,7 +726,8 @@ std::string jit_tile_source(const Pass& p, int R, int N, bool stage_params, int 
   o << "    double2 ";
   for (int j = 0; j < A; ++j) o << (j ? ", " : "") << "a" << j;
   o << ";\n";
-  for (const StageDesc& sd : p.stages) {
+  for (size_t si = 0; si < p.stages.size(); ++si) {
+    const StageDesc& sd = p.stages[si];
     o << "    {\n      const u32 lb = 0u";
     for (int q = 0; q < sd.ntid; ++q) o << " | (((tx >> " << q << ") & 1u) << " << sd.tid[q] << ")";
     o << ";\n";
@@ -725,7 +738,7 @@ std::string jit_tile_source(const Pass& p, int R, int N, bool stage_params, int 
     for (int j = 0; j < A; ++j) sg.nm[j] = j;
     for (int q = 0; q < sd.nops; ++q) sg.emit(p.mops[sd.op0 + q]);
     for (int j = 0; j < A; ++j) o << "      tl[swz(lb | " << reg_off_const(j, R, sd.reg) << ")] = " << sg.v(j) << ";\n";
-    o << "      __syncthreads();\n    }\n";
+    o << stage_sync(p, si) << "    }\n";
   }
   o << "    asm volatile(\"fence.proxy.async.shared::cta;\" ::: \"memory\");\n    __syncthreads();\n";
   {
@@ -919,7 +932,8 @@ std::string jit_adjoint_source(const Pass& p, int R, int N, bool stage_params, i
   o << "    double2 ";
   for (int j = 0; j < A; ++j) o << (j ? ", " : "") << "y" << j << ", d" << j;
   o << ";\n";
-  for (const StageDesc& sd : p.stages) {
+  for (size_t si = 0; si < p.stages.size(); ++si) {
+    const StageDesc& sd = p.stages[si];
     o << "    {\n      const u32 lb = 0u";
     for (int q = 0; q < sd.ntid; ++q) o << " | (((tx >> " << q << ") & 1u) << " << sd.tid[q] << ")";
     o << ";\n";
@@ -956,7 +970,7 @@ std::string jit_adjoint_source(const Pass& p, int R, int N, bool stage_params, i
     for (int j = 0; j < A; ++j)
       o << "      ty[swz(lb | " << reg_off_const(j, R, sd.reg) << ")] = " << gy.v(j) << "; td[swz(lb | "
         << reg_off_const(j, R, sd.reg) << ")] = " << gd.v(j) << ";\n";
-    o << "      __syncthreads();\n    }\n";
+    o << stage_sync(p, si) << "    }\n";
   }
   o << "    asm volatile(\"fence.proxy.async.shared::cta;\" ::: \"memory\");\n    __syncthreads();\n";
   o << "    if (tx == 0) { " << subst(st, "", "&tmy", "ty", "") << " " << subst(st, "", "&tmd", "td", "") << " }\n";
