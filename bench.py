@@ -413,6 +413,16 @@ def _case_setup(name, mq, W):
         th = c.active_parameters()
         return f"K6 adjoint dual-state passes: HEA n={n} depth {depth}", \
             lambda: mq.value_and_gradient(mq.AdjointGradient(), obj, th)
+    if name == "grad24":
+        # the gradient workload's pure part: 24 qubits, depth 16, 1152 angles, checkpoints
+        # every 4 layers (every kernel of one value_and_gradient in the report)
+        n, depth = 24, 16
+        c = W.hea_circuit(n, depth, W.hea_angles(n, depth, W.rng_for(3)))
+        obj = mq.ExpectationObjective(c, W.tfim(n), mq.StateVector(n))
+        th = c.active_parameters()
+        method = mq.AdjointGradient(checkpoint_every=4 * (3 * n + n - 1))
+        return f"K6 adjoint gradient: HEA n={n} depth {depth}, 1152 angles", \
+            lambda: mq.value_and_gradient(method, obj, th)
     if name == "marginal":
         n = 26
         s = mq.StateVector(n)
@@ -451,8 +461,8 @@ def _case_setup(name, mq, W):
     raise ValueError(f"unknown kernel case {name}")
 
 
-KERNEL_CASES = ("dense1_low", "dense1_high", "tile", "density", "pauli", "adjoint", "marginal", "dmma", "dense5",
-                "batch_pure", "batch_pure_small")
+KERNEL_CASES = ("dense1_low", "dense1_high", "tile", "density", "pauli", "adjoint", "grad24", "marginal", "dmma",
+                "dense5", "batch_pure", "batch_pure_small")
 
 
 def kernel_workload(args):
