@@ -394,6 +394,7 @@ static double mop_flops(const MOp& m) {
     case MOP_RROT: case MOP_IROT: return 8.0;  // four real multiply-adds per amplitude
     case MOP_LIFT: return 6.0;                 // three fused multiply-adds per amplitude
     case MOP_GRADP: return 4.0;                // two multiply-adds per amplitude
+    case MOP_CHAN: return 4.0;                 // 12 real multiply-adds per 4 amplitudes
     default: return 0.0;
   }
 }
@@ -850,6 +851,46 @@ static void fuse_runs(mb_circuit c, std::vector<FOp>& seq, int n, bool dm, Sched
 // S: the schedule being built; when given (forward schedules), single-qubit runs are fused at
 // bind time and fixed single-qubit ops are split into phases and shear rotations, with the
 // phases merged.
+// Fixed single-qubit channel supermatrices on a density matrix's (row q, column q + n) pair
+// whose entries are real with the population/coherence pattern of depolarizing, amplitude
+// damping and dephasing channels (and of their products, inverses and adjoints) run as
+// MOP_CHAN: populations mix through a real 2x2, coherences scale by real factors, 12 real
+// multiply-adds per 4 amplitudes instead of 64 for a dense complex 4x4.
+static void chan_forms(mb_circuit c, std::vector<FOp>& seq, int n, const std::vector<double2>* xt) {
+  static const int keep[6] = {0, 12, 5, 10, 3, 15};  // (0,0) (0,3) (1,1) (2,2) (3,0) (3,3), column-major
+  for (FOp& f : seq) {
+    if (f.type != MOP_U2 || f.param || f.nb != 2 || f.tgt[0] >= n || f.tgt[1] != f.tgt[0] + n) continue;
+    bool ok = true;
+    for (int e = 0; e < 16 && ok; ++e) {
+      const int o = f.off[e];
+      double2 x;
+      if (o & kXtabFlag) {
+        const size_t i = size_t(o & ~kXtabFlag);
+        if (!xt || i >= xt->size()) {
+          ok = false;
+          break;
+        }
+        x = (*xt)[i];
+      } else {
+        if (o < 0 || size_t(o) >= c->fixed_table.size()) {
+          ok = false;
+          break;
+        }
+        x = c->fixed_table[size_t(o)];
+      }
+      const bool in = e == 0 || e == 12 || e == 5 || e == 10 || e == 3 || e == 15;
+      if (x.y != 0.0 || (!in && x.x != 0.0)) ok = false;
+    }
+    if (!ok) continue;
+    int no[6];
+    for (int k = 0; k < 6; ++k) no[k] = f.off[keep[k]];
+    std::memset(f.off, 0, sizeof(f.off));
+    for (int k = 0; k < 6; ++k) f.off[k] = no[k];
+    f.type = MOP_CHAN;
+    f.conj = 0;
+  }
+}
+
 static void build_fops(mb_circuit c, int n, int dm, bool dagger, std::vector<FOp>& out, int lo = 0, int hi = -1,
                        Schedule* S = nullptr) {
   out.clear();
@@ -898,6 +939,7 @@ static void build_fops(mb_circuit c, int n, int dm, bool dagger, std::vector<FOp
       seq.swap(split);
     }
   }
+  if (dm && !getenv("MB_NO_CHAN")) chan_forms(c, seq, n, S ? &S->xtab : nullptr);
   out = seq;
 }
 
@@ -1054,6 +1096,7 @@ static bool build_adjoint_fops(mb_circuit c, int lo, int hi, std::vector<FOp>& o
       if (dm) out.push_back(grad_fop(op, n));
     }
   }
+  if (dm && !getenv("MB_NO_CHAN")) chan_forms(c, out, n, xt);
   return true;
 }
 
@@ -1321,6 +1364,9 @@ static void plan_stages(const std::vector<FOp>& fops, const std::vector<int>& op
           }
           m.r0 = int16_t(ra);
           m.r1 = int16_t(rb);
+        } else if (f.type == MOP_CHAN) {
+          m.r0 = int16_t(regidx(f.tgt[0]));  // row bit
+          m.r1 = int16_t(regidx(f.tgt[1]));  // column bit
         } else if (f.type == MOP_DIAG) {
           m.nsel = int16_t(f.nb);
           for (int j = 0; j < f.nb; ++j) m.sel[j] = sel(f.bits[j]);
@@ -1447,6 +1493,9 @@ static void encode_reg_pass(const std::vector<FOp>& fops, const std::vector<int>
       }
       m.r0 = int16_t(ra);
       m.r1 = int16_t(rb);
+    } else if (f.type == MOP_CHAN) {
+      m.r0 = int16_t(regidx(f.tgt[0]));
+      m.r1 = int16_t(regidx(f.tgt[1]));
     } else if (f.type == MOP_DIAG) {
       m.nsel = int16_t(f.nb);
       for (int j = 0; j < f.nb; ++j) m.sel[j] = int16_t(f.bits[j]);
@@ -1609,7 +1658,7 @@ static void build_schedule(Schedule& S, int nsamples, bool allow_reg = true) {
     p.geom = bg;
     if (p.kind == PASS_TILE) plan_stages(S.fops, best_taken, p, R, S.adjoint ? nullptr : &S.xtab);
     else encode_reg_pass(S.fops, best_taken, p);
-    for (const MOp& m : p.mops) p.has_u2 |= m.type == MOP_U2;
+    for (const MOp& m : p.mops) p.has_u2 |= m.type == MOP_U2 || m.type == MOP_CHAN;
     S.passes.push_back(p);
     std::vector<int> left;
     size_t k = 0;
@@ -1814,9 +1863,10 @@ static int get_schedule_impl(mb_circuit c, int n, int dm, int adjoint, int lo, i
     for (const MOp& m : p.mops) {
       const bool needs = m.type == MOP_U1 || m.type == MOP_CTRL || m.type == MOP_CTRLX || m.type == MOP_U2 ||
                          m.type == MOP_GRAD || m.type == MOP_RROT || m.type == MOP_IROT || m.type == MOP_LIFT ||
-                         m.type == MOP_GRADP;
+                         m.type == MOP_GRADP || m.type == MOP_CHAN;
       const bool two = m.type == MOP_U2 || (m.type == MOP_GRAD && m.nsel == 2);
-      if (needs && (m.r0 < 0 || m.r0 >= R || (two && (m.r1 <= m.r0 || m.r1 >= R)))) {
+      const bool chan_bad = m.type == MOP_CHAN && (m.r1 < 0 || m.r1 >= R || m.r1 == m.r0);
+      if (needs && (m.r0 < 0 || m.r0 >= R || (two && (m.r1 <= m.r0 || m.r1 >= R)) || chan_bad)) {
         set_error("internal scheduling error: micro-op %d without a register target", int(m.type));
         return MB_EUNSUPPORTED;
       }
@@ -2749,6 +2799,21 @@ void host_apply_fop(const HostLowering& L, const FOp& f, std::vector<hcd>& v) {
       }
       return;
     }
+    case MOP_CHAN: {
+      double k[6];
+      for (int e = 0; e < 6; ++e) k[e] = L.el(f.off[e], 0, f.param).real();
+      const int b0 = f.tgt[0], b1 = f.tgt[1];
+      for (int64_t i = 0; i < len; ++i) {
+        if (bit(i, b0) || bit(i, b1)) continue;
+        const int64_t i1 = i | (int64_t(1) << b0), i2 = i | (int64_t(1) << b1), i3 = i1 | i2;
+        const hcd x0 = v[i], x3 = v[i3];
+        v[i] = k[0] * x0 + k[1] * x3;
+        v[i3] = k[4] * x0 + k[5] * x3;
+        v[i1] *= k[2];
+        v[i2] *= k[3];
+      }
+      return;
+    }
     case MOP_DIAG: {
       for (int64_t i = 0; i < len; ++i) {
         int a = 0;
@@ -2826,6 +2891,21 @@ void host_apply_mop(const HostLowering& L, const Pass& p, const StageDesc& sd, c
           for (int q = 0; q < 4; ++q) y[r] += el(r + 4 * q) * x[q];
         }
         for (int a = 0; a < 4; ++a) v[id[a]] = y[a];
+      }
+      return;
+    }
+    case MOP_CHAN: {
+      const int b0 = gbit_of_reg(m.r0), b1 = gbit_of_reg(m.r1);
+      double k[6];
+      for (int e = 0; e < 6; ++e) k[e] = el(e).real();
+      for (int64_t i = 0; i < len; ++i) {
+        if (bit(i, b0) || bit(i, b1)) continue;
+        const int64_t i1 = i | (int64_t(1) << b0), i2 = i | (int64_t(1) << b1), i3 = i1 | i2;
+        const hcd x0 = v[i], x3 = v[i3];
+        v[i] = k[0] * x0 + k[1] * x3;
+        v[i3] = k[4] * x0 + k[5] * x3;
+        v[i1] *= k[2];
+        v[i2] *= k[3];
       }
       return;
     }

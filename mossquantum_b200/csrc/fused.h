@@ -25,6 +25,10 @@ enum MopType : int16_t {
   MOP_GRADP = 10, // adjoint sweep: Re<y|D|delta> on register bit r0 for a constant generator of
                   // a rotation family, D = (i/2)X, (i/2)Y, (i/2)Z or diag(0, -i) (r1 = 1..4),
                   // negated when conj = 1 (adjoint gates); active = accumulator index
+  MOP_CHAN = 11,  // single-qubit channel on a density matrix whose supermatrix is real with the
+                  // population/coherence pattern of depolarizing, damping and dephasing channels:
+                  // row bit r0, column bit r1, populations x00' = a x00 + b x11, x11' = e x00 +
+                  // f x11, coherences x10' = c x10, x01' = d x01 (real parts of off[0..5] = a..f)
 };
 
 // Matrix offsets with this bit set index the schedule's own table of derived coefficients

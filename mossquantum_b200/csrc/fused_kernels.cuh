@@ -155,6 +155,23 @@ __device__ __forceinline__ void u2(double2 (&a)[1 << R], const double2* m, const
     }
 }
 
+// Real channel supermatrix on (row bit K0, column bit K1): populations mix through a 2x2,
+// coherences scale (MOP_CHAN).
+template <int R, int K0, int K1>
+__device__ __forceinline__ void chan(double2 (&a)[1 << R], double ca, double cb, double cc, double cd, double ce,
+                                     double cf) {
+#pragma unroll
+  for (int j = 0; j < (1 << R); ++j)
+    if (!((j >> K0) & 1) && !((j >> K1) & 1)) {
+      const int i1 = j | (1 << K0), i2 = j | (1 << K1), i3 = j | (1 << K0) | (1 << K1);
+      const double2 x0 = a[j], x3 = a[i3];
+      a[j] = make_double2(fma(ca, x0.x, cb * x3.x), fma(ca, x0.y, cb * x3.y));
+      a[i3] = make_double2(fma(ce, x0.x, cf * x3.x), fma(ce, x0.y, cf * x3.y));
+      a[i1] = make_double2(cc * a[i1].x, cc * a[i1].y);
+      a[i2] = make_double2(cd * a[i2].x, cd * a[i2].y);
+    }
+}
+
 template <int R>
 __device__ __forceinline__ void diag(double2 (&a)[1 << R], const double2* m, const double2* xt, const MOp* __restrict__ op,
                                      int nsel, int conj, uint64_t lbase, const int* reg, uint64_t gbase) {
@@ -320,6 +337,19 @@ __device__ __forceinline__ void run_mops(double2 (&a)[1 << R], const MOp* __rest
     } else if (type == MOP_DIAG) {
       diag<R>(a, m, xt, op, nsel, conj, lbase, reg, gbase);
     } else if constexpr (HAS_U2) {
+      if (type == MOP_CHAN) {
+        const double ca = ldm(m, xt, op->off[0], 0).x, cb = ldm(m, xt, op->off[1], 0).x;
+        const double cc = ldm(m, xt, op->off[2], 0).x, cd = ldm(m, xt, op->off[3], 0).x;
+        const double ce = ldm(m, xt, op->off[4], 0).x, cf = ldm(m, xt, op->off[5], 0).x;
+#define FK_CHAN(K0, K1) \
+  case K0 * 8 + K1: if constexpr (K0 < R && K1 < R) chan<R, K0, K1>(a, ca, cb, cc, cd, ce, cf); break;
+        switch (r0 * 8 + op->r1) {
+          FK_CHAN(0, 1) FK_CHAN(0, 2) FK_CHAN(0, 3) FK_CHAN(0, 4) FK_CHAN(1, 0) FK_CHAN(1, 2) FK_CHAN(1, 3)
+          FK_CHAN(1, 4) FK_CHAN(2, 0) FK_CHAN(2, 1) FK_CHAN(2, 3) FK_CHAN(2, 4) FK_CHAN(3, 0) FK_CHAN(3, 1)
+          FK_CHAN(3, 2) FK_CHAN(3, 4) FK_CHAN(4, 0) FK_CHAN(4, 1) FK_CHAN(4, 2) FK_CHAN(4, 3)
+        }
+#undef FK_CHAN
+      }
       if (type == MOP_U2) {
         switch (r0 * 8 + op->r1) {
           case 0 * 8 + 1: u2<R, 0, 1>(a, m, xt, op, conj); break;

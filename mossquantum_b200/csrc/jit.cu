@@ -331,6 +331,22 @@ struct StageGen {
         o << "}\n";
         break;
       }
+      case MOP_CHAN: {
+        const int b0 = 1 << m.r0, b1 = 1 << m.r1;
+        o << "{ const double ca = (" << ldm(m, 0) << ").x, cb = (" << ldm(m, 1) << ").x, cc = (" << ldm(m, 2)
+          << ").x, cd = (" << ldm(m, 3) << ").x, ce = (" << ldm(m, 4) << ").x, cf = (" << ldm(m, 5) << ").x;\n";
+        for (int j = 0; j < A; ++j)
+          if (!(j & b0) && !(j & b1)) {
+            const std::string x0 = v(j), x1 = v(j | b0), x2 = v(j | b1), x3 = v(j | b0 | b1);
+            o << "  { const double2 p0 = " << x0 << ", p3 = " << x3 << "; " << x0
+              << " = make_double2(fma(ca, p0.x, cb * p3.x), fma(ca, p0.y, cb * p3.y)); " << x3
+              << " = make_double2(fma(ce, p0.x, cf * p3.x), fma(ce, p0.y, cf * p3.y)); " << x1 << " = make_double2(cc * "
+              << x1 << ".x, cc * " << x1 << ".y); " << x2 << " = make_double2(cd * " << x2 << ".x, cd * " << x2
+              << ".y); }\n";
+          }
+        o << "}\n";
+        break;
+      }
       case MOP_U2: {
         const int b0 = 1 << m.r0, b1 = 1 << m.r1;
         o << "{ double2 u[16];\n";
@@ -568,6 +584,7 @@ static SharedMats shared_mats(const Pass& p, bool with_params) {
       case MOP_U1: case MOP_CTRL: case MOP_RROT: case MOP_IROT: for (int e = 0; e < 4; ++e) add(e); break;
       case MOP_LIFT: add(0); break;
       case MOP_U2: for (int e = 0; e < 16; ++e) add(e); break;
+      case MOP_CHAN: for (int e = 0; e < 6; ++e) add(e); break;
       case MOP_DIAG: for (int e = 0; e < (1 << m.nsel); ++e) if ((m.active >> e) & 1) add(e); break;
       case MOP_CPHASE: if (!m.r1) add(0); break;
       case MOP_GRAD: for (int e = 0; e < (m.nsel == 1 ? 4 : 16); ++e) add(e); break;
