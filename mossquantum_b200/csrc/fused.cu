@@ -183,13 +183,16 @@ __global__ void k_fuse(const FuseRec* __restrict__ recs, int nrecs, const FuseCo
 // Host: fused ops
 // ---------------------------------------------------------------------------------------------
 // Persistent uneven batch: one launch over samples of different register sizes, each with its
-// own parameters. A CTA takes one sample at a time from a work counter (largest samples first)
-// and runs that sample's whole circuit: the |0..0> start and every tile pass of its size's
-// schedule, tile by tile. A sample is owned by one CTA, so the passes need no synchronisation
-// between CTAs; samples of at most 2^17 amplitudes (2 MiB) keep their passes in L2. Two
-// launches before it bind every sample's parameter row and form its fused single-qubit
-// products, for all sizes at once (the pass kernel reads the tables through the read-only
-// cache, so they are written before it starts).
+// own parameters. The work items are (sample, pass, chunk of up to 2^15 amplitudes' tiles),
+// ordered by pass index first, so every pass-0 chunk of every sample comes before any pass-1
+// chunk; CTAs take items from a work counter. Before an item of pass p a CTA waits until its
+// sample has completed every chunk of pass p-1 (a per-sample counter); those chunks were all
+// taken earlier by running CTAs, so the wait always ends (it is also bounded, and sets the
+// error flag). Pass 0 generates |0..0> instead of loading. Chunks of one pass touch disjoint
+// amplitudes; the state is read through L2 (ld.global.cg), so another SM's writes of the
+// previous pass are seen after the counter. Two launches before it bind every sample's
+// parameter row and form its fused single-qubit products, for all sizes at once (the pass
+// kernel reads the tables through the read-only cache, so they are written before it starts).
 constexpr int kUnevenThreads = 128;
 constexpr int kUnevenMaxTile = 11;   // 2^11-amplitude tiles, 16 amplitudes per thread
 
@@ -197,6 +200,8 @@ struct UnevenGroup {
   int n;                      // amplitude bits of one sample
   int B;                      // samples
   int pass0, npasses;         // this size's passes in the plan's pass array
+  int sample0;                // first of this group's per-sample completion counters
+  int nchunks;                // items per pass and sample
   int64_t bind0, fuse0;       // first work item of this group in the bind and fuse launches
   int nbinds, nslots;
   const BindRec* binds;
@@ -252,71 +257,93 @@ __global__ void k_uneven_fuse(const UnevenGroup* __restrict__ groups, int ng, in
   for (int e = 0; e < rec.d * rec.d; ++e) out[e] = M[e];
 }
 
+// Work item: x = group, y = sample, z = pass index within the group, w = chunk.
 template <bool U2>
 __global__ void __launch_bounds__(kUnevenThreads, 2)
     k_uneven(const UnevenGroup* __restrict__ groups, const UnevenPass* __restrict__ passes,
-             const int2* __restrict__ items, int nitems, unsigned* next, int zero_init) {
+             const int4* __restrict__ items, int nitems, unsigned* next, unsigned* done, int zero_init,
+             unsigned* err) {
   constexpr int R = 4;
   extern __shared__ unsigned char smem_raw[];
   double2* tl = reinterpret_cast<double2*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* loc = reinterpret_cast<uint64_t*>(tl + (1 << kUnevenMaxTile));
-  __shared__ int s_item;
+  __shared__ int s_item, s_ok;
   const int tx = threadIdx.x;
   for (;;) {
     if (tx == 0) s_item = int(atomicAdd(next, 1u));
     __syncthreads();
     const int item = s_item;
-    __syncthreads();
     if (item >= nitems) break;
-    const int2 it = items[item];
-    const UnevenGroup G = groups[it.x];
-    const int b = it.y;
+    const int4 it = items[item];
+    const UnevenGroup& G = groups[it.x];
+    const int b = it.y, pi = it.z, chunk = it.w;
+    unsigned* cnt = done + G.sample0 + b;
+    if (tx == 0) {
+      // every chunk of the previous passes of this sample
+      const unsigned need = unsigned(pi) * unsigned(G.nchunks);
+      int ok = 1;
+      for (uint32_t spin = 0; atomicAdd(cnt, 0u) < need; ++spin) {
+        if (spin > (1u << 24)) {
+          atomicOr(err, 1u);
+          ok = 0;
+          break;
+        }
+        __nanosleep(64);
+      }
+      __threadfence();
+      s_ok = ok;
+    }
+    __syncthreads();
+    if (!s_ok) break;
+    const UnevenPass& P = passes[G.pass0 + pi];
+    const int t = P.t, T = 1 << t;
     const int64_t dim = int64_t(1) << G.n;
     double2* v = G.states + int64_t(b) * dim;
     const double2* xs = G.xtabs ? G.xtabs + int64_t(b) * G.xrow : nullptr;
-    if (zero_init)
-      for (int64_t j = tx; j < dim; j += kUnevenThreads) v[j] = make_double2(j == 0 ? 1.0 : 0.0, 0.0);
-    __syncthreads();
-    for (int pi = 0; pi < G.npasses; ++pi) {
-      const UnevenPass& P = passes[G.pass0 + pi];
-      const int t = P.t, T = 1 << t;
-      for (int l = tx; l < T; l += kUnevenThreads) {
-        uint64_t o = 0;
-        for (int q = 0; q < t; ++q) o |= uint64_t((l >> q) & 1) << P.bits[q];
-        loc[l] = o;
-      }
-      __syncthreads();
-      const int64_t ntiles = dim >> t;
-      for (int64_t tile = 0; tile < ntiles; ++tile) {
-        uint64_t base = uint64_t(tile);
-        for (int q = 0; q < t; ++q) {
-          const int p = P.bits[q];
-          base = ((base >> p) << (p + 1)) | (base & ((uint64_t(1) << p) - 1));
-        }
-        for (int l = tx; l < T; l += kUnevenThreads) tl[fk::swz(uint32_t(l))] = v[base | loc[l]];
-        __syncthreads();
-        for (int s = 0; s < P.nstages; ++s) {
-          const StageDesc& sd = P.stages[s];
-          int reg[kMaxRegBits];
-#pragma unroll
-          for (int k = 0; k < R; ++k) reg[k] = sd.reg[k];
-          const int vthreads = 1 << sd.ntid;
-          for (int vt = tx; vt < vthreads; vt += kUnevenThreads) {
-            uint32_t lbase = 0;
-            for (int q = 0; q < sd.ntid; ++q) lbase |= ((uint32_t(vt) >> q) & 1u) << sd.tid[q];
-            double2 a[1 << R];
-#pragma unroll
-            for (int j = 0; j < (1 << R); ++j) a[j] = tl[fk::swz(lbase | uint32_t(fk::reg_offset<R>(j, reg)))];
-            fk::run_mops<R, U2>(a, P.mops + sd.op0, sd.nops, lbase, reg, base, G.table, G.xtab, xs, G.tstride, b);
-#pragma unroll
-            for (int j = 0; j < (1 << R); ++j) tl[fk::swz(lbase | uint32_t(fk::reg_offset<R>(j, reg)))] = a[j];
-          }
-          __syncthreads();
-        }
-        for (int l = tx; l < T; l += kUnevenThreads) v[base | loc[l]] = tl[fk::swz(uint32_t(l))];
-        __syncthreads();
-      }
+    for (int l = tx; l < T; l += kUnevenThreads) {
+      uint64_t o = 0;
+      for (int q = 0; q < t; ++q) o |= uint64_t((l >> q) & 1) << P.bits[q];
+      loc[l] = o;
     }
+    __syncthreads();
+    const int64_t ntiles = dim >> t;
+    const int64_t per = (ntiles + G.nchunks - 1) / G.nchunks;
+    const int64_t t0 = int64_t(chunk) * per, t1 = t0 + per < ntiles ? t0 + per : ntiles;
+    const bool gen = zero_init && pi == 0;
+    for (int64_t tile = t0; tile < t1; ++tile) {
+      uint64_t base = uint64_t(tile);
+      for (int q = 0; q < t; ++q) {
+        const int p = P.bits[q];
+        base = ((base >> p) << (p + 1)) | (base & ((uint64_t(1) << p) - 1));
+      }
+      for (int l = tx; l < T; l += kUnevenThreads)
+        tl[fk::swz(uint32_t(l))] = gen ? make_double2((base | loc[l]) == 0 ? 1.0 : 0.0, 0.0) : __ldcg(v + (base | loc[l]));
+      __syncthreads();
+      for (int s = 0; s < P.nstages; ++s) {
+        const StageDesc& sd = P.stages[s];
+        int reg[kMaxRegBits];
+#pragma unroll
+        for (int k = 0; k < R; ++k) reg[k] = sd.reg[k];
+        const int vthreads = 1 << sd.ntid;
+        for (int vt = tx; vt < vthreads; vt += kUnevenThreads) {
+          uint32_t lbase = 0;
+          for (int q = 0; q < sd.ntid; ++q) lbase |= ((uint32_t(vt) >> q) & 1u) << sd.tid[q];
+          double2 a[1 << R];
+#pragma unroll
+          for (int j = 0; j < (1 << R); ++j) a[j] = tl[fk::swz(lbase | uint32_t(fk::reg_offset<R>(j, reg)))];
+          fk::run_mops<R, U2>(a, P.mops + sd.op0, sd.nops, lbase, reg, base, G.table, G.xtab, xs, G.tstride, b);
+#pragma unroll
+          for (int j = 0; j < (1 << R); ++j) tl[fk::swz(lbase | uint32_t(fk::reg_offset<R>(j, reg)))] = a[j];
+        }
+        __syncthreads();
+      }
+      for (int l = tx; l < T; l += kUnevenThreads) v[base | loc[l]] = tl[fk::swz(uint32_t(l))];
+      __syncthreads();
+    }
+    // publish this chunk: every thread's stores, then the counter
+    __threadfence();
+    __syncthreads();
+    if (tx == 0) atomicAdd(cnt, 1u);
   }
 }
 
@@ -2318,8 +2345,9 @@ struct mb_uneven_s {
   std::vector<mb::UnevenPass> hpasses;
   mb::UnevenGroup* d_groups = nullptr;
   mb::UnevenPass* d_passes = nullptr;
-  int2* d_items = nullptr;
-  unsigned* d_next = nullptr;
+  int4* d_items = nullptr;
+  unsigned* d_next = nullptr;           // work counter, then one completion counter per sample
+  int nsamples = 0;
   int nitems = 0;
   int64_t nbind = 0, nfuse = 0;
   bool u2 = false;
@@ -2334,7 +2362,7 @@ constexpr int kUnevenMaxBits = 17;
 // when a larger batch of parameters is staged).
 void uneven_descriptors(mb_uneven u, std::vector<UnevenGroup>& out) {
   out.clear();
-  int pass0 = 0;
+  int pass0 = 0, sample0 = 0;
   int64_t b0 = 0, f0 = 0;
   for (size_t i = 0; i < u->pgroups.size(); ++i) {
     mb_circuit c = u->cs[u->pgroups[i]];
@@ -2346,6 +2374,11 @@ void uneven_descriptors(mb_uneven u, std::vector<UnevenGroup>& out) {
     g.pass0 = pass0;
     g.npasses = int(S->passes.size());
     pass0 += g.npasses;
+    g.sample0 = sample0;
+    sample0 += g.B;
+    // chunks of up to 2^15 amplitudes (the same for every pass of the group: its tiles are
+    // at most 2^11 amplitudes, so a pass has at least 2^(n-11) tiles)
+    g.nchunks = int(std::max<int64_t>(1, (int64_t(1) << s->n) >> 15));
     g.bind0 = b0;
     g.fuse0 = f0;
     g.nbinds = int(c->binds.size());
@@ -2436,12 +2469,22 @@ extern "C" int mb_uneven_create(const mb_circuit* circuits, const mb_state* stat
       u->flops += pass_flops_per_amp(p, false) * amps;
     }
   }
-  std::vector<int2> items;
-  for (size_t i = 0; i < u->pgroups.size(); ++i)
-    for (int b = 0; b < u->ss[u->pgroups[i]]->batch; ++b) items.push_back(make_int2(int(i), b));
-  u->nitems = int(items.size());
   int rc;
   uneven_descriptors(u.get(), u->hgroups);
+  // items by pass index first (every chunk of pass p of every sample before any of pass p+1),
+  // then largest groups first
+  std::vector<int4> items;
+  int maxp = 0;
+  for (const UnevenGroup& g : u->hgroups) maxp = std::max(maxp, g.npasses);
+  for (int pi = 0; pi < maxp; ++pi)
+    for (size_t i = 0; i < u->hgroups.size(); ++i) {
+      const UnevenGroup& g = u->hgroups[i];
+      if (pi >= g.npasses) continue;
+      for (int b = 0; b < g.B; ++b)
+        for (int ch = 0; ch < g.nchunks; ++ch) items.push_back(make_int4(int(i), b, pi, ch));
+    }
+  u->nitems = int(items.size());
+  for (const UnevenGroup& g : u->hgroups) u->nsamples += g.B;
   for (const UnevenGroup& g : u->hgroups) {
     u->nbind += int64_t(g.nbinds) * g.B;
     u->nfuse += int64_t(g.nrecs) * g.B;
@@ -2449,8 +2492,8 @@ extern "C" int mb_uneven_create(const mb_circuit* circuits, const mb_state* stat
   if (!u->pgroups.empty()) {
     if ((rc = dev_alloc((void**)&u->d_groups, sizeof(UnevenGroup) * u->hgroups.size())) ||
         (rc = dev_alloc((void**)&u->d_passes, sizeof(UnevenPass) * std::max<size_t>(1, u->hpasses.size()))) ||
-        (rc = dev_alloc((void**)&u->d_items, sizeof(int2) * items.size())) ||
-        (rc = dev_alloc((void**)&u->d_next, sizeof(unsigned)))) {
+        (rc = dev_alloc((void**)&u->d_items, sizeof(int4) * items.size())) ||
+        (rc = dev_alloc((void**)&u->d_next, sizeof(unsigned) * (1 + size_t(u->nsamples))))) {
       uneven_release(u.get());
       return rc;
     }
@@ -2460,7 +2503,7 @@ extern "C" int mb_uneven_create(const mb_circuit* circuits, const mb_state* stat
     if (!u->hpasses.empty())
       MB_CHECK_CUDA(cudaMemcpyAsync(u->d_passes, u->hpasses.data(), sizeof(UnevenPass) * u->hpasses.size(),
                                     cudaMemcpyHostToDevice, st));
-    MB_CHECK_CUDA(cudaMemcpyAsync(u->d_items, items.data(), sizeof(int2) * items.size(), cudaMemcpyHostToDevice, st));
+    MB_CHECK_CUDA(cudaMemcpyAsync(u->d_items, items.data(), sizeof(int4) * items.size(), cudaMemcpyHostToDevice, st));
     MB_CHECK_CUDA(cudaStreamSynchronize(st));
   }
   *out = u.release();
@@ -2511,13 +2554,14 @@ extern "C" int mb_uneven_apply(mb_uneven u, int flags) {
       k_uneven_fuse<<<unsigned((u->nfuse + 127) / 128), 128, 0, st>>>(u->d_groups, ng, u->nfuse);
       MB_LAUNCHED();
     }
-    MB_CHECK_CUDA(cudaMemsetAsync(u->d_next, 0, sizeof(unsigned), st));
+    MB_CHECK_CUDA(cudaMemsetAsync(u->d_next, 0, sizeof(unsigned) * (1 + size_t(u->nsamples)), st));
     const size_t shm = (size_t(16) << kUnevenMaxTile) + (size_t(8) << kUnevenMaxTile) + 1024;
     const int grid = std::min(u->nitems, g_ctx.sm_count * 2);
     ProfScope ps("k_uneven", u->bytes, st, u->flops);
     auto launch = [&](auto kern) {
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm));
-      kern<<<grid, kUnevenThreads, shm, st>>>(u->d_groups, u->d_passes, u->d_items, u->nitems, u->d_next, zero ? 1 : 0);
+      kern<<<grid, kUnevenThreads, shm, st>>>(u->d_groups, u->d_passes, u->d_items, u->nitems, u->d_next,
+                                              u->d_next + 1, zero ? 1 : 0, g_ctx.flags + 2);
     };
     u->u2 ? launch(k_uneven<true>) : launch(k_uneven<false>);
     MB_LAUNCHED();
