@@ -1777,10 +1777,9 @@ static bool want_jit(int N) {
   return N >= lo;
 }
 
-// Defaults: sizes run by the specialised kernels use 2^11-amplitude tiles with 8 amplitudes per
-// thread and two CTAs per SM (the fastest point of a sweep over tile bits 10-12, register bits
-// 3-4 and 1-6 CTAs per SM on the 28-qubit U3 circuit); the interpreter kernels use 2^12 tiles
-// with 16 amplitudes per thread. mb_tuning_set / the autotuner override both per register size.
+// Defaults: sizes run by the specialised kernels use the shape below; the interpreter kernels
+// use 2^12 tiles with 16 amplitudes per thread. mb_tuning_set / the autotuner override both per
+// register size.
 static Tuning tuning_for(int N) {
   Tuning tu;
   if (want_jit(N) && jit_available()) {
