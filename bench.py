@@ -316,6 +316,7 @@ def batch_measure(steps=3, warmup=2, per_size=3, dm_samples=4):
         small_ms[persistent] = start.elapsed_time(end) / steps
         plan_small.close()
     persistent_info = plan.persistent_info()
+    choice = plan.choice
     # plain per-call path: stratified sample
     plain_s = {}
     for n in sorted(counts):
@@ -338,7 +339,7 @@ def batch_measure(steps=3, warmup=2, per_size=3, dm_samples=4):
             "density_ms_per_step": dm_ms / steps, "small_sizes_ms_per_step": small_ms[True],
             "small_sizes_per_size_launches_ms_per_step": small_ms[False],
             "persistent_launch": {"groups": persistent_info[0], "samples": persistent_info[2],
-                                  "groups_on_per_size_path": persistent_info[1]},
+                                  "groups_on_per_size_path": persistent_info[1], "plan_choice": choice},
             "evals_per_step": evals, "steps": steps, "warmup": warmup,
             "sizes": counts, "plan_build_s": prep_s,
             "autotuned": {str(k): list(v) for k, v in {**plan.tuned, **plan_dm.tuned}.items()},

@@ -230,6 +230,10 @@ MB_API int mb_tuning_get(int nbits, int* tile_bits, int* reg_bits);
  * into one matrix at bind time (2x2 on pure states; on density matrices both gate halves with
  * the channels after them as one 4x4), 0 applies every gate as its own micro-op. */
 MB_API int mb_tuning_set_fusion(int nbits, int fusion);
+/* Specialised (NVRTC-compiled) pass kernels per register size: 1 always, 0 never, -1 the default
+ * (sizes from 18 bits; MB_JIT_MIN_BITS moves the threshold). Prepared plans that replay many
+ * times use 1 for smaller sizes, where the compile cost is paid once. */
+MB_API int mb_tuning_set_specialised(int nbits, int mode);
 MB_API int mb_tuning_get_fusion(int nbits, int* fusion);
 /* Times the fused execution of c on s for each candidate (t, R, fusion width) and records the
  * fastest for s's register size; best_ms receives its time per apply. Sizes that run on

@@ -152,6 +152,7 @@ def load():
         "mb_tuning_get": ([ctypes.c_int, ip, ip], ctypes.c_int),
         "mb_tuning_set_fusion": ([ctypes.c_int, ctypes.c_int], ctypes.c_int),
         "mb_tuning_get_fusion": ([ctypes.c_int, ip], ctypes.c_int),
+        "mb_tuning_set_specialised": ([ctypes.c_int, ctypes.c_int], ctypes.c_int),
         "mb_autotune": ([vp, vp, dp, sz, ctypes.c_int, ip, ip, dp], ctypes.c_int),
         "mb_measure_fp64_peak": ([dp], ctypes.c_int),
         "mb_qubit_weights": ([vp, ctypes.c_int, dp], ctypes.c_int),

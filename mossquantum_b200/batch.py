@@ -13,6 +13,7 @@ sequence (reset, parameter binding, passes, expectations) is recorded once into 
 from __future__ import annotations
 
 import ctypes
+import time
 
 import numpy as np
 
@@ -27,7 +28,12 @@ class BatchPlan:
     """groups: {n: (template circuit for n qubits, samples B_n)}; observable_for(n) gives the
     observable evaluated on every sample of size n. kind: "pure" or "density"."""
 
-    def __init__(self, groups, observable_for, kind="pure", autotune=False, autotune_max_bits=24, persistent=True):
+    def __init__(self, groups, observable_for, kind="pure", autotune=False, autotune_max_bits=24,
+                 persistent="auto"):
+        """persistent: True runs the pure groups of 8..17 qubits in one persistent launch, False
+        runs every group with its own pass launches; "auto" captures both and keeps the faster
+        replay (the per-size form then uses the specialised kernels for those sizes too, whose
+        compile cost the plan pays once)."""
         self.kind = kind
         self.tuned = {}
         self.groups = []
@@ -62,7 +68,9 @@ class BatchPlan:
         # Eager warm-up with zero parameters: builds schedules, kernels and reduction plans.
         self._stage({g["n"]: np.zeros((g["B"], g["circuit"].nparameters())) for g in self.groups})
         self.uneven = None
-        if persistent and kind == "pure" and self.groups:
+        self.choice = None
+        small = [g["n"] for g in self.groups if 8 <= g["n"] <= 17] if kind == "pure" else []
+        if persistent and small:
             cs = (ctypes.c_void_p * len(self.groups))(*[g["compiled"].handle.value for g in self.groups])
             ss = (ctypes.c_void_p * len(self.groups))(*[g["state"].handle.value for g in self.groups])
             u = ctypes.c_void_p()
@@ -71,6 +79,53 @@ class BatchPlan:
         self._record_body()
         N.synchronize()
         self._capture()
+        if persistent == "auto" and self.uneven is not None:
+            self._choose(small)
+
+    def _replay_ms(self, reps=3):
+        N.check(N.lib().mb_graph_launch(self.graph), "mb_graph_launch")
+        N.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            N.check(N.lib().mb_graph_launch(self.graph), "mb_graph_launch")
+        N.synchronize()
+        return (time.perf_counter() - t0) * 1e3 / reps
+
+    def _choose(self, small):
+        """Times the persistent form against per-size launches of specialised kernels for the
+        same groups (both as captured graphs) and keeps the faster."""
+        from . import autotune as A
+        L = N.lib()
+        t_persistent = self._replay_ms()
+        graph_p, uneven_p = self.graph, self.uneven
+        saved = {n: (A.get(n), A.get_fusion(n)) for n in small}
+        self.graph, self.uneven = None, None
+        t_specialised = None
+        try:
+            for n in small:
+                N.check(L.mb_tuning_set_specialised(n, 1), "mb_tuning_set_specialised")
+                A.set(n, 10, 3)
+            self._record_body()
+            N.synchronize()
+            self._capture()
+            t_specialised = self._replay_ms()
+        except Exception:  # noqa: BLE001 - any failure keeps the persistent form
+            t_specialised = None
+        if t_specialised is not None and t_specialised < t_persistent:
+            L.mb_graph_free(graph_p)
+            L.mb_uneven_free(uneven_p)
+            chosen = "per-size specialised"
+        else:
+            if self.graph is not None:
+                L.mb_graph_free(self.graph)
+            for n in small:
+                L.mb_tuning_set_specialised(n, -1)
+                (t, r), f = saved[n]
+                A.set(n, t, r)
+                A.set_fusion(n, f)
+            self.graph, self.uneven = graph_p, uneven_p
+            chosen = "persistent"
+        self.choice = {"persistent_ms": t_persistent, "per_size_specialised_ms": t_specialised, "chosen": chosen}
 
     def _stage(self, thetas):
         for g in self.groups:

@@ -1769,9 +1769,17 @@ std::map<int, int> g_fusion;                   // register bits -> fusion width
 
 // Specialised kernels are used from MB_JIT_MIN_BITS register bits on (default 18); MB_JIT=0
 // disables them. Small states keep the interpreter kernels (no compile latency).
+std::mutex g_spec_mu;
+std::map<int, int> g_specialised;  // register bits -> 1 always / 0 never use the specialised kernels
+
 static bool want_jit(int N) {
   const char* e = getenv("MB_JIT");
   if (e && atoi(e) == 0) return false;
+  {
+    std::lock_guard<std::mutex> lk(g_spec_mu);
+    auto it = g_specialised.find(N);
+    if (it != g_specialised.end()) return it->second != 0;
+  }
   int lo = 18;
   if (const char* m = getenv("MB_JIT_MIN_BITS")) lo = atoi(m);
   return N >= lo;
@@ -2514,7 +2522,7 @@ extern "C" int mb_uneven_info(mb_uneven u, int* persistent_groups, int* fallback
   if (!u) return MB_EINVAL;
   if (persistent_groups) *persistent_groups = int(u->pgroups.size());
   if (fallback_groups) *fallback_groups = int(u->fallback.size());
-  if (samples) *samples = u->nitems;
+  if (samples) *samples = u->nsamples;
   return MB_OK;
 }
 
@@ -2618,6 +2626,14 @@ extern "C" int mb_tuning_set_fusion(int nbits, int fusion) {
   }
   std::lock_guard<std::mutex> lk(mb::g_tune_mu);
   mb::g_fusion[nbits] = fusion;
+  return MB_OK;
+}
+
+extern "C" int mb_tuning_set_specialised(int nbits, int mode) {
+  if (nbits < 1 || nbits > 40 || mode < -1 || mode > 1) return MB_EINVAL;
+  std::lock_guard<std::mutex> lk(mb::g_spec_mu);
+  if (mode < 0) mb::g_specialised.erase(nbits);
+  else mb::g_specialised[nbits] = mode;
   return MB_OK;
 }
 

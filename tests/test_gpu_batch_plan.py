@@ -67,7 +67,7 @@ def test_persistent_uneven_launch(mq, O):
     sizes = {6: 2, 8: 3, 11: 2, 14: 2, 17: 2, 18: 1}
     depth = 3
     groups = {n: (W.hea_circuit(n, depth), B) for n, B in sizes.items()}
-    plan = BatchPlan(groups, W.xxz)
+    plan = BatchPlan(groups, W.xxz, persistent=True)
     assert plan.persistent_info() == (4, 2, 9)
     rng = np.random.default_rng(17)
     thetas = {n: rng.uniform(0, 2 * np.pi, size=(B, groups[n][0].nparameters())) for n, B in sizes.items()}
@@ -93,3 +93,26 @@ def test_persistent_uneven_launch(mq, O):
     assert rep["k_uneven"][0] == 1, rep
     assert "k_tile_pass" not in rep, rep
     plan.close()
+
+
+def test_plan_keeps_the_faster_form(mq, O):
+    """The default plan captures the persistent form and per-size specialised launches, keeps
+    the faster replay, and either form gives the oracle's expectations."""
+    from mossquantum_b200 import workloads as W
+    from mossquantum_b200.batch import BatchPlan
+    sizes = {10: 3, 12: 2, 15: 2}
+    groups = {n: (W.hea_circuit(n, 2), B) for n, B in sizes.items()}
+    plan = BatchPlan(groups, W.xxz)
+    assert plan.choice is not None and plan.choice["chosen"] in ("persistent", "per-size specialised")
+    rng = np.random.default_rng(23)
+    thetas = {n: rng.uniform(0, 2 * np.pi, size=(B, groups[n][0].nparameters())) for n, B in sizes.items()}
+    res = plan.run(thetas)
+    for n, B in sizes.items():
+        for b in range(B):
+            c = groups[n][0].copy().reset_parameters(thetas[n][b])
+            ref = O.expect(O.apply(c.specs(), O.zero_state(n), n), n, W.xxz(n).specs())
+            assert abs(res[n][b] - ref) <= 1e-11
+    plan.close()
+    from mossquantum_b200 import _native as N
+    for n in sizes:
+        N.check(N.lib().mb_tuning_set_specialised(n, -1))
