@@ -459,11 +459,24 @@ def _case_setup(name, mq, W):
                 st.set_zero()
                 mq.apply_(c, st, theta=th)
         return f"uneven batch, pure part: {sum(counts.values())} states, sizes {min(counts)}..{max(counts)}", step
+    if name == "uneven":
+        # the uneven batch's sizes below 18 qubits in the persistent launch (k_uneven), run
+        # eagerly (binding and fused products of all sizes, then the one pass launch)
+        from mossquantum_b200.batch import BatchPlan
+        rng2 = W.rng_for(2)
+        sizes = rng2.integers(10, 23, size=512)
+        counts = {int(n): int((sizes == n).sum()) for n in np.unique(sizes) if n < 18}
+        groups = {n: (W.hea_circuit(n, 8), B) for n, B in counts.items()}
+        plan = BatchPlan(groups, W.xxz, persistent=True)
+        th = {n: np.random.default_rng(n).uniform(0, 2 * np.pi, size=(B, c.nparameters()))
+              for n, (c, B) in groups.items()}
+        plan._stage(th)
+        return f"persistent uneven launch: {sum(counts.values())} states, sizes 10..17", plan._record_body
     raise ValueError(f"unknown kernel case {name}")
 
 
 KERNEL_CASES = ("dense1_low", "dense1_high", "tile", "density", "pauli", "adjoint", "grad24", "marginal", "dmma",
-                "dense5", "batch_pure", "batch_pure_small")
+                "dense5", "batch_pure", "batch_pure_small", "uneven")
 
 
 def kernel_workload(args):
