@@ -111,6 +111,13 @@ class BatchPlan:
             t_specialised = self._replay_ms()
         except Exception:  # noqa: BLE001 - any failure keeps the persistent form
             t_specialised = None
+        # The captured graph keeps the kernels it was recorded with, so the process-wide
+        # settings of these register sizes go back to what they were either way.
+        for n in small:
+            L.mb_tuning_set_specialised(n, -1)
+            (t, r), f = saved[n]
+            A.set(n, t, r)
+            A.set_fusion(n, f)
         if t_specialised is not None and t_specialised < t_persistent:
             L.mb_graph_free(graph_p)
             L.mb_uneven_free(uneven_p)
@@ -118,11 +125,6 @@ class BatchPlan:
         else:
             if self.graph is not None:
                 L.mb_graph_free(self.graph)
-            for n in small:
-                L.mb_tuning_set_specialised(n, -1)
-                (t, r), f = saved[n]
-                A.set(n, t, r)
-                A.set_fusion(n, f)
             self.graph, self.uneven = graph_p, uneven_p
             chosen = "persistent"
         self.choice = {"persistent_ms": t_persistent, "per_size_specialised_ms": t_specialised, "chosen": chosen}

@@ -102,8 +102,11 @@ def test_plan_keeps_the_faster_form(mq, O):
     from mossquantum_b200.batch import BatchPlan
     sizes = {10: 3, 12: 2, 15: 2}
     groups = {n: (W.hea_circuit(n, 2), B) for n, B in sizes.items()}
+    from mossquantum_b200 import autotune as A
+    before = {n: A.get(n) for n in sizes}
     plan = BatchPlan(groups, W.xxz)
     assert plan.choice is not None and plan.choice["chosen"] in ("persistent", "per-size specialised")
+    assert {n: A.get(n) for n in sizes} == before   # the choice leaves the process-wide tuning as it was
     rng = np.random.default_rng(23)
     thetas = {n: rng.uniform(0, 2 * np.pi, size=(B, groups[n][0].nparameters())) for n, B in sizes.items()}
     res = plan.run(thetas)
@@ -113,6 +116,3 @@ def test_plan_keeps_the_faster_form(mq, O):
             ref = O.expect(O.apply(c.specs(), O.zero_state(n), n), n, W.xxz(n).specs())
             assert abs(res[n][b] - ref) <= 1e-11
     plan.close()
-    from mossquantum_b200 import _native as N
-    for n in sizes:
-        N.check(N.lib().mb_tuning_set_specialised(n, -1))
