@@ -673,9 +673,8 @@ static void merge_phases(std::vector<FOp>& seq, bool dm, std::vector<double2>* x
       glob *= f.glob;
       continue;
     }
-    for (int q = 0; q < 64; ++q)
-      if ((f.nd >> q) & 1) flush(q);
-    out.push_back(f);
+    for (uint64_t m = f.nd; m; m &= m - 1) flush(__builtin_ctzll(m));
+    out.push_back(std::move(f));
   }
   for (int q = 0; q < 64; ++q) flush(q);
   if (!dm && glob != cd(1, 0)) {
@@ -960,14 +959,14 @@ static void build_fops(mb_circuit c, int n, int dm, bool dagger, std::vector<FOp
     if (!getenv("MB_NO_SPLIT")) {
       std::vector<FOp> split;
       split.reserve(seq.size() * 2);
-      for (const FOp& f : seq)
-        if (!split_fixed_1q(c, f, dm, &S->xtab, split)) split.push_back(f);
+      for (FOp& f : seq)
+        if (!split_fixed_1q(c, f, dm, &S->xtab, split)) split.push_back(std::move(f));
       merge_phases(split, dm, &S->xtab);
       seq.swap(split);
     }
   }
   if (dm && !getenv("MB_NO_CHAN")) chan_forms(c, seq, n, S ? &S->xtab : nullptr);
-  out = seq;
+  out.swap(seq);
 }
 
 // Reverse sweep of a pure-state circuit range: U' of every gate in reverse order, each active
@@ -1240,8 +1239,11 @@ static void plan_stages(const std::vector<FOp>& fops, const std::vector<int>& op
   for (int i = 0; i < t; ++i) loc[p.bits[i]] = i;
   auto lmask = [&](uint64_t gm) {
     uint64_t m = 0;
-    for (int g = 0; g < 64; ++g)
-      if ((gm >> g) & 1) m |= uint64_t(1) << loc[g];
+    while (gm) {
+      const int g = __builtin_ctzll(gm);
+      gm &= gm - 1;
+      if (loc[g] >= 0) m |= uint64_t(1) << loc[g];
+    }
     return m;
   };
   // Warp bits: a stage of 2^(t-R) threads has t-R-5 warp-index bits. Local bits >= 6 that the
@@ -1548,6 +1550,29 @@ static std::vector<int> window(int lo, int len, int N) {
   return w;
 }
 
+struct SchedChoice {
+  int kind;               // PassKind, or -1: no candidate held the first op
+  std::vector<int> bits;
+};
+
+// Tile choices of earlier schedules by op structure (bounded; a full map is cleared).
+static std::mutex g_sched_memo_mu;
+static std::map<std::vector<uint64_t>, std::vector<SchedChoice>> g_sched_memo;
+
+static bool sched_memo_find(const std::vector<uint64_t>& sig, std::vector<SchedChoice>* out) {
+  std::lock_guard<std::mutex> lk(g_sched_memo_mu);
+  auto it = g_sched_memo.find(sig);
+  if (it == g_sched_memo.end()) return false;
+  *out = it->second;
+  return true;
+}
+
+static void sched_memo_store(const std::vector<uint64_t>& sig, const std::vector<SchedChoice>& rec) {
+  std::lock_guard<std::mutex> lk(g_sched_memo_mu);
+  if (g_sched_memo.size() >= 256) g_sched_memo.clear();
+  g_sched_memo[sig] = rec;
+}
+
 static void build_schedule(Schedule& S, int nsamples, bool allow_reg = true) {
   const int N = S.N, t = std::min(S.t, N), R = S.R;
   const uint64_t full = N >= 64 ? ~uint64_t(0) : ((uint64_t(1) << N) - 1);
@@ -1557,6 +1582,22 @@ static void build_schedule(Schedule& S, int nsamples, bool allow_reg = true) {
   std::vector<int> rem(S.fops.size());
   for (size_t i = 0; i < rem.size(); ++i) rem[i] = int(i);
   S.passes.clear();
+  // The greedy choices depend only on the ops' masks, kinds and targets and on the shape, so
+  // a circuit of the same structure (a fresh host circuit with new angles) replays the tile
+  // choices of an earlier schedule instead of scoring candidates again.
+  std::vector<uint64_t> sig = {uint64_t(N), uint64_t(t), uint64_t(R), uint64_t(nsamples > 1), uint64_t(S.dm),
+                               uint64_t(S.adjoint), uint64_t(allow_reg), uint64_t(two_windows), S.fops.size()};
+  for (const FOp& f : S.fops) {
+    sig.push_back(uint64_t(uint32_t(f.type)) | (uint64_t(uint32_t(f.ntgt)) << 32));
+    sig.push_back(f.nd);
+    sig.push_back(f.all);
+    sig.push_back(uint64_t(uint32_t(f.tgt[0])) | (uint64_t(uint32_t(f.tgt[1])) << 32));
+  }
+  std::vector<SchedChoice> replay_v;
+  const bool have = sched_memo_find(sig, &replay_v);
+  const std::vector<SchedChoice>* replay = have ? &replay_v : nullptr;
+  std::vector<SchedChoice> record;
+  size_t ri = 0;
   while (!rem.empty()) {
     const FOp& f0 = S.fops[rem[0]];
     if (f0.type == F_UNFUSABLE) {
@@ -1568,106 +1609,123 @@ static void build_schedule(Schedule& S, int nsamples, bool allow_reg = true) {
       rem.erase(rem.begin());
       continue;
     }
-    std::vector<Cand> cands;
-    std::vector<SlimOp> slim;
-    cands.push_back({PASS_TILE, window(0, t, N)});
-    if (N > t) {
-      // first target bit not coverable by the low tile, in circuit order
-      int h0 = -1;
-      for (int idx : rem) {
-        const FOp& f = S.fops[idx];
-        for (int j = 0; j < f.ntgt && h0 < 0; ++j)
-          if (f.tgt[j] >= t) h0 = f.tgt[j];
-        if (h0 >= 0) break;
-      }
-      if (h0 >= 0) {
-        const int w = t - 3;
-        for (int lo : {std::min(h0, N - w), std::max(3, h0 - w + 1)}) {
-          lo = std::max(3, std::min(lo, N - w));
-          std::vector<int> b = {0, 1, 2};
-          for (int q : window(lo, w, N)) b.push_back(q);
-          cands.push_back({PASS_TILE, b});
-        }
-        const int rlo = std::max(5, std::min(h0, N - R));
-        if (allow_reg && N - 5 >= R) cands.push_back({PASS_REG, window(rlo, R, N)});
-        if (two_windows) {
-          // Bits 0..2 and two windows [a, a + w1), [b, b + w2) with w1 + w2 = t - 3: one pass
-          // can then continue a chain of gates at two places (the tail of one layer's light
-          // cone and the head of the next). Every single window of each width is scored with
-          // bits 0..2; the best six positions of width w1 are paired with the best six of
-          // width t - 3 - w1 (an exhaustive search over all pairs finds tiles of the same
-          // quality on the tested circuits at five times the cost).
-          if (slim.empty()) slim_ops(S.fops, rem, slim);
-          constexpr int kTop = 6;
-          std::vector<std::vector<std::pair<double, int>>> top(w + 1);
-          for (int ww = 2; ww <= w - 2; ++ww) {
-            std::vector<std::pair<double, int>> sc;
-            for (int a = 3; a + ww <= N; ++a) {
-              const uint64_t m = uint64_t(7) | (((uint64_t(1) << ww) - 1) << a);
-              sc.push_back({-score_mask(slim, m, full), a});
-            }
-            std::sort(sc.begin(), sc.end());
-            if (sc.size() > size_t(kTop)) sc.resize(kTop);
-            top[ww] = sc;
-          }
-          for (int w1 = 2; w1 <= w - 2; ++w1) {
-            const int w2 = w - w1;
-            if (w1 > w2) break;  // pairs (w1, w2) and (w2, w1) give the same tiles
-            for (const auto& pa : top[w1])
-              for (const auto& pb : top[w2]) {
-                int a = pa.second, la = w1, b = pb.second, lb = w2;
-                if (a > b) {
-                  std::swap(a, b);
-                  std::swap(la, lb);
-                }
-                if (b < a + la + 1) continue;  // overlapping or touching: not two windows
-                std::vector<int> bb = {0, 1, 2};
-                for (int q : window(a, la, N)) bb.push_back(q);
-                for (int q : window(b, lb, N)) bb.push_back(q);
-                cands.push_back({PASS_TILE, bb});
-              }
-          }
-        }
-        if (S.dm) {
-          // Paired windows for density matrices: row bits [a, a+w1) and the matching column
-          // bits [b, b+w2) (b = a + n), so a channel's supermatrix on (q, q+n) and both halves
-          // of a gate fit one tile even when n exceeds a single window.
-          const int nq = N / 2, w1 = (t - 3) / 2, w2 = t - 3 - w1, q0 = h0 % nq;
-          if (nq - w1 >= 3) {
-            for (int a : {q0, q0 - w1 / 2}) {
-              a = std::max(3, std::min(a, nq - w1));
-              int b = std::max(nq, std::min((q0 < 3 ? 0 : a) + nq, N - w2));
-              std::vector<int> bb = {0, 1, 2};
-              for (int q : window(a, w1, N)) bb.push_back(q);
-              for (int q : window(b, w2, N)) bb.push_back(q);
-              cands.push_back({PASS_TILE, bb});
-            }
-          }
-        }
-      }
-    }
-    double best = -1;
-    int bi = -1;
     std::vector<int> best_taken;
     TmaGeom bg{};
-    if (slim.empty()) slim_ops(S.fops, rem, slim);
-    for (size_t ci = 0; ci < cands.size(); ++ci) {
-      double sc = score_mask(slim, mask_of(cands[ci].bits), full);
-      if (cands[ci].kind == PASS_REG) sc *= 0.999;  // prefer the wider tile on ties
-      if (sc <= best) continue;
-      TmaGeom g{};
-      if (cands[ci].kind == PASS_TILE && !tile_geom(cands[ci].bits, N, nsamples, g)) continue;
-      best = sc;
-      bi = int(ci);
-      bg = g;
+    int ckind = -1;
+    std::vector<int> cbits;
+    if (replay && ri < replay->size()) {
+      const SchedChoice& ch = (*replay)[ri++];
+      ckind = ch.kind;
+      cbits = ch.bits;
+      if (ckind == PASS_TILE) tile_geom(cbits, N, nsamples, bg);
+      if (ckind >= 0) best_taken = take_ops(S.fops, rem, mask_of(cbits), full, nullptr);
+    } else {
+      replay = nullptr;
+      std::vector<Cand> cands;
+      std::vector<SlimOp> slim;
+      cands.push_back({PASS_TILE, window(0, t, N)});
+      if (N > t) {
+        // first target bit not coverable by the low tile, in circuit order
+        int h0 = -1;
+        for (int idx : rem) {
+          const FOp& f = S.fops[idx];
+          for (int j = 0; j < f.ntgt && h0 < 0; ++j)
+            if (f.tgt[j] >= t) h0 = f.tgt[j];
+          if (h0 >= 0) break;
+        }
+        if (h0 >= 0) {
+          const int w = t - 3;
+          for (int lo : {std::min(h0, N - w), std::max(3, h0 - w + 1)}) {
+            lo = std::max(3, std::min(lo, N - w));
+            std::vector<int> b = {0, 1, 2};
+            for (int q : window(lo, w, N)) b.push_back(q);
+            cands.push_back({PASS_TILE, b});
+          }
+          const int rlo = std::max(5, std::min(h0, N - R));
+          if (allow_reg && N - 5 >= R) cands.push_back({PASS_REG, window(rlo, R, N)});
+          if (two_windows) {
+            // Bits 0..2 and two windows [a, a + w1), [b, b + w2) with w1 + w2 = t - 3: one pass
+            // can then continue a chain of gates at two places (the tail of one layer's light
+            // cone and the head of the next). Every single window of each width is scored with
+            // bits 0..2; the best six positions of width w1 are paired with the best six of
+            // width t - 3 - w1 (an exhaustive search over all pairs finds tiles of the same
+            // quality on the tested circuits at five times the cost).
+            if (slim.empty()) slim_ops(S.fops, rem, slim);
+            constexpr int kTop = 6;
+            std::vector<std::vector<std::pair<double, int>>> top(w + 1);
+            for (int ww = 2; ww <= w - 2; ++ww) {
+              std::vector<std::pair<double, int>> sc;
+              for (int a = 3; a + ww <= N; ++a) {
+                const uint64_t m = uint64_t(7) | (((uint64_t(1) << ww) - 1) << a);
+                sc.push_back({-score_mask(slim, m, full), a});
+              }
+              std::sort(sc.begin(), sc.end());
+              if (sc.size() > size_t(kTop)) sc.resize(kTop);
+              top[ww] = sc;
+            }
+            for (int w1 = 2; w1 <= w - 2; ++w1) {
+              const int w2 = w - w1;
+              if (w1 > w2) break;  // pairs (w1, w2) and (w2, w1) give the same tiles
+              for (const auto& pa : top[w1])
+                for (const auto& pb : top[w2]) {
+                  int a = pa.second, la = w1, b = pb.second, lb = w2;
+                  if (a > b) {
+                    std::swap(a, b);
+                    std::swap(la, lb);
+                  }
+                  if (b < a + la + 1) continue;  // overlapping or touching: not two windows
+                  std::vector<int> bb = {0, 1, 2};
+                  for (int q : window(a, la, N)) bb.push_back(q);
+                  for (int q : window(b, lb, N)) bb.push_back(q);
+                  cands.push_back({PASS_TILE, bb});
+                }
+            }
+          }
+          if (S.dm) {
+            // Paired windows for density matrices: row bits [a, a+w1) and the matching column
+            // bits [b, b+w2) (b = a + n), so a channel's supermatrix on (q, q+n) and both halves
+            // of a gate fit one tile even when n exceeds a single window.
+            const int nq = N / 2, w1 = (t - 3) / 2, w2 = t - 3 - w1, q0 = h0 % nq;
+            if (nq - w1 >= 3) {
+              for (int a : {q0, q0 - w1 / 2}) {
+                a = std::max(3, std::min(a, nq - w1));
+                int b = std::max(nq, std::min((q0 < 3 ? 0 : a) + nq, N - w2));
+                std::vector<int> bb = {0, 1, 2};
+                for (int q : window(a, w1, N)) bb.push_back(q);
+                for (int q : window(b, w2, N)) bb.push_back(q);
+                cands.push_back({PASS_TILE, bb});
+              }
+            }
+          }
+        }
+      }
+      double best = -1;
+      int bi = -1;
+      if (slim.empty()) slim_ops(S.fops, rem, slim);
+      for (size_t ci = 0; ci < cands.size(); ++ci) {
+        double sc = score_mask(slim, mask_of(cands[ci].bits), full);
+        if (cands[ci].kind == PASS_REG) sc *= 0.999;  // prefer the wider tile on ties
+        if (sc <= best) continue;
+        TmaGeom g{};
+        if (cands[ci].kind == PASS_TILE && !tile_geom(cands[ci].bits, N, nsamples, g)) continue;
+        best = sc;
+        bi = int(ci);
+        bg = g;
+      }
+      if (bi >= 0) {
+        ckind = cands[bi].kind;
+        cbits = cands[bi].bits;
+        best_taken = take_ops(S.fops, rem, mask_of(cbits), full, nullptr);
+      }
+      record.push_back({ckind, cbits});
     }
-    if (bi >= 0) best_taken = take_ops(S.fops, rem, mask_of(cands[bi].bits), full, nullptr);
-    if (bi < 0 || best_taken.empty()) {
+    if (ckind < 0 || best_taken.empty()) {
       // No candidate holds the first op (its bits lie farther apart than any window): run it
       // by itself with the plain kernel, which always makes progress. The adjoint has no
       // plain form of its gradient ops, so its schedule is refused instead.
       if (S.adjoint) {
         S.unschedulable = true;
+        if (!have) sched_memo_store(sig, record);
         return;
       }
       Pass p;
@@ -1679,8 +1737,8 @@ static void build_schedule(Schedule& S, int nsamples, bool allow_reg = true) {
       continue;
     }
     Pass p;
-    p.kind = cands[bi].kind;
-    p.bits = cands[bi].bits;
+    p.kind = ckind;
+    p.bits = cbits;
     p.t = int(p.bits.size());
     p.geom = bg;
     if (p.kind == PASS_TILE) plan_stages(S.fops, best_taken, p, R, S.adjoint ? nullptr : &S.xtab);
@@ -1695,6 +1753,7 @@ static void build_schedule(Schedule& S, int nsamples, bool allow_reg = true) {
     }
     rem.swap(left);
   }
+  if (!have) sched_memo_store(sig, record);
 }
 
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
