@@ -150,7 +150,7 @@ class QCircuit(Instruction):
             extra = None
             base = getattr(it, "parent", it)
             if isinstance(it, Gate) and getattr(base, "family", "MATRIX") == "MATRIX":
-                extra = it.mat().tobytes()
+                extra = it._sig_bytes()
             if isinstance(it, QuantumMap):
                 extra = b"".join(k.tobytes() for k in it.kraus)
             if hasattr(it, "signature_data"):

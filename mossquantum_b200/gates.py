@@ -182,6 +182,10 @@ class Gate(Instruction):
         op.data = buf.ctypes.data
         return [op], 0
 
+    def _sig_bytes(self):
+        """Bytes of the matrix, for the compiled-circuit cache key."""
+        return self.mat().tobytes()
+
     def __repr__(self):
         return f"{type(self).__name__}{self.pos}"
 
@@ -256,6 +260,23 @@ class QuantumGate(Gate):
 
     def _spec_data(self):
         return self.data.copy()
+
+    def _sig_bytes(self):
+        return self.data.tobytes()
+
+    def _ops(self, next_slot: int, keep: list):
+        op = N.MbOp()
+        op.kind = N.MB_OP_GATE
+        op.nq = len(self.pos)
+        for j, p in enumerate(self.pos):
+            op.pos[j] = p - 1
+        op.family = N.FAMILIES["MATRIX"]
+        op.slot = -1
+        # column-major complex128 as interleaved doubles (a fresh buffer the op points into)
+        buf = np.ascontiguousarray(self.data.T).view(np.float64)
+        keep.append(buf)
+        op.data = buf.ctypes.data
+        return [op], 0
 
     def copy_instruction(self):
         return QuantumGate(self.pos, self.data)
