@@ -25,12 +25,18 @@
 namespace mb {
 
 typedef std::complex<double> cdd;
-constexpr int kPR = 5;                    // register bits per pass
-constexpr int kPLocal = 5 + kPR;          // local bits of a tile (lanes + registers)
-constexpr int kPTile = 1 << kPLocal;      // 1024 amplitudes, 16 KiB of shared memory
+constexpr int kPRMax = 7;                 // register bits per pass: 7 from 12 qubits, else 5
 constexpr int kPThreads = 256;
-constexpr int kPPerThread = kPTile / kPThreads;
 constexpr int kPMaxGroups = 128;          // groups per pass (per-tile constants in shared memory)
+constexpr int kPTableMin = 4;             // local strings of a group tabulated from this many on
+
+// Tile of a pass with NR register bits: the lane bits 0..4 and NR register bits, 2^(5+NR)
+// amplitudes in shared memory (64 KiB for NR = 7), tile / 256 amplitudes per thread.
+template <int NR> struct PShape {
+  static constexpr int local = 5 + NR;
+  static constexpr int tile = 1 << local;
+  static constexpr int per = tile / kPThreads;
+};
 
 struct PString {
   uint64_t z;
@@ -44,14 +50,15 @@ struct PGroup {
   int xl;       // flip mask as a local index (bits 0..4 lanes, 5..9 registers)
   int k0, nk;
   int v0, nv;
-  int tab;      // offset of the group's 1024-entry table, or -1
+  int tab;      // offset of the group's table (one entry per local index), or -1
   int herm;     // every string's coefficient without i^{#Y} is real (the group is Hermitian)
   int hb;       // highest set bit of xl (flip groups)
 };
 
 struct PPassArgs {
   int n;
-  int reg[kPR];
+  int nr;                 // register bits of the pass's tiles (5 or 7)
+  int reg[kPRMax];
   int g0, ngroups;
   const PGroup* groups;
   const PString* strings;
@@ -61,6 +68,7 @@ struct PPassArgs {
 
 struct PauliProgram {
   int n = -1;
+  int nr = 5;
   std::vector<PPassArgs> passes;
   PGroup* d_groups = nullptr;
   PString* d_strings = nullptr;
@@ -76,17 +84,19 @@ struct PauliData {
 namespace {
 
 // Global bits of local index l: lane bits as they are, register bit k at reg[k].
-__host__ __device__ __forceinline__ uint64_t local_bits(int l, const int* reg) {
+__host__ __device__ __forceinline__ uint64_t local_bits(int l, const int* reg, int nr) {
   uint64_t o = uint64_t(l & 31);
-  for (int k = 0; k < kPR; ++k)
+  for (int k = 0; k < nr; ++k)
     if ((l >> (5 + k)) & 1) o |= uint64_t(1) << reg[k];
   return o;
 }
 
 // Tile base: tile index T with zeros inserted at the lane bits and the register bits.
+template <int NR>
 __device__ __forceinline__ uint64_t tile_base(int64_t T, const int* reg) {
   uint64_t base = uint64_t(T) << 5;
-  for (int k = 0; k < kPR; ++k) {
+#pragma unroll
+  for (int k = 0; k < NR; ++k) {
     const int p = reg[k];
     base = ((base >> p) << (p + 1)) | (base & ((uint64_t(1) << p) - 1));
   }
@@ -94,21 +104,28 @@ __device__ __forceinline__ uint64_t tile_base(int64_t T, const int* reg) {
 }
 
 // Loads a tile into shared memory (each warp reads 32 consecutive amplitudes) and computes the
-// per-tile constants of the pass's groups (descriptors already in shared memory).
+// per-tile constants of the pass's groups (descriptors already in shared memory): one warp per
+// group, its lanes over the group's constant strings.
+template <int NR>
 __device__ __forceinline__ void stage_tile(const double2* __restrict__ vs, uint64_t base, const uint64_t* loc,
                                            const PPassArgs& a, const PGroup* gd, double2* tile, double2* kconst) {
 #pragma unroll
-  for (int k = 0; k < kPPerThread; ++k) tile[threadIdx.x + k * kPThreads] = vs[base | loc[k]];
-  for (int gi = threadIdx.x; gi < a.ngroups; gi += kPThreads) {
+  for (int k = 0; k < PShape<NR>::per; ++k) tile[threadIdx.x + k * kPThreads] = vs[base | loc[k]];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int gi = warp; gi < a.ngroups; gi += kPThreads / 32) {
     const int k0 = gd[gi].k0, nk = gd[gi].nk;
     double2 kc = cz();
-    for (int s = k0; s < k0 + nk; ++s) {
+    for (int s = k0 + lane; s < k0 + nk; s += 32) {
       const PString ps = a.strings[s];
       const bool odd = __popcll(base & ps.z) & 1;
       kc.x += odd ? -ps.c.x : ps.c.x;
       kc.y += odd ? -ps.c.y : ps.c.y;
     }
-    kconst[gi] = kc;
+    for (int o = 16; o > 0; o >>= 1) {
+      kc.x += __shfl_xor_sync(0xffffffffu, kc.x, o);
+      kc.y += __shfl_xor_sync(0xffffffffu, kc.y, o);
+    }
+    if (lane == 0) kconst[gi] = kc;
   }
 }
 
@@ -137,28 +154,31 @@ __device__ __forceinline__ void load_groups(const PPassArgs& a, PGroup* gd) {
 // tile), the thread's amplitudes the inner one. A Hermitian flip group sums over pairs
 // (j, j^x) only: conj(psi_j) f(j) psi_{j^x} + conj(psi_{j^x}) f(j^x) psi_j equals
 // 2 Re(conj(psi_j) f(j) psi_{j^x}) because f(j^x) = conj(f(j)), so half the amplitudes of the
-// tile (local bit hb clear) carry the group.
+// tile (local bit hb clear) carry the group. The tile is dynamic shared memory.
+template <int NR>
 __global__ void __launch_bounds__(kPThreads) k_pauli_pass(const double2* __restrict__ v, const PPassArgs a,
                                                          double2* partials, unsigned* counters, double2* out) {
-  __shared__ double2 tile[kPTile];
+  constexpr int PER = PShape<NR>::per;
+  extern __shared__ double2 pauli_tile[];
+  double2* tile = pauli_tile;
   __shared__ double2 kconst[kPMaxGroups];
   __shared__ PGroup gd[kPMaxGroups];
   __shared__ double2 wp[kPThreads / 32];
   __shared__ bool last;
   const int b = blockIdx.y, G = gridDim.x;
   const double2* vs = v + (int64_t(b) << a.n);
-  int reg[kPR];
+  int reg[NR];
 #pragma unroll
-  for (int k = 0; k < kPR; ++k) reg[k] = a.reg[k];
-  uint64_t loc[kPPerThread];
+  for (int k = 0; k < NR; ++k) reg[k] = a.reg[k];
+  uint64_t loc[PER];
 #pragma unroll
-  for (int k = 0; k < kPPerThread; ++k) loc[k] = local_bits(threadIdx.x + k * kPThreads, reg);
+  for (int k = 0; k < PER; ++k) loc[k] = local_bits(threadIdx.x + k * kPThreads, reg, NR);
   load_groups(a, gd);
   __syncthreads();
   double2 acc = cz();
   for (int64_t T = blockIdx.x; T < a.tiles_per_sample; T += G) {
-    const uint64_t base = tile_base(T, reg);
-    stage_tile(vs, base, loc, a, gd, tile, kconst);
+    const uint64_t base = tile_base<NR>(T, reg);
+    stage_tile<NR>(vs, base, loc, a, gd, tile, kconst);
     __syncthreads();
     for (int gi = 0; gi < a.ngroups; ++gi) {
       const PGroup g = gd[gi];
@@ -166,7 +186,7 @@ __global__ void __launch_bounds__(kPThreads) k_pauli_pass(const double2* __restr
       if (g.xl == 0) {
         // diagonal group: f(j) |psi_j|^2
 #pragma unroll
-        for (int k = 0; k < kPPerThread; ++k) {
+        for (int k = 0; k < PER; ++k) {
           const int l = threadIdx.x + k * kPThreads;
           const double2 amp = tile[l];
           const double2 f = group_factor(g, a, kc, l, base, loc[k]);
@@ -177,18 +197,18 @@ __global__ void __launch_bounds__(kPThreads) k_pauli_pass(const double2* __restr
       } else if (g.herm) {
         const int hb = g.hb;
 #pragma unroll
-        for (int k = 0; k < kPPerThread / 2; ++k) {
+        for (int k = 0; k < PER / 2; ++k) {
           const int m = threadIdx.x + k * kPThreads;
           const int l = ((m >> hb) << (hb + 1)) | (m & ((1 << hb) - 1));
           const double2 amp = tile[l], p = tile[l ^ g.xl];
-          const double2 f = group_factor(g, a, kc, l, base, g.nv ? local_bits(l, reg) : 0);
+          const double2 f = group_factor(g, a, kc, l, base, g.nv ? local_bits(l, reg, NR) : 0);
           // 2 Re(conj(amp) p f)
           const double cr = amp.x * p.x + amp.y * p.y, ci = amp.x * p.y - amp.y * p.x;
           acc.x = fma(2.0 * f.x, cr, fma(-2.0 * f.y, ci, acc.x));
         }
       } else {
 #pragma unroll
-        for (int k = 0; k < kPPerThread; ++k) {
+        for (int k = 0; k < PER; ++k) {
           const int l = threadIdx.x + k * kPThreads;
           const double2 amp = tile[l], p = tile[l ^ g.xl];
           const double2 f = group_factor(g, a, kc, l, base, loc[k]);
@@ -222,43 +242,52 @@ __global__ void __launch_bounds__(kPThreads) k_pauli_pass(const double2* __restr
 }
 
 // Seed variant: out (+)= scale * H psi, with (P psi)_j = i^{#Y} (-1)^{|(j^x)&z|} psi_{j^x}.
-// Same tiles; the first pass writes, later passes add the groups they hold.
+// Same tiles; the first pass writes, later passes add the groups they hold. The thread's
+// amplitudes are taken four at a time (four accumulators), each quarter over all groups.
+template <int NR>
 __global__ void __launch_bounds__(kPThreads) k_pauli_apply(const double2* __restrict__ v, double2* __restrict__ out,
                                                           const PPassArgs a, double scale, int first) {
-  __shared__ double2 tile[kPTile];
+  constexpr int PER = PShape<NR>::per;
+  constexpr int Q = PER < 4 ? PER : 4;
+  extern __shared__ double2 pauli_tile[];
+  double2* tile = pauli_tile;
   __shared__ double2 kconst[kPMaxGroups];
   __shared__ PGroup gd[kPMaxGroups];
   const int b = blockIdx.y, G = gridDim.x;
   const double2* vs = v + (int64_t(b) << a.n);
   double2* os = out + (int64_t(b) << a.n);
-  int reg[kPR];
+  int reg[NR];
 #pragma unroll
-  for (int k = 0; k < kPR; ++k) reg[k] = a.reg[k];
-  uint64_t loc[kPPerThread];
+  for (int k = 0; k < NR; ++k) reg[k] = a.reg[k];
+  uint64_t loc[PER];
 #pragma unroll
-  for (int k = 0; k < kPPerThread; ++k) loc[k] = local_bits(threadIdx.x + k * kPThreads, reg);
+  for (int k = 0; k < PER; ++k) loc[k] = local_bits(threadIdx.x + k * kPThreads, reg, NR);
   load_groups(a, gd);
   __syncthreads();
   for (int64_t T = blockIdx.x; T < a.tiles_per_sample; T += G) {
-    const uint64_t base = tile_base(T, reg);
-    stage_tile(vs, base, loc, a, gd, tile, kconst);
-    double2 r[kPPerThread];
-#pragma unroll
-    for (int k = 0; k < kPPerThread; ++k) r[k] = cz();
+    const uint64_t base = tile_base<NR>(T, reg);
+    stage_tile<NR>(vs, base, loc, a, gd, tile, kconst);
     __syncthreads();
-    for (int gi = 0; gi < a.ngroups; ++gi) {
-      const PGroup g = gd[gi];
-      const double2 kc = kconst[gi];
 #pragma unroll
-      for (int k = 0; k < kPPerThread; ++k) {
-        const int l = threadIdx.x + k * kPThreads;
-        r[k] = cfma(group_factor(g, a, kc, l, base, loc[k]), tile[l ^ g.xl], r[k]);
+    for (int k0 = 0; k0 < PER; k0 += Q) {
+      double2 r[Q];
+#pragma unroll
+      for (int k = 0; k < Q; ++k) r[k] = cz();
+      for (int gi = 0; gi < a.ngroups; ++gi) {
+        const PGroup g = gd[gi];
+        const double2 kc = kconst[gi];
+#pragma unroll
+        for (int k = 0; k < Q; ++k) {
+          const int l = threadIdx.x + (k0 + k) * kPThreads;
+          r[k] = cfma(group_factor(g, a, kc, l, base, loc[k0 + k]), tile[l ^ g.xl], r[k]);
+        }
       }
-    }
 #pragma unroll
-    for (int k = 0; k < kPPerThread; ++k) {
-      const double2 o = first ? cz() : os[base | loc[k]];
-      os[base | loc[k]] = make_double2(fma(scale, r[k].x, o.x), fma(scale, r[k].y, o.y));
+      for (int k = 0; k < Q; ++k) {
+        const uint64_t j = base | loc[k0 + k];
+        const double2 o = first ? cz() : os[j];
+        os[j] = make_double2(fma(scale, r[k].x, o.x), fma(scale, r[k].y, o.y));
+      }
     }
     __syncthreads();
   }
@@ -337,13 +366,15 @@ void pauli_free(mb_observable o) {
 }
 
 // Pass plan for an n-qubit state, or nullptr when the fused form does not apply (fewer than
-// 10 qubits, or a group flips more than kPR bits above the lane bits). Each pass takes the
-// groups whose flip bits fit its local bits; per group the strings are ordered constant,
-// straddling, tabulated, and the tabulated ones are summed here over the 1024 local indices.
+// 10 qubits, or a group flips more register bits than a tile holds: 7 from 12 qubits, else 5).
+// Each pass takes the groups whose flip bits fit its local bits; per group the strings are
+// ordered constant, per-amplitude, tabulated, and the tabulated ones (a group with at least
+// four strings inside the tile) are summed here over the tile's local indices.
 static int pauli_program(mb_observable o, int n, PauliProgram** out) {
   *out = nullptr;
   PauliData* pd = o->pauli;
-  if (!pd || n < kPLocal) return MB_OK;
+  if (!pd || n < 10) return MB_OK;
+  const int nr = n >= 12 ? 7 : 5, local = 5 + nr;
   for (PauliProgram* p : pd->programs)
     if (p->n == n) {
       *out = p;
@@ -352,7 +383,7 @@ static int pauli_program(mb_observable o, int n, PauliProgram** out) {
   std::vector<int> rem;
   for (size_t g = 0; g < pd->groups.size(); ++g) {
     const uint64_t hi = pd->groups[g].first & ~uint64_t(31);
-    if (__builtin_popcountll(hi) > kPR || (pd->groups[g].first >> n) != 0) return MB_OK;
+    if (__builtin_popcountll(hi) > nr || (pd->groups[g].first >> n) != 0) return MB_OK;
     const int s0 = pd->groups[g].second.first, ns = pd->groups[g].second.second;
     for (int s = s0; s < s0 + ns; ++s)
       if ((pd->strings[s].z >> n) != 0) return MB_OK;
@@ -360,6 +391,7 @@ static int pauli_program(mb_observable o, int n, PauliProgram** out) {
   }
   std::unique_ptr<PauliProgram> P(new PauliProgram());
   P->n = n;
+  P->nr = nr;
   std::vector<PGroup> hg;
   std::vector<PString> hs;
   std::vector<double2> ht;
@@ -367,11 +399,12 @@ static int pauli_program(mb_observable o, int n, PauliProgram** out) {
     uint64_t regm = 0;
     for (int g : rem) {
       const uint64_t hi = pd->groups[g].first & ~uint64_t(31);
-      if (__builtin_popcountll(regm | hi) <= kPR) regm |= hi;
+      if (__builtin_popcountll(regm | hi) <= nr) regm |= hi;
     }
-    for (int q = n - 1; q >= 5 && __builtin_popcountll(regm) < kPR; --q) regm |= uint64_t(1) << q;
+    for (int q = n - 1; q >= 5 && __builtin_popcountll(regm) < nr; --q) regm |= uint64_t(1) << q;
     PPassArgs pa{};
     pa.n = n;
+    pa.nr = nr;
     int k = 0;
     for (int q = 5; q < n; ++q)
       if ((regm >> q) & 1) pa.reg[k++] = q;
@@ -387,7 +420,7 @@ static int pauli_program(mb_observable o, int n, PauliProgram** out) {
       PGroup G{};
       G.x = x;
       G.xl = int(x & 31);
-      for (int r = 0; r < kPR; ++r)
+      for (int r = 0; r < nr; ++r)
         if ((x >> pa.reg[r]) & 1) G.xl |= 1 << (5 + r);
       const int s0 = pd->groups[g].second.first, ns = pd->groups[g].second.second;
       std::vector<PString> kc, st, tb;
@@ -401,6 +434,11 @@ static int pauli_program(mb_observable o, int n, PauliProgram** out) {
         const uint64_t zl = ps.z & localm, zh = ps.z & ~localm;
         (zl == 0 ? kc : (zh == 0 ? tb : st)).push_back(ps);
       }
+      // a table pays off for several strings inside the tile; fewer are evaluated per amplitude
+      if (int(tb.size()) < kPTableMin) {
+        st.insert(st.end(), tb.begin(), tb.end());
+        tb.clear();
+      }
       G.k0 = int(hs.size());
       G.nk = int(kc.size());
       hs.insert(hs.end(), kc.begin(), kc.end());
@@ -411,8 +449,8 @@ static int pauli_program(mb_observable o, int n, PauliProgram** out) {
       if (!tb.empty()) {
         // sum over the strings inside the local bits, for every local index l
         G.tab = int(ht.size());
-        for (int l = 0; l < kPTile; ++l) {
-          const uint64_t k_idx = local_bits(l, pa.reg) ^ x;
+        for (int l = 0; l < (1 << local); ++l) {
+          const uint64_t k_idx = local_bits(l, pa.reg, nr) ^ x;
           double2 f = cz();
           for (const PString& ps : tb) {
             const bool odd = __builtin_popcountll(k_idx & ps.z) & 1;
@@ -425,7 +463,7 @@ static int pauli_program(mb_observable o, int n, PauliProgram** out) {
       hg.push_back(G);
     }
     pa.ngroups = int(hg.size()) - pa.g0;
-    pa.tiles_per_sample = int64_t(1) << (n - kPLocal);
+    pa.tiles_per_sample = int64_t(1) << (n - local);
     P->passes.push_back(pa);
     rem.swap(left);
     if (pd->groups.empty()) break;
@@ -468,7 +506,7 @@ int expect_pauli(mb_observable o, mb_state s, double2* out) {
   if (g_ctx.capturing) {
     for (PauliProgram* q : o->pauli->programs)
       if (q->n == s->n) P = q;
-    if (!P && s->n >= kPLocal) {
+    if (!P && s->n >= 10) {
       set_error("record the expectation once before capturing it (its pass plan is built lazily)");
       return MB_EUNSUPPORTED;
     }
@@ -489,7 +527,12 @@ int expect_pauli(mb_observable o, mb_state s, double2* out) {
       return MB_EUNSUPPORTED;
     }
     ProfScope ps("k_pauli_pass", 16.0 * double(s->elems) * s->batch, st);
-    k_pauli_pass<<<dim3(G, s->batch), kPThreads, 0, st>>>(s->d, pa, g_ctx.partials, g_ctx.counters, out);
+    const size_t shm = size_t(16) << (5 + pa.nr);
+    auto launch = [&](auto kern) {
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm));
+      kern<<<dim3(G, s->batch), kPThreads, shm, st>>>(s->d, pa, g_ctx.partials, g_ctx.counters, out);
+    };
+    pa.nr == 7 ? launch(k_pauli_pass<7>) : launch(k_pauli_pass<5>);
     MB_LAUNCHED();
   }
   return MB_OK;
@@ -508,7 +551,12 @@ int pauli_apply(mb_observable o, const double2* in, double2* out, int n, int nsa
     if (pa.ngroups == 0) continue;
     const int G = int(std::min<int64_t>(pa.tiles_per_sample, int64_t(g_ctx.sm_count) * 16));
     ProfScope ps("k_pauli_apply", (first ? 32.0 : 48.0) * double(int64_t(1) << n) * nsamples, st);
-    k_pauli_apply<<<dim3(G, nsamples), kPThreads, 0, st>>>(in, out, pa, scale, first ? 1 : 0);
+    const size_t shm = size_t(16) << (5 + pa.nr);
+    auto launch = [&](auto kern) {
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm));
+      kern<<<dim3(G, nsamples), kPThreads, shm, st>>>(in, out, pa, scale, first ? 1 : 0);
+    };
+    pa.nr == 7 ? launch(k_pauli_apply<7>) : launch(k_pauli_apply<5>);
     MB_LAUNCHED();
     first = false;
   }
