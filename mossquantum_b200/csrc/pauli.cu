@@ -25,7 +25,7 @@
 namespace mb {
 
 typedef std::complex<double> cdd;
-constexpr int kPRMax = 7;                 // register bits per pass: 7 from 12 qubits, else 5
+constexpr int kPRMax = 7;                 // register bits per pass: 7 from 20 qubits, else 5
 constexpr int kPThreads = 256;
 constexpr int kPMaxGroups = 128;          // groups per pass (per-tile constants in shared memory)
 constexpr int kPTableMin = 4;             // local strings of a group tabulated from this many on
@@ -366,7 +366,7 @@ void pauli_free(mb_observable o) {
 }
 
 // Pass plan for an n-qubit state, or nullptr when the fused form does not apply (fewer than
-// 10 qubits, or a group flips more register bits than a tile holds: 7 from 12 qubits, else 5).
+// 10 qubits, or a group flips more register bits than a tile holds: 7 from 20 qubits, else 5).
 // Each pass takes the groups whose flip bits fit its local bits; per group the strings are
 // ordered constant, per-amplitude, tabulated, and the tabulated ones (a group with at least
 // four strings inside the tile) are summed here over the tile's local indices.
@@ -374,7 +374,7 @@ static int pauli_program(mb_observable o, int n, PauliProgram** out) {
   *out = nullptr;
   PauliData* pd = o->pauli;
   if (!pd || n < 10) return MB_OK;
-  const int nr = n >= 12 ? 7 : 5, local = 5 + nr;
+  const int nr = n >= 20 ? 7 : 5, local = 5 + nr;  // large tiles pay off once a pass is long
   for (PauliProgram* p : pd->programs)
     if (p->n == n) {
       *out = p;
