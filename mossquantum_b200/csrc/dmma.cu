@@ -12,9 +12,10 @@
 // consecutive e are 32 consecutive amplitudes (512 contiguous bytes) for any target set.
 // Only the FP64 tensor pipe does arithmetic: 8 * 2^k flop per amplitude.
 // Shared-memory layout of X (and Y): row r of 2D rows, column g of 64, at
-// r * 72 + (g ^ ((r >> 2) & 7)). The stride (8 mod 16 doubles) spreads the four rows of a
-// B fragment over both bank halves; the XOR, constant within each fragment's rows, spreads a
-// staging access whose 32 lanes hold 32 rows of one column over all banks.
+// r * 68 + (g ^ ((r >> 2) & 7)). A half-warp's 64-bit accesses are conflict-free when their 16
+// word addresses differ mod 16: the stride (4 mod 16 doubles) puts the four rows of a B
+// fragment at offsets 0, 4, 8, 12 beside its four consecutive columns; the XOR, constant within
+// each fragment's rows, keeps a staging access whose lanes hold 16 rows of one column distinct.
 #include <algorithm>
 
 #include "kernels.h"
@@ -43,7 +44,7 @@ __device__ __forceinline__ void dmma_m8n8k4(double& d0, double& d1, double a, do
                : "d"(a), "d"(b));
 }
 
-constexpr int kXS = kGT + 8;
+constexpr int kXS = kGT + 4;
 __device__ __forceinline__ int xsw(int r, int g) { return r * kXS + (g ^ ((r >> 2) & 7)); }
 
 template <int K>
@@ -139,7 +140,7 @@ __global__ void __launch_bounds__(kDThreads) k_dmma_block(double2* __restrict__ 
 
 template <int K>
 constexpr size_t dmma_smem() {
-  return sizeof(double) * size_t(2 * (1 << K)) * size_t((2 * (1 << K) + 4) + (kGT + 8));
+  return sizeof(double) * size_t(2 * (1 << K)) * size_t((2 * (1 << K) + 4) + kXS);
 }
 
 }  // namespace
