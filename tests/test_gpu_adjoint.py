@@ -188,3 +188,32 @@ def test_fused_adjoint_shared_parameters(mq, O):
     vr, gr = O.adjoint(cb.specs(), O.zero_state(n), n, W.tfim(n).specs())
     assert abs(v - vr) <= 1e-11
     assert np.max(np.abs(g - mq.accumulate_parameter_gradients(pm, gr))) <= 1e-10
+
+
+def test_density_channel_kinds_forward_and_gradient(mq, O):
+    """Every single-qubit channel family after the gates of a 6-qubit density matrix: the ones
+    with the real population/coherence pattern run as channel micro-ops (forward, and inverted
+    or adjoined in the fused reverse), bit flips keep the dense 4x4. State and gradient against
+    the oracle."""
+    from mossquantum_b200 import workloads as W
+    n, depth = 6, 2
+    c0 = W.hea_circuit(n, depth, W.hea_angles(n, depth, W.rng_for(6, n)))
+    chans = [lambda q: mq.Depolarizing(q, 0.03), lambda q: mq.AmplitudeDamping(q, 0.05),
+             lambda q: mq.PhaseDamping(q, 0.04), lambda q: mq.PhaseFlip(q, 0.02),
+             lambda q: mq.GeneralizedAmplitudeDamping(q, 0.05, 0.2), lambda q: mq.ResetChannel(q, 0, 0.1),
+             lambda q: mq.ThermalRelaxation(q, 50.0, 40.0, 1.0), lambda q: mq.BitFlip(q, 0.02),
+             lambda q: mq.BitPhaseFlip(q, 0.01)]
+    c = mq.QCircuit()
+    for i, g in enumerate(c0.flat()):
+        c.push(g)
+        for q in g.positions:
+            c.push(chans[(i + q) % len(chans)](q))
+    s = mq.apply_(c, mq.DensityMatrix(n))
+    rho = O.apply(c.specs(), O.zero_state(n, True), n, True)
+    assert np.max(np.abs(s.to_numpy().ravel(order="F") - rho)) <= 1e-12
+    H = W.tfim(n)
+    obj = mq.ExpectationObjective(c, H, mq.DensityMatrix(n))
+    theta = np.array(c.active_parameters())
+    v, g = mq.value_and_gradient(mq.AdjointGradient(), obj, theta)
+    vr, gr = O.adjoint(c.specs(), O.zero_state(n, True), n, H.specs(), dm=True)
+    assert abs(v - vr) <= 1e-11 and np.max(np.abs(g - gr)) <= 1e-10

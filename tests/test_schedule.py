@@ -190,3 +190,25 @@ def test_two_window_tiles_cut_passes():
     assert npasses <= 12, npasses
     ea, eb = lowering_errors(c, n, t=9, R=3)
     assert ea <= 1e-12 and eb <= 1e-12, (ea, eb)
+
+
+# Channels whose supermatrix is real with the population/coherence pattern (depolarizing,
+# amplitude and phase damping, phase flip, generalized amplitude damping, reset, thermal
+# relaxation) lower to the channel micro-op; bit flips and mixed unitaries keep the dense 4x4.
+# Both kinds, fused and unfused, must lower exactly.
+def test_lowering_channel_forms():
+    n = 5
+    c = W.u3_brickwork(n, 2, W.u3_params(n, 2, W.rng_for(1, 7)))
+    noisy = mq.QCircuit()
+    chans = [lambda q: mq.Depolarizing(q, 0.03), lambda q: mq.AmplitudeDamping(q, 0.05),
+             lambda q: mq.PhaseDamping(q, 0.04), lambda q: mq.PhaseFlip(q, 0.02),
+             lambda q: mq.GeneralizedAmplitudeDamping(q, 0.05, 0.2), lambda q: mq.ResetChannel(q, 0, 0.1),
+             lambda q: mq.ThermalRelaxation(q, 50.0, 40.0, 1.0), lambda q: mq.BitFlip(q, 0.02),
+             lambda q: mq.BitPhaseFlip(q, 0.01)]
+    for i, g in enumerate(c.flat()):
+        noisy.push(g)
+        for q in g.positions:
+            noisy.push(chans[(i + q) % len(chans)](q))
+    for t_bits, R in ((8, 3), (10, 4)):
+        ea, eb = lowering_errors(noisy, n, dm=True, t=t_bits, R=R)
+        assert ea <= 1e-12 and eb <= 1e-12, (ea, eb)
