@@ -15,6 +15,7 @@
 // passes instead of 2n-1 key passes.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <complex>
 #include <map>
 #include <memory>
@@ -374,7 +375,11 @@ static int pauli_program(mb_observable o, int n, PauliProgram** out) {
   *out = nullptr;
   PauliData* pd = o->pauli;
   if (!pd || n < 10) return MB_OK;
-  const int nr = n >= 20 ? 7 : 5, local = 5 + nr;  // large tiles pay off once a pass is long
+  // large tiles from MB_PAULI_WIDE_BITS qubits (default 20); tables for groups with at least
+  // MB_PAULI_TABLE_MIN strings inside the tile (default 4)
+  static const int wide_from = getenv("MB_PAULI_WIDE_BITS") ? atoi(getenv("MB_PAULI_WIDE_BITS")) : 20;
+  static const int table_min = getenv("MB_PAULI_TABLE_MIN") ? atoi(getenv("MB_PAULI_TABLE_MIN")) : kPTableMin;
+  const int nr = n >= wide_from && n >= 12 ? 7 : 5, local = 5 + nr;
   for (PauliProgram* p : pd->programs)
     if (p->n == n) {
       *out = p;
@@ -435,7 +440,7 @@ static int pauli_program(mb_observable o, int n, PauliProgram** out) {
         (zl == 0 ? kc : (zh == 0 ? tb : st)).push_back(ps);
       }
       // a table pays off for several strings inside the tile; fewer are evaluated per amplitude
-      if (int(tb.size()) < kPTableMin) {
+      if (int(tb.size()) < table_min) {
         st.insert(st.end(), tb.begin(), tb.end());
         tb.clear();
       }
