@@ -237,8 +237,8 @@ MB_API int mb_tuning_set_specialised(int nbits, int mode);
 MB_API int mb_tuning_get_fusion(int nbits, int* fusion);
 /* Times the fused execution of c on s for each candidate (t, R, fusion width) and records the
  * fastest for s's register size; best_ms receives its time per apply. Sizes that run on
- * specialised kernels try the current (t, R) with and without fusion, so tuning them costs one
- * extra set of kernel compilations. */
+ * specialised kernels try 2^10- and 2^11-amplitude tiles with 8 amplitudes per thread and
+ * fusion, then the faster of the two without fusion: three sets of kernel compilations. */
 MB_API int mb_autotune(mb_circuit c, mb_state s, const double* theta, size_t ntheta, int flags, int* best_t,
                        int* best_r, double* best_ms);
 

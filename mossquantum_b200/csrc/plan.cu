@@ -133,8 +133,13 @@ extern "C" int mb_autotune(mb_circuit c, mb_state s, const double* theta, size_t
   mb_tuning_get(N, &t0, &r0);
   mb_tuning_get_fusion(N, &f0);
   std::vector<std::array<int, 3>> cand;
-  if (jit_sizes(N)) {
-    for (int f : {1, 0}) cand.push_back({t0, r0, f});
+  const bool jit = jit_sizes(N);
+  if (jit) {
+    // specialised kernels: tiles of 2^10 and 2^11 amplitudes with bind-time fusion, then the
+    // better of the two without fusion (each candidate compiles its own kernels)
+    cand.push_back({10, 3, 1});
+    cand.push_back({11, 3, 1});
+    if (!((t0 == 10 || t0 == 11) && r0 == 3)) cand.push_back({t0, r0, 1});
   } else {
     for (int f : {1, 0})
       for (auto tr : {std::array<int, 2>{12, 4}, {11, 4}, {10, 4}, {12, 3}, {11, 3}, {10, 3}}) cand.push_back({tr[0], tr[1], f});
@@ -145,18 +150,19 @@ extern "C" int mb_autotune(mb_circuit c, mb_state s, const double* theta, size_t
   MB_CHECK_CUDA(cudaEventCreate(&a));
   MB_CHECK_CUDA(cudaEventCreate(&b));
   int rc = MB_OK;
-  for (auto& cd : cand) {
-    if (cd[0] > N) continue;
-    if ((rc = mb_tuning_set(N, cd[0], cd[1]))) break;
-    if ((rc = mb_tuning_set_fusion(N, cd[2]))) break;
-    // warm-up builds the schedule and its kernels; then two timed applies
+  // times one candidate (a warm-up apply builds its schedule and kernels, then two timed
+  // applies); false on an error that ends the search
+  auto run = [&](const std::array<int, 3>& cd) -> bool {
+    if (cd[0] > N) return true;
+    if ((rc = mb_tuning_set(N, cd[0], cd[1]))) return false;
+    if ((rc = mb_tuning_set_fusion(N, cd[2]))) return false;
     if ((rc = mb_apply(c, s, theta, ntheta, flags & ~MB_APPLY_PLAIN))) {
       rc = MB_OK;  // a width this circuit cannot use (e.g. no specialised kernels): skip it
-      continue;
+      return true;
     }
     int et = 0, er = 0;
     mb_tuning_get(N, &et, &er);
-    if (et != cd[0] || er != cd[1]) continue;  // the library fell back to another width: not this candidate
+    if (et != cd[0] || er != cd[1]) return true;  // the library fell back to another width
     cudaEventRecord(a, g_ctx.stream);
     for (int k = 0; k < 2 && !rc; ++k) rc = mb_apply(c, s, theta, ntheta, flags & ~MB_APPLY_PLAIN);
     cudaEventRecord(b, g_ctx.stream);
@@ -169,8 +175,13 @@ extern "C" int mb_autotune(mb_circuit c, mb_state s, const double* theta, size_t
       br = cd[1];
       bf = cd[2];
     }
-    if (rc) break;
-  }
+    return rc == MB_OK;
+  };
+  bool ok = true;
+  for (const auto& cd : cand)
+    if (!(ok = run(cd))) break;
+  // specialised sizes: the better fused shape once more without fusion
+  if (ok && jit && best < 1e300) run({bt, br, 0});
   cudaEventDestroy(a);
   cudaEventDestroy(b);
   mb_tuning_set(N, bt, br);
