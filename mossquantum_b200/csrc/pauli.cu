@@ -26,10 +26,10 @@
 namespace mb {
 
 typedef std::complex<double> cdd;
-constexpr int kPRMax = 7;                 // register bits per pass: 7 from 20 qubits, else 5
+constexpr int kPRMax = 7;                 // register bits per pass: 7 from 24 qubits, else 5
 constexpr int kPThreads = 256;
 constexpr int kPMaxGroups = 128;          // groups per pass (per-tile constants in shared memory)
-constexpr int kPTableMin = 4;             // local strings of a group tabulated from this many on
+constexpr int kPTableMin = 1;             // local strings of a group tabulated from this many on
 
 // Tile of a pass with NR register bits: the lane bits 0..4 and NR register bits, 2^(5+NR)
 // amplitudes in shared memory (64 KiB for NR = 7), tile / 256 amplitudes per thread.
@@ -367,17 +367,19 @@ void pauli_free(mb_observable o) {
 }
 
 // Pass plan for an n-qubit state, or nullptr when the fused form does not apply (fewer than
-// 10 qubits, or a group flips more register bits than a tile holds: 7 from 20 qubits, else 5).
+// 10 qubits, or a group flips more register bits than a tile holds: 7 from 24 qubits, else 5).
 // Each pass takes the groups whose flip bits fit its local bits; per group the strings are
-// ordered constant, per-amplitude, tabulated, and the tabulated ones (a group with at least
-// four strings inside the tile) are summed here over the tile's local indices.
+// ordered constant, per-amplitude, tabulated, and the tabulated ones (strings inside the
+// tile) are summed here over the tile's local indices.
 static int pauli_program(mb_observable o, int n, PauliProgram** out) {
   *out = nullptr;
   PauliData* pd = o->pauli;
   if (!pd || n < 10) return MB_OK;
-  // large tiles from MB_PAULI_WIDE_BITS qubits (default 20); tables for groups with at least
-  // MB_PAULI_TABLE_MIN strings inside the tile (default 4)
-  static const int wide_from = getenv("MB_PAULI_WIDE_BITS") ? atoi(getenv("MB_PAULI_WIDE_BITS")) : 20;
+  // large tiles from MB_PAULI_WIDE_BITS qubits (default 24: fewer passes pay off for long
+  // passes; at 20-22 qubits the smaller tiles measured faster on XXZ batches); tables for groups
+  // with at least MB_PAULI_TABLE_MIN strings inside the tile (default 1: a table lookup is
+  // cheaper than one per-amplitude parity)
+  static const int wide_from = getenv("MB_PAULI_WIDE_BITS") ? atoi(getenv("MB_PAULI_WIDE_BITS")) : 24;
   static const int table_min = getenv("MB_PAULI_TABLE_MIN") ? atoi(getenv("MB_PAULI_TABLE_MIN")) : kPTableMin;
   const int nr = n >= wide_from && n >= 12 ? 7 : 5, local = 5 + nr;
   for (PauliProgram* p : pd->programs)
@@ -439,7 +441,7 @@ static int pauli_program(mb_observable o, int n, PauliProgram** out) {
         const uint64_t zl = ps.z & localm, zh = ps.z & ~localm;
         (zl == 0 ? kc : (zh == 0 ? tb : st)).push_back(ps);
       }
-      // a table pays off for several strings inside the tile; fewer are evaluated per amplitude
+      // strings inside the tile go to the table unless there are fewer than table_min
       if (int(tb.size()) < table_min) {
         st.insert(st.end(), tb.begin(), tb.end());
         tb.clear();
