@@ -124,6 +124,10 @@ __device__ __forceinline__ double2 cfma(double2 a, double2 b, double2 c) {
 __device__ __forceinline__ double2 ld(const double2* p) { return __ldg(p); }
 __device__ __forceinline__ double2 ldc(const double2* p) { double2 x = __ldg(p); return make_double2(x.x, -x.y); }
 __device__ __forceinline__ double2 neg(double2 a) { return make_double2(-a.x, -a.y); }
+__device__ __forceinline__ double2 cneg(double2 a, u64 s) {
+  return make_double2(__longlong_as_double(__double_as_longlong(a.x) ^ (long long)s),
+                      __longlong_as_double(__double_as_longlong(a.y) ^ (long long)s));
+}
 __device__ __forceinline__ double2 cj(double2 a) { return make_double2(a.x, -a.y); }
 __device__ __forceinline__ u32 swz(u32 i) { return i ^ ((i >> 3) & 7u); }
 __device__ __forceinline__ u32 sa(const void* p) { return (u32)__cvta_generic_to_shared(p); }
@@ -321,6 +325,15 @@ struct StageGen {
         int need;
         std::string cond;
         split(m, need, cond);
+        if (m.r1 && !cond.empty()) {
+          // a sign flip under a thread or tile condition: flip the sign bits without a branch
+          // (no divergence inside a warp, one basic block for the scheduler)
+          o << "{ const u64 sg = (u64)(" << cond << ") << 63;\n";
+          for (int j = 0; j < A; ++j)
+            if ((j & need) == need) o << "  " << v(j) << " = cneg(" << v(j) << ", sg);\n";
+          o << "}\n";
+          break;
+        }
         o << "{ ";
         if (!m.r1) o << "const double2 f = " << ldm(m, 0) << "; ";
         if (!cond.empty()) o << "if (" << cond << ") {";
