@@ -192,12 +192,37 @@ class Gate(Instruction):
 
 class _FixedGate(Gate):
     matrix = None
+    _packed = None  # per class: the matrix as column-major interleaved doubles (read-only)
 
     def __init__(self, *positions):
         super().__init__(positions[0] if len(positions) == 1 and not isinstance(positions[0], int) else positions)
 
     def mat(self):
         return np.array(self.matrix, dtype=complex)
+
+    @classmethod
+    def _packed_matrix(cls):
+        if cls.__dict__.get("_packed") is None:
+            buf = np.ascontiguousarray(np.array(cls.matrix, dtype=complex).T).view(np.float64)
+            buf.flags.writeable = False
+            cls._packed = buf
+        return cls._packed
+
+    def _sig_bytes(self):
+        return self._packed_matrix().tobytes()
+
+    def _ops(self, next_slot: int, keep: list):
+        op = N.MbOp()
+        op.kind = N.MB_OP_GATE
+        op.nq = len(self.pos)
+        for j, p in enumerate(self.pos):
+            op.pos[j] = p - 1
+        op.family = N.FAMILIES["MATRIX"]
+        op.slot = -1
+        buf = self._packed_matrix()  # shared by every gate of the class; the library copies it
+        keep.append(buf)
+        op.data = buf.ctypes.data
+        return [op], 0
 
     def copy_instruction(self):
         return type(self)(*self.pos)
