@@ -195,6 +195,7 @@ __global__ void k_fuse(const FuseRec* __restrict__ recs, int nrecs, const FuseCo
 // kernel reads the tables through the read-only cache, so they are written before it starts).
 constexpr int kUnevenThreads = 128;
 constexpr int kUnevenMaxTile = 11;   // 2^11-amplitude tiles, 16 amplitudes per thread
+constexpr int kUnevenJitTile = 10;   // specialised form (mbk_uneven): 2^10 tiles, 8 per thread
 
 struct UnevenGroup {
   int n;                      // amplitude bits of one sample
@@ -2011,10 +2012,11 @@ static int get_schedule_impl(mb_circuit c, int n, int dm, int adjoint, int lo, i
                                   cudaMemcpyHostToDevice, g_ctx.stream));
   }
   MB_CHECK_CUDA(cudaStreamSynchronize(g_ctx.stream));
-  if (!adjoint && S->R == 3 && !getenv("MB_REG_BITS")) {
+  if (!adjoint && !tile_only && S->R == 3 && !getenv("MB_REG_BITS")) {
     // Register width 3 exists only as specialised kernels: if they cannot all be built (source
     // limits, compile budget), use width 4 for this register size from now on. (A width forced
-    // through MB_REG_BITS is kept; run_schedule then reports the missing kernels.)
+    // through MB_REG_BITS is kept; run_schedule then reports the missing kernels. Tile-only
+    // schedules belong to the persistent uneven launch, which compiles its own kernel.)
     prepare_jit(S.get());
     if (S->jit != 1) {
       if (getenv("MB_JIT_VERBOSE")) fprintf(stderr, "mossb200: %d-bit schedules fall back to register width 4\n", N);
@@ -2415,14 +2417,26 @@ struct mb_uneven_s {
   unsigned* d_next = nullptr;           // work counter, then one completion counter per sample
   int nsamples = 0;
   int nitems = 0;
+  int chunk_bits = 15;                   // work items hold 2^chunk_bits amplitudes of a sample
   int64_t nbind = 0, nfuse = 0;
   bool u2 = false;
   double bytes = 0, flops = 0;           // algorithmic bytes and flops of one launch
+  // Specialised form (mbk_uneven): straight-line code per pass, register width 3; null when
+  // the interpreter form k_uneven runs.
+  void* jit_fn = nullptr;
+  int jthreads = 0, jctas = 0;
+  size_t jshm = 0;
+  mb::UnevenJitGroup* d_jgroups = nullptr;
+  int4* d_pinfo = nullptr;
 };
 
 namespace mb {
 namespace {
-constexpr int kUnevenMaxBits = 17;
+// Largest register size in the persistent launch (MB_UNEVEN_MAX_BITS, 8..26; default 17).
+int uneven_max_bits() {
+  const char* e = getenv("MB_UNEVEN_MAX_BITS");
+  return e ? std::max(8, std::min(26, atoi(e))) : 17;
+}
 
 // Descriptors from the circuits' current tables and parameters (their device buffers move
 // when a larger batch of parameters is staged).
@@ -2442,9 +2456,9 @@ void uneven_descriptors(mb_uneven u, std::vector<UnevenGroup>& out) {
     pass0 += g.npasses;
     g.sample0 = sample0;
     sample0 += g.B;
-    // chunks of up to 2^15 amplitudes (the same for every pass of the group: its tiles are
-    // at most 2^11 amplitudes, so a pass has at least 2^(n-11) tiles)
-    g.nchunks = int(std::max<int64_t>(1, (int64_t(1) << s->n) >> 15));
+    // chunks of up to 2^chunk_bits amplitudes (the same for every pass of the group: a pass
+    // has at least 2^(n - chunk_bits) tiles)
+    g.nchunks = int(std::max<int64_t>(1, (int64_t(1) << s->n) >> u->chunk_bits));
     g.bind0 = b0;
     g.fuse0 = f0;
     g.nbinds = int(c->binds.size());
@@ -2470,15 +2484,28 @@ bool same_descriptors(const std::vector<UnevenGroup>& a, const std::vector<Uneve
   return a.size() == b.size() && (a.empty() || std::memcmp(a.data(), b.data(), sizeof(UnevenGroup) * a.size()) == 0);
 }
 
+std::vector<UnevenJitGroup> jit_groups(const std::vector<UnevenGroup>& gs) {
+  std::vector<UnevenJitGroup> out;
+  for (const UnevenGroup& g : gs)
+    out.push_back(UnevenJitGroup{g.states, g.table, g.xtab, g.xtabs, (long long)g.tstride, (long long)g.xrow});
+  return out;
+}
+
 void uneven_release(mb_uneven u) {
   dev_free(u->d_groups);
   dev_free(u->d_passes);
   dev_free(u->d_items);
   dev_free(u->d_next);
+  dev_free(u->d_jgroups);
+  dev_free(u->d_pinfo);
+  if (u->jit_fn) jit_release(u->jit_fn);
   u->d_groups = nullptr;
   u->d_passes = nullptr;
   u->d_items = nullptr;
   u->d_next = nullptr;
+  u->d_jgroups = nullptr;
+  u->d_pinfo = nullptr;
+  u->jit_fn = nullptr;
 }
 }  // namespace
 }  // namespace mb
@@ -2499,47 +2526,102 @@ extern "C" int mb_uneven_create(const mb_circuit* circuits, const mb_state* stat
   std::vector<int> order(ngroups);
   for (int g = 0; g < ngroups; ++g) order[g] = g;
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return u->ss[a]->n > u->ss[b]->n; });
-  for (int g : order) {
-    mb_circuit c = u->cs[g];
-    mb_state s = u->ss[g];
-    bool ok = (s->kind == MB_PURE || s->kind == MB_BATCH_PURE) && s->n >= 8 && s->n <= kUnevenMaxBits &&
-              s->batch > 0;
-    for (const COp& op : c->ops)
-      if (op.kind == MB_OP_GATE && op.k == 0) ok = false;
-    Schedule* S = nullptr;
-    if (ok) {
-      Tuning f;
-      f.t = std::min(kUnevenMaxTile, s->n);
-      f.R = 4;
-      if (int rc = get_schedule_impl(c, s->n, 0, 0, 0, -1, s->batch, &f, true, &S)) return rc;
-      for (const Pass& p : S->passes) ok = ok && p.kind == PASS_TILE && p.t <= kUnevenMaxTile && p.t >= 4;
-      ok = ok && S->R == 4;
+  // Schedules of every group that fits: 2^min(10, n)-amplitude tiles with 3 register bits for
+  // the specialised form, 2^min(11, n) with 4 for the interpreter form.
+  const int max_bits = uneven_max_bits();
+  auto collect = [&](bool jit) -> int {
+    u->pgroups.clear();
+    u->fallback.clear();
+    u->scheds.clear();
+    u->hpasses.clear();
+    u->u2 = false;
+    u->bytes = u->flops = 0;
+    for (int g : order) {
+      mb_circuit c = u->cs[g];
+      mb_state s = u->ss[g];
+      bool ok = (s->kind == MB_PURE || s->kind == MB_BATCH_PURE) && s->n >= 8 && s->n <= max_bits &&
+                s->batch > 0;
+      for (const COp& op : c->ops)
+        if (op.kind == MB_OP_GATE && op.k == 0) ok = false;
+      Schedule* S = nullptr;
+      if (ok) {
+        Tuning f;
+        f.t = std::min(jit ? kUnevenJitTile : kUnevenMaxTile, s->n);
+        f.R = jit ? 3 : 4;
+        if (int rc = get_schedule_impl(c, s->n, 0, 0, 0, -1, s->batch, &f, true, &S)) return rc;
+        for (const Pass& p : S->passes) ok = ok && p.kind == PASS_TILE && p.t <= f.t && p.t >= f.R + 1;
+        ok = ok && S->R == f.R;
+      }
+      if (!ok) {
+        u->fallback.push_back(g);
+        continue;
+      }
+      u->pgroups.push_back(g);
+      u->scheds.push_back(S);
+      for (const Pass& p : S->passes) {
+        UnevenPass up{};
+        up.t = p.t;
+        up.nstages = int(p.stages.size());
+        for (int q = 0; q < p.t; ++q) up.bits[q] = p.bits[q];
+        up.stages = S->d_stages + p.stage_off;
+        up.mops = S->d_mops;
+        u->hpasses.push_back(up);
+        u->u2 = u->u2 || p.has_u2;
+        const double amps = double(int64_t(1) << s->n) * s->batch;
+        u->bytes += 32.0 * amps;
+        u->flops += pass_flops_per_amp(p, false) * amps;
+      }
     }
-    if (!ok) {
-      u->fallback.push_back(g);
-      continue;
-    }
-    u->pgroups.push_back(g);
-    u->scheds.push_back(S);
-    for (const Pass& p : S->passes) {
-      UnevenPass up{};
-      up.t = p.t;
-      up.nstages = int(p.stages.size());
-      for (int q = 0; q < p.t; ++q) up.bits[q] = p.bits[q];
-      up.stages = S->d_stages + p.stage_off;
-      up.mops = S->d_mops;
-      u->hpasses.push_back(up);
-      u->u2 = u->u2 || p.has_u2;
-      const double amps = double(int64_t(1) << s->n) * s->batch;
-      u->bytes += 32.0 * amps;
-      u->flops += pass_flops_per_amp(p, false) * amps;
-    }
-  }
+    return MB_OK;
+  };
   int rc;
+  const char* ej = getenv("MB_UNEVEN_JIT");
+  bool jit = jit_available() && !(ej && atoi(ej) == 0);
+  // Chunks of the specialised form hold 2^12 amplitudes (four tiles), so even the largest
+  // sample's pass spreads over many CTAs; the interpreter form keeps 2^15 (MB_UNEVEN_CHUNK_BITS
+  // overrides either, 10..20).
+  auto chunk_bits = [&](bool j) {
+    const char* e = getenv("MB_UNEVEN_CHUNK_BITS");
+    return e ? std::max(10, std::min(20, atoi(e))) : (j ? 12 : 15);
+  };
+  u->chunk_bits = chunk_bits(jit);
+  if ((rc = collect(jit))) return rc;
+  if (jit && !u->pgroups.empty()) {
+    // one module with a device function per pass of every persistent group
+    std::vector<UnevenJitPass> jp;
+    for (size_t i = 0; i < u->pgroups.size(); ++i) {
+      const int n = u->ss[u->pgroups[i]]->n;
+      const Schedule* S = u->scheds[i];
+      for (size_t k = 0; k < S->passes.size(); ++k)
+        jp.push_back(UnevenJitPass{&S->passes[k], n, k == 0,
+                                   int(std::max<int64_t>(1, (int64_t(1) << n) >> u->chunk_bits))});
+    }
+    size_t shm = 0;
+    int threads = 0;
+    const size_t need = (size_t(16) << kUnevenJitTile) + 16 * 2048 + 1024;
+    u->jctas = std::max(1, std::min(4, int((227 * 1024) / need)));
+    std::vector<std::string> src{jit_uneven_source(jp, 3, u->jctas, &threads, &shm)};
+    std::vector<CUfunction> fns;
+    std::string err;
+    if (jit_prepare(src, fns, &err, 0.0) == MB_OK && fns[0]) {
+      u->jit_fn = (void*)fns[0];
+      jit_retain(u->jit_fn);
+      u->jthreads = threads;
+      u->jshm = shm;
+    } else {
+      if (getenv("MB_JIT_VERBOSE")) fprintf(stderr, "mossb200: persistent launch interpreted: %s\n", err.c_str());
+      jit = false;
+      u->chunk_bits = chunk_bits(false);
+      if ((rc = collect(false))) return rc;
+    }
+  } else {
+    jit = false;
+  }
   uneven_descriptors(u.get(), u->hgroups);
   // items by pass index first (every chunk of pass p of every sample before any of pass p+1),
-  // then largest groups first
-  std::vector<int4> items;
+  // then largest groups first; the specialised form names the pass by its index over all
+  // groups and finds the counters and the group through pinfo
+  std::vector<int4> items, pinfo;
   int maxp = 0;
   for (const UnevenGroup& g : u->hgroups) maxp = std::max(maxp, g.npasses);
   for (int pi = 0; pi < maxp; ++pi)
@@ -2547,8 +2629,13 @@ extern "C" int mb_uneven_create(const mb_circuit* circuits, const mb_state* stat
       const UnevenGroup& g = u->hgroups[i];
       if (pi >= g.npasses) continue;
       for (int b = 0; b < g.B; ++b)
-        for (int ch = 0; ch < g.nchunks; ++ch) items.push_back(make_int4(int(i), b, pi, ch));
+        for (int ch = 0; ch < g.nchunks; ++ch)
+          items.push_back(jit ? make_int4(g.pass0 + pi, b, ch, 0) : make_int4(int(i), b, pi, ch));
     }
+  for (size_t i = 0; i < u->hgroups.size(); ++i) {
+    const UnevenGroup& g = u->hgroups[i];
+    for (int pi = 0; pi < g.npasses; ++pi) pinfo.push_back(make_int4(g.sample0, pi * g.nchunks, int(i), 0));
+  }
   u->nitems = int(items.size());
   for (const UnevenGroup& g : u->hgroups) u->nsamples += g.B;
   for (const UnevenGroup& g : u->hgroups) {
@@ -2559,13 +2646,22 @@ extern "C" int mb_uneven_create(const mb_circuit* circuits, const mb_state* stat
     if ((rc = dev_alloc((void**)&u->d_groups, sizeof(UnevenGroup) * u->hgroups.size())) ||
         (rc = dev_alloc((void**)&u->d_passes, sizeof(UnevenPass) * std::max<size_t>(1, u->hpasses.size()))) ||
         (rc = dev_alloc((void**)&u->d_items, sizeof(int4) * items.size())) ||
-        (rc = dev_alloc((void**)&u->d_next, sizeof(unsigned) * (1 + size_t(u->nsamples))))) {
+        (rc = dev_alloc((void**)&u->d_next, sizeof(unsigned) * (1 + size_t(u->nsamples)))) ||
+        (u->jit_fn && (rc = dev_alloc((void**)&u->d_jgroups, sizeof(UnevenJitGroup) * u->hgroups.size()))) ||
+        (u->jit_fn && (rc = dev_alloc((void**)&u->d_pinfo, sizeof(int4) * pinfo.size())))) {
       uneven_release(u.get());
       return rc;
     }
     cudaStream_t st = g_ctx.stream;
     MB_CHECK_CUDA(cudaMemcpyAsync(u->d_groups, u->hgroups.data(), sizeof(UnevenGroup) * u->hgroups.size(),
                                   cudaMemcpyHostToDevice, st));
+    if (u->jit_fn) {
+      const std::vector<UnevenJitGroup> jg = jit_groups(u->hgroups);
+      MB_CHECK_CUDA(cudaMemcpyAsync(u->d_jgroups, jg.data(), sizeof(UnevenJitGroup) * jg.size(), cudaMemcpyHostToDevice,
+                                    st));
+      MB_CHECK_CUDA(cudaMemcpyAsync(u->d_pinfo, pinfo.data(), sizeof(int4) * pinfo.size(), cudaMemcpyHostToDevice, st));
+      MB_CHECK_CUDA(cudaStreamSynchronize(st));  // jg and pinfo leave scope
+    }
     if (!u->hpasses.empty())
       MB_CHECK_CUDA(cudaMemcpyAsync(u->d_passes, u->hpasses.data(), sizeof(UnevenPass) * u->hpasses.size(),
                                     cudaMemcpyHostToDevice, st));
@@ -2606,6 +2702,10 @@ extern "C" int mb_uneven_apply(mb_uneven u, int flags) {
       if (int rc = check_not_capturing("mb_uneven_apply after the circuits' parameter buffers moved")) return rc;
       MB_CHECK_CUDA(cudaMemcpyAsync(u->d_groups, cur.data(), sizeof(UnevenGroup) * cur.size(), cudaMemcpyHostToDevice,
                                     st));
+      const std::vector<UnevenJitGroup> jg = jit_groups(cur);
+      if (u->jit_fn)
+        MB_CHECK_CUDA(cudaMemcpyAsync(u->d_jgroups, jg.data(), sizeof(UnevenJitGroup) * jg.size(),
+                                      cudaMemcpyHostToDevice, st));
       MB_CHECK_CUDA(cudaStreamSynchronize(st));
       u->hgroups = cur;
     }
@@ -2621,16 +2721,25 @@ extern "C" int mb_uneven_apply(mb_uneven u, int flags) {
       MB_LAUNCHED();
     }
     MB_CHECK_CUDA(cudaMemsetAsync(u->d_next, 0, sizeof(unsigned) * (1 + size_t(u->nsamples)), st));
-    const size_t shm = (size_t(16) << kUnevenMaxTile) + (size_t(8) << kUnevenMaxTile) + 1024;
-    const int grid = std::min(u->nitems, g_ctx.sm_count * 2);
-    ProfScope ps("k_uneven", u->bytes, st, u->flops);
-    auto launch = [&](auto kern) {
-      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm));
-      kern<<<grid, kUnevenThreads, shm, st>>>(u->d_groups, u->d_passes, u->d_items, u->nitems, u->d_next,
-                                              u->d_next + 1, zero ? 1 : 0, g_ctx.flags + 2);
-    };
-    u->u2 ? launch(k_uneven<true>) : launch(k_uneven<false>);
-    MB_LAUNCHED();
+    if (u->jit_fn) {
+      const int grid = std::min(u->nitems, g_ctx.sm_count * u->jctas);
+      ProfScope ps("mbk_uneven", u->bytes, st, u->flops);
+      if (int rc = jit_launch_uneven((CUfunction)u->jit_fn, u->d_jgroups, u->d_pinfo, u->d_items, u->nitems, u->d_next,
+                                     u->d_next + 1, zero ? 1 : 0, g_ctx.flags + 2, u->jthreads, u->jshm, grid, st))
+        return rc;
+      MB_LAUNCHED();
+    } else {
+      const size_t shm = (size_t(16) << kUnevenMaxTile) + (size_t(8) << kUnevenMaxTile) + 1024;
+      const int grid = std::min(u->nitems, g_ctx.sm_count * 2);
+      ProfScope ps("k_uneven", u->bytes, st, u->flops);
+      auto launch = [&](auto kern) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm));
+        kern<<<grid, kUnevenThreads, shm, st>>>(u->d_groups, u->d_passes, u->d_items, u->nitems, u->d_next,
+                                                u->d_next + 1, zero ? 1 : 0, g_ctx.flags + 2);
+      };
+      u->u2 ? launch(k_uneven<true>) : launch(k_uneven<false>);
+      MB_LAUNCHED();
+    }
   }
   for (int g : u->fallback) {
     mb_circuit c = u->cs[g];

@@ -187,6 +187,7 @@ struct StageGen {
   std::string pre = "a";  // variable prefix
   const std::map<int, int>* smap = nullptr;  // table offset -> slot of the pass's shared-memory copy
   const std::map<int, int>* pmap = nullptr;  // per-sample entry -> slot of the tile's shared copy (spar)
+  int pkey = 0;        // added to the smap key of per-sample entries (copies holding both kinds)
 
   // Selector classification: register bit k (>= 0), or -1 with a runtime expression.
   int regbit(int sel) const {
@@ -214,7 +215,7 @@ struct StageGen {
   std::string v(int j) const { return pre + std::to_string(nm[j]); }
   std::string ldm(const MOp& m, int e) const {
     if (smap) {
-      auto it = smap->find(smat_key(m, e));
+      auto it = smap->find(smat_key(m, e) | (m.param ? pkey : 0));
       if (it != smap->end()) {
         const std::string x = "smat[" + std::to_string(it->second) + "]";
         return m.conj ? "cj(" + x + ")" : x;
@@ -433,9 +434,12 @@ std::string reg_off_const(int j, int R, const int* reg) {
   return std::to_string(c) + "ull";
 }
 
-// Entry point of a generated source: mbk_tile (tile pass), mbk_reg (strided sweep) or
-// mbk_adj (adjoint dual-state pass).
+// Entry point of a generated source: mbk_tile (tile pass), mbk_reg (strided sweep), mbk_adj
+// (adjoint dual-state pass), mbk_uneven (persistent launch over several register sizes) or
+// mbk_pauli (Pauli-string expectation pass).
 const char* kernel_name(const std::string& src) {
+  if (src.find(" mbk_uneven(") != std::string::npos) return "mbk_uneven";
+  if (src.find(" mbk_pauli(") != std::string::npos) return "mbk_pauli";
   if (src.find(" mbk_adj(") != std::string::npos) return "mbk_adj";
   if (src.find(" mbk_reg(") != std::string::npos) return "mbk_reg";
   return "mbk_tile";
@@ -1066,6 +1070,369 @@ std::string jit_reg_source(const Pass& p, int N, bool stage_params) {
   for (int j = 0; j < A; ++j) o << "    vs[lb | " << reg_off_const(j, R, reg) << "] = " << sg.v(j) << ";\n";
   o << "  }\n}\n";
   return o.str();
+}
+
+// ---- persistent uneven launch ----------------------------------------------------------------
+// One kernel over samples of several register sizes: its work items are (pass, sample, chunk of
+// tiles), ordered by pass index, taken from a work counter, each waiting on its sample's
+// completion counter for the chunks of the previous pass (the protocol of the interpreter form
+// k_uneven). Every pass is a straight-line device function of its own; the kernel dispatches an
+// item to it with a switch. Functions are not inlined, so each is optimised and register-
+// allocated on its own, and the module's compile time grows with the number of passes, not
+// faster.
+
+// Matrix elements of one pass for one sample, fixed and per-sample entries in one shared copy
+// (per-sample keys carry kRowKey), filled once per work item. At most 2048 entries (32 KB); a
+// pass with more reads its elements from the tables.
+constexpr int32_t kRowKey = 1 << 28;
+constexpr int32_t kKeyOff = kRowKey - 1;
+
+static SharedMats uneven_mats(const Pass& p) {
+  SharedMats sm;
+  bool ok = true;
+  auto add = [&](const MOp& m, int e) {
+    if ((m.off[e] & ~kXtabFlag) > kKeyOff) ok = false;
+    const int key = smat_key(m, e) | (m.param ? kRowKey : 0);
+    if (sm.slot.count(key)) return;
+    sm.slot[key] = int(sm.offs.size());
+    sm.offs.push_back(key);
+  };
+  for (const MOp& m : p.mops) switch (m.type) {
+      case MOP_U1: case MOP_CTRL: case MOP_RROT: case MOP_IROT: for (int e = 0; e < 4; ++e) add(m, e); break;
+      case MOP_LIFT: add(m, 0); break;
+      case MOP_U2: for (int e = 0; e < 16; ++e) add(m, e); break;
+      case MOP_CHAN: for (int e = 0; e < 6; ++e) add(m, e); break;
+      case MOP_DIAG: for (int e = 0; e < (1 << m.nsel); ++e) if ((m.active >> e) & 1) add(m, e); break;
+      case MOP_CPHASE: if (!m.r1) add(m, 0); break;
+      default: break;
+    }
+  if (!ok || sm.offs.size() > 2048) sm = SharedMats();
+  return sm;
+}
+
+// Global offset of the pass-local index `l` (a u32 expression): every run of consecutive pass
+// bits moves as one masked shift.
+static std::string deposit_expr(const Pass& p, const char* l) {
+  std::ostringstream e;
+  e << "(0ull";
+  for (int q = 0; q < p.t;) {
+    int r = q + 1;
+    while (r < p.t && p.bits[r] == p.bits[r - 1] + 1) ++r;
+    e << " | ((u64)((" << l << " >> " << q << ") & " << ((1u << (r - q)) - 1) << "u) << " << p.bits[q] << ")";
+    q = r;
+  }
+  e << ")";
+  return e.str();
+}
+
+// Device function mbp<k>: every tile of one chunk of pass k for sample b (load through L2, the
+// register stages, store).
+static void emit_uneven_pass(std::ostringstream& o, const UnevenJitPass& up, int k, int R, int threads, int tmax) {
+  const Pass& p = *up.p;
+  const int A = 1 << R, T = 1 << p.t, vt = 1 << (p.t - R);
+  const SharedMats sm = uneven_mats(p);
+  if (!sm.offs.empty()) {
+    o << "__constant__ int k_um" << k << "[" << sm.offs.size() << "] = {";
+    for (size_t i = 0; i < sm.offs.size(); ++i) o << (i ? "," : "") << sm.offs[i];
+    o << "};\n";
+  }
+  o << "static __device__ __noinline__ void mbp" << k << "(const UG* __restrict__ gd, int b, int chunk, int zero_init) {\n";
+  o << "  const u32 tx = threadIdx.x;\n  double2* tl = dynsm;\n  double2* smat = dynsm + " << (1 << tmax)
+    << "; (void)smat; (void)zero_init;\n";
+  o << "  const UG G = *gd;\n  const double2* tab = G.table; const double2* xtab = G.xtab; (void)tab; (void)xtab;\n";
+  o << "  const double2* tb = tab + (long long)b * G.tstride; const double2* xb = G.xtabs + (long long)b * G.xrow;"
+    << " (void)tb; (void)xb;\n";
+  o << "  double2* v = G.states + ((long long)b << " << up.n << ");\n";
+  if (!sm.offs.empty())
+    o << "  for (u32 i = tx; i < " << sm.offs.size() << "u; i += " << threads << "u) { const int mo = k_um" << k
+      << "[i]; smat[i] = (mo & " << kXrowKey << ") ? __ldg(xb + (mo & " << kKeyOff << ")) : (mo & " << kRowKey
+      << ") ? __ldg(tb + (mo & " << kKeyOff << ")) : (mo & " << kXtabFlag << ") ? __ldg(xtab + (mo & " << kKeyOff
+      << ")) : __ldg(tab + mo); }\n";
+  const long long ntiles = 1ll << (up.n - p.t);
+  const long long per = (ntiles + up.nchunks - 1) / up.nchunks;
+  o << "  const long long t0 = (long long)chunk * " << per << "ll;\n  const long long t1 = t0 + " << per << "ll < "
+    << ntiles << "ll ? t0 + " << per << "ll : " << ntiles << "ll;\n";
+  o << "  for (long long tile = t0; tile < t1; ++tile) {\n    u64 gb = (u64)tile;\n";
+  std::vector<int> sorted(p.bits.begin(), p.bits.begin() + p.t);
+  std::sort(sorted.begin(), sorted.end());
+  for (int bit : sorted)
+    o << "    gb = ((gb >> " << bit << ") << " << (bit + 1) << ") | (gb & " << ((1ull << bit) - 1) << "ull);\n";
+  const std::string dep = deposit_expr(p, "l");
+  o << "    for (u32 l = tx; l < " << T << "u; l += " << threads << "u) {\n      const u64 go = gb | " << dep << ";\n";
+  if (up.first)
+    o << "      tl[swz(l)] = zero_init ? make_double2(go == 0ull ? 1.0 : 0.0, 0.0) : __ldcg(v + go);\n";
+  else
+    o << "      tl[swz(l)] = __ldcg(v + go);\n";
+  o << "    }\n    __syncthreads();\n    double2 ";
+  for (int j = 0; j < A; ++j) o << (j ? ", " : "") << "a" << j;
+  o << ";\n";
+  for (size_t si = 0; si < p.stages.size(); ++si) {
+    const StageDesc& sd = p.stages[si];
+    o << "    " << (vt < threads ? "if (tx < " + std::to_string(vt) + "u) " : std::string()) << "{\n      const u32 lb = 0u";
+    for (int q = 0; q < sd.ntid; ++q) o << " | (((tx >> " << q << ") & 1u) << " << sd.tid[q] << ")";
+    o << ";\n";
+    for (int j = 0; j < A; ++j) o << "      a" << j << " = tl[swz(lb | " << reg_off_const(j, R, sd.reg) << ")];\n";
+    StageGen sg{R, sd.reg, o, false, std::vector<int>(A)};
+    sg.smap = &sm.slot;
+    sg.pkey = kRowKey;
+    for (int j = 0; j < A; ++j) sg.nm[j] = j;
+    for (int q = 0; q < sd.nops; ++q) sg.emit(p.mops[sd.op0 + q]);
+    for (int j = 0; j < A; ++j) o << "      tl[swz(lb | " << reg_off_const(j, R, sd.reg) << ")] = " << sg.v(j) << ";\n";
+    o << "    }\n" << stage_sync(p, si);
+  }
+  o << "    __syncthreads();\n    for (u32 l = tx; l < " << T << "u; l += " << threads << "u) v[gb | " << dep
+    << "] = tl[swz(l)];\n    __syncthreads();\n  }\n}\n";
+}
+
+std::string jit_uneven_source(const std::vector<UnevenJitPass>& passes, int R, int ctas, int* threads, size_t* shm) {
+  int tmax = R + 5;
+  size_t ne = 0;
+  for (const UnevenJitPass& up : passes) {
+    tmax = std::max(tmax, up.p->t);
+    ne = std::max(ne, uneven_mats(*up.p).offs.size());
+  }
+  const int th = 1 << (tmax - R);
+  std::ostringstream o;
+  o << kPrelude;
+  o << "struct UG { double2* states; const double2* table; const double2* xtab; const double2* xtabs; "
+    << "long long tstride; long long xrow; };\n";
+  o << "extern __shared__ double2 dynsm[];\n";
+  for (size_t k = 0; k < passes.size(); ++k) emit_uneven_pass(o, passes[k], int(k), R, th, tmax);
+  o << "extern \"C\" __global__ void __launch_bounds__(" << th << ", " << std::max(1, ctas)
+    << ") mbk_uneven(const UG* __restrict__ groups, const int4* __restrict__ pinfo, const int4* __restrict__ items, "
+    << "int nitems, u32* next, u32* done, int zero_init, u32* err) {\n";
+  o << "  __shared__ int s_item, s_ok;\n  const u32 tx = threadIdx.x;\n  for (;;) {\n";
+  o << "    if (tx == 0) s_item = (int)atomicAdd(next, 1u);\n    __syncthreads();\n    const int item = s_item;\n"
+    << "    if (item >= nitems) break;\n    const int4 it = items[item];\n    const int4 pi = pinfo[it.x];\n"
+    << "    u32* cnt = done + pi.x + it.y;\n";
+  // every chunk of the previous passes of this sample (taken earlier by running CTAs)
+  o << "    if (tx == 0) {\n      int ok = 1;\n"
+    << "      for (u32 spin = 0; atomicAdd(cnt, 0u) < (u32)pi.y; ++spin) {\n"
+    << "        if (spin > (1u << 24)) { atomicOr(err, 1u); ok = 0; break; }\n        __nanosleep(64);\n      }\n"
+    << "      __threadfence();\n      s_ok = ok;\n    }\n    __syncthreads();\n    if (!s_ok) break;\n";
+  o << "    switch (it.x) {\n";
+  for (size_t k = 0; k < passes.size(); ++k)
+    o << "      case " << k << ": mbp" << k << "(groups + pi.z, it.y, it.z, zero_init); break;\n";
+  o << "      default: break;\n    }\n";
+  // publish this chunk: every thread's stores, then the counter
+  o << "    __threadfence();\n    __syncthreads();\n    if (tx == 0) atomicAdd(cnt, 1u);\n  }\n}\n";
+  *threads = th;
+  *shm = (size_t(16) << tmax) + 16 * ne;
+  return o.str();
+}
+
+int jit_launch_uneven(CUfunction fn, const UnevenJitGroup* groups, const int4* pinfo, const int4* items, int nitems,
+                      unsigned* next, unsigned* done, int zero_init, unsigned* err, int threads, size_t shm, int grid,
+                      cudaStream_t st) {
+  Drv& d = drv();
+  if (d.setattr(fn, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, int(shm)) != CUDA_SUCCESS) return MB_EDEVICE;
+  int ni = nitems, zi = zero_init;
+  void* params[] = {(void*)&groups, (void*)&pinfo, (void*)&items, &ni, &next, &done, &zi, &err};
+  if (d.launch(fn, grid, 1, 1, threads, 1, 1, unsigned(shm), (CUstream)st, params, nullptr) != CUDA_SUCCESS) {
+    set_error("persistent uneven launch failed");
+    return MB_EDEVICE;
+  }
+  return MB_OK;
+}
+
+// ---- Pauli-string expectation pass -------------------------------------------------------------
+// The pass of k_pauli_pass (tiles of the five lane bits and nr register bits in shared memory,
+// every flip group of the pass evaluated against its partner amplitudes) with the groups,
+// their flip masks and the strings' Z masks as constants. A string's sign at index
+// j = base | l splits into a tile-base part (-1)^{|base & zh|} and a local part
+// (-1)^{|(l ^ x) & zl|}; strings of a group with the same zh form a class whose local sum
+// F(l) = sum_s c_s (-1)^{|(l ^ x) & zl_s|} depends only on the thread's own local indices, so it
+// is formed once per thread before the tile loop and each tile costs one sign per class.
+// Coefficients come from an array, so observables that differ only in them share the kernel.
+
+// Global bits of local index `e` (a u32 expression): lane bits 0..4, then register bits.
+static std::string pauli_local_bits(const PauliJitPass& p, const std::string& e) {
+  std::ostringstream o;
+  o << "((u64)((" << e << ") & 31u)";
+  for (int r = 0; r < p.nr;) {
+    int q = r + 1;
+    while (q < p.nr && p.reg[q] == p.reg[q - 1] + 1) ++q;
+    o << " | ((u64)(((" << e << ") >> " << (5 + r) << ") & " << ((1u << (q - r)) - 1) << "u) << " << p.reg[r] << ")";
+    r = q;
+  }
+  o << ")";
+  return o.str();
+}
+
+std::string jit_pauli_source(const PauliJitPass& p, int max_vals) {
+  constexpr int kThreads = 256;
+  const int local = 5 + p.nr, per = (1 << local) / kThreads;
+  uint64_t localm = 31;
+  for (int r = 0; r < p.nr; ++r) localm |= uint64_t(1) << p.reg[r];
+  // classes of every group (strings with the same zh); a class is real when all of its
+  // coefficients are, and local when some string has Z bits among the local bits
+  struct Cls {
+    uint64_t zh;
+    std::vector<PauliJitString> s;
+    bool local, real;
+  };
+  std::vector<std::vector<Cls>> cls(p.groups.size());
+  std::vector<bool> greal(p.groups.size(), true);
+  int vals = 0;
+  for (size_t g = 0; g < p.groups.size(); ++g) {
+    const PauliJitGroup& G = p.groups[g];
+    std::map<uint64_t, size_t> at;
+    for (const PauliJitString& s : G.strings) {
+      const uint64_t zh = s.z & ~localm;
+      if (!at.count(zh)) {
+        at[zh] = cls[g].size();
+        cls[g].push_back(Cls{zh, {}, false, true});
+      }
+      Cls& c = cls[g][at[zh]];
+      c.s.push_back(s);
+      c.local = c.local || (s.z & localm) != 0;
+      c.real = c.real && s.real;
+    }
+    const int slots = (G.xl != 0 && G.herm) ? per / 2 : per;
+    for (const Cls& c : cls[g]) {
+      if (c.local) vals += slots * (c.real ? 1 : 2);
+      greal[g] = greal[g] && c.real;
+    }
+  }
+  if (vals > max_vals) return "";
+  auto fname = [](size_t g, size_t c, int k) {
+    return "F" + std::to_string(g) + "_" + std::to_string(c) + "_" + std::to_string(k);
+  };
+  std::ostringstream o;
+  o << kPrelude;
+  o << "__device__ __forceinline__ double dneg(double a, u64 s) { return __longlong_as_double(__double_as_longlong(a) ^ "
+       "(long long)s); }\n";
+  o << "extern \"C\" __global__ void __launch_bounds__(" << kThreads << ", 2) mbk_pauli(const double2* __restrict__ v, "
+    << "const double2* __restrict__ coef, long long tps, double2* partials, u32* counters, double2* out) {\n";
+  o << "  extern __shared__ double2 tile[];\n  __shared__ double2 wp[" << kThreads / 32 << "];\n  __shared__ bool last;\n";
+  o << "  const u32 tx = threadIdx.x;\n  const int b = blockIdx.y, G = gridDim.x;\n";
+  o << "  const double2* vs = v + ((long long)b << " << p.n << ");\n";
+  for (int k = 0; k < per; ++k)
+    o << "  const u64 lk" << k << " = " << pauli_local_bits(p, "tx + " + std::to_string(k * kThreads) + "u") << ";\n";
+  auto idx = [&](size_t g, int k) {
+    const PauliJitGroup& G = p.groups[g];
+    return (G.xl != 0 && G.herm) ? "i" + std::to_string(g) + "_" + std::to_string(k)
+                                 : "(tx + " + std::to_string(k * kThreads) + "u)";
+  };
+  auto lbits = [&](size_t g, int k) {
+    const PauliJitGroup& G = p.groups[g];
+    return (G.xl != 0 && G.herm) ? "b" + std::to_string(g) + "_" + std::to_string(k) : "lk" + std::to_string(k);
+  };
+  // factors of the local classes at the thread's own local indices (Hermitian flip groups: the
+  // pair members with bit hb clear)
+  for (size_t g = 0; g < p.groups.size(); ++g) {
+    const PauliJitGroup& G = p.groups[g];
+    const bool herm = G.xl != 0 && G.herm;
+    const int slots = herm ? per / 2 : per;
+    if (herm)
+      for (int k = 0; k < slots; ++k) {
+        const std::string m = "(tx + " + std::to_string(k * kThreads) + "u)";
+        const std::string nm = "i" + std::to_string(g) + "_" + std::to_string(k);
+        o << "  const u32 " << nm << " = ((" << m << " >> " << G.hb << ") << " << (G.hb + 1) << ") | (" << m << " & "
+          << ((1u << G.hb) - 1) << "u);\n";
+        o << "  const u64 b" << g << "_" << k << " = " << pauli_local_bits(p, nm) << ";\n";
+      }
+    for (size_t c = 0; c < cls[g].size(); ++c) {
+      const Cls& C = cls[g][c];
+      if (!C.local) continue;
+      for (int k = 0; k < slots; ++k) {
+        const std::string F = fname(g, c, k);
+        o << "  " << (C.real ? "double " : "double2 ") << F << (C.real ? " = 0.0;\n" : " = make_double2(0.0, 0.0);\n");
+        for (const PauliJitString& s : C.s) {
+          const uint64_t zl = s.z & localm;
+          const std::string q = "__ldg(coef + " + std::to_string(s.s) + ")";
+          const std::string sg = "(u64)(__popcll((" + lbits(g, k) + " ^ " + std::to_string(G.x) + "ull) & " +
+                                 std::to_string(zl) + "ull) & 1) << 63";
+          if (C.real)
+            o << "  " << F << " += " << (zl ? "dneg(" + q + ".x, " + sg + ")" : q + ".x") << ";\n";
+          else
+            o << "  { const double2 t = " << (zl ? "cneg(" + q + ", " + sg + ")" : q) << "; " << F << ".x += t.x; " << F
+              << ".y += t.y; }\n";
+        }
+      }
+    }
+  }
+  o << "  double ar = 0.0, ai = 0.0;\n";
+  o << "  for (long long T = blockIdx.x; T < tps; T += G) {\n    u64 base = (u64)T << 5;\n";
+  std::vector<int> regs(p.reg, p.reg + p.nr);
+  std::sort(regs.begin(), regs.end());
+  for (int bit : regs)
+    o << "    base = ((base >> " << bit << ") << " << (bit + 1) << ") | (base & " << ((1ull << bit) - 1) << "ull);\n";
+  for (int k = 0; k < per; ++k) o << "    tile[tx + " << k * kThreads << "u] = vs[base | lk" << k << "];\n";
+  o << "    __syncthreads();\n";
+  for (size_t g = 0; g < p.groups.size(); ++g) {
+    const PauliJitGroup& G = p.groups[g];
+    const bool herm = G.xl != 0 && G.herm, re = greal[g];
+    const int slots = herm ? per / 2 : per;
+    // classes without local Z bits: one value per tile (coefficients read through the cache)
+    o << "    {\n      double kx = 0.0" << (re ? "" : ", ky = 0.0") << ";\n";
+    for (size_t c = 0; c < cls[g].size(); ++c) {
+      const Cls& C = cls[g][c];
+      const std::string sg = "(u64)(__popcll(base & " + std::to_string(C.zh) + "ull) & 1) << 63";
+      if (C.local) {
+        if (C.zh) o << "      const u64 s" << c << " = " << sg << ";\n";
+        continue;
+      }
+      o << "      { double2 t = make_double2(0.0, 0.0);";
+      for (const PauliJitString& s : C.s) o << " { const double2 q = __ldg(coef + " << s.s << "); t.x += q.x; t.y += q.y; }";
+      if (C.zh) o << " t = cneg(t, " << sg << ");";
+      o << " kx += t.x;" << (re ? "" : " ky += t.y;") << " }\n";
+    }
+    for (int k = 0; k < slots; ++k) {
+      o << "      { double fx = kx" << (re ? "" : ", fy = ky") << ";\n";
+      for (size_t c = 0; c < cls[g].size(); ++c) {
+        const Cls& C = cls[g][c];
+        if (!C.local) continue;
+        const std::string F = fname(g, c, k), s = "s" + std::to_string(c);
+        if (C.real)
+          o << "        fx += " << (C.zh ? "dneg(" + F + ", " + s + ")" : F) << ";\n";
+        else
+          o << "        { const double2 t = " << (C.zh ? "cneg(" + F + ", " + s + ")" : F) << "; fx += t.x; fy += t.y; }\n";
+      }
+      const std::string i = idx(g, k);
+      if (G.xl == 0) {
+        o << "        const double2 a = tile[" << i << "]; const double p2 = fma(a.x, a.x, a.y * a.y);\n"
+          << "        ar = fma(fx, p2, ar);" << (re ? "" : " ai = fma(fy, p2, ai);") << " }\n";
+      } else {
+        o << "        const double2 a = tile[" << i << "], q = tile[" << i << " ^ " << G.xl << "u];\n"
+          << "        const double cr = fma(a.x, q.x, a.y * q.y), ci = fma(a.x, q.y, -a.y * q.x); (void)ci;\n";
+        if (herm)
+          o << "        ar = fma(2.0 * fx, cr, " << (re ? "ar" : "fma(-2.0 * fy, ci, ar)") << "); }\n";
+        else if (re)
+          o << "        ar = fma(fx, cr, ar); ai = fma(fx, ci, ai); }\n";
+        else
+          o << "        ar = fma(fx, cr, fma(-fy, ci, ar)); ai = fma(fx, ci, fma(fy, cr, ai)); }\n";
+      }
+    }
+    o << "    }\n";
+  }
+  o << "    __syncthreads();\n  }\n";
+  // block sum, then the last block of the sample adds the blocks' sums in block order
+  o << "  for (int d = 16; d > 0; d >>= 1) { ar += __shfl_down_sync(0xffffffffu, ar, d); "
+    << "ai += __shfl_down_sync(0xffffffffu, ai, d); }\n";
+  o << "  if ((tx & 31u) == 0u) wp[tx >> 5] = make_double2(ar, ai);\n  __syncthreads();\n";
+  o << "  if (tx == 0) {\n    double sx = 0.0, sy = 0.0;\n    for (int w = 0; w < " << kThreads / 32
+    << "; ++w) { sx += wp[w].x; sy += wp[w].y; }\n"
+    << "    partials[(long long)b * G + blockIdx.x] = make_double2(sx, sy);\n    __threadfence();\n"
+    << "    last = atomicAdd(&counters[b], 1u) == (u32)(G - 1);\n  }\n  __syncthreads();\n";
+  o << "  if (last && tx == 0) {\n    double sx = 0.0, sy = 0.0;\n"
+    << "    for (int g = 0; g < G; ++g) { const double2 q = __ldcg(&partials[(long long)b * G + g]); sx += q.x; sy += q.y; }\n"
+    << "    const double2 o0 = __ldcg(&out[b]);\n    out[b] = make_double2(o0.x + sx, o0.y + sy);\n"
+    << "    counters[b] = 0;\n  }\n}\n";
+  return o.str();
+}
+
+int jit_launch_pauli(CUfunction fn, const double2* v, const double2* coef, int64_t tps, double2* partials,
+                     unsigned* counters, double2* out, int grid, int batch, size_t shm, cudaStream_t st) {
+  Drv& d = drv();
+  if (d.setattr(fn, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, int(shm)) != CUDA_SUCCESS) return MB_EDEVICE;
+  long long tp = tps;
+  void* params[] = {(void*)&v, (void*)&coef, &tp, &partials, &counters, &out};
+  if (d.launch(fn, grid, batch, 1, 256, 1, 1, unsigned(shm), (CUstream)st, params, nullptr) != CUDA_SUCCESS) {
+    set_error("specialised Pauli pass launch failed");
+    return MB_EDEVICE;
+  }
+  return MB_OK;
 }
 
 int jit_prepare(std::vector<std::string>& sources, std::vector<CUfunction>& out, std::string* err, double budget_s) {

@@ -31,6 +31,53 @@ std::string jit_adjoint_source(const Pass& p, int R, int N, bool stage_params, i
 int jit_launch_adjoint(CUfunction fn, const CUtensorMap* my, const CUtensorMap* md, const double2* tab, int64_t tstride,
                        int64_t tps, int64_t ntiles, unsigned* err, double* gpart, unsigned* gcount, double* gout,
                        const int* gslot, const double2* xtab, int threads, size_t shm, int grid, cudaStream_t st);
+// One pass of a persistent uneven launch (mbk_uneven).
+struct UnevenJitPass {
+  const Pass* p;
+  int n;          // amplitude bits of one sample
+  bool first;     // pass 0 of its size: generates |0..0> when the launch asks for it
+  int nchunks;    // work items per pass and sample
+};
+// Per-size descriptor mbk_uneven reads (the generated source declares the same layout).
+struct UnevenJitGroup {
+  double2* states;        // samples back to back
+  const double2* table;   // matrix table, one row of tstride entries per sample
+  const double2* xtab;    // derived coefficients
+  const double2* xtabs;   // per-sample rows of xrow derived entries
+  long long tstride, xrow;
+};
+static_assert(sizeof(UnevenJitGroup) == 48, "UnevenJitGroup layout is mirrored in generated code");
+// Source of the persistent kernel over `passes` (item x of a launch names passes[x]) with
+// register width R, compiled for `ctas` CTAs per SM; returns its threads per CTA and dynamic
+// shared memory.
+std::string jit_uneven_source(const std::vector<UnevenJitPass>& passes, int R, int ctas, int* threads, size_t* shm);
+// pinfo[x] = (first completion counter of pass x's samples, chunks before pass x, group, 0);
+// items[i] = (pass, sample, chunk, 0).
+int jit_launch_uneven(CUfunction fn, const UnevenJitGroup* groups, const int4* pinfo, const int4* items, int nitems,
+                      unsigned* next, unsigned* done, int zero_init, unsigned* err, int threads, size_t shm, int grid,
+                      cudaStream_t st);
+// One pass of a Pauli-string expectation (pauli.cu) for a specialised kernel (mbk_pauli): the
+// pass's register bits and its flip groups with their strings (coefficient index, Z mask).
+struct PauliJitString {
+  int s;
+  uint64_t z;
+  bool real;   // the coefficient (with i^{#Y}) has no imaginary part
+};
+struct PauliJitGroup {
+  uint64_t x;
+  int xl, herm, hb;
+  std::vector<PauliJitString> strings;
+};
+struct PauliJitPass {
+  int n, nr;
+  int reg[7];
+  std::vector<PauliJitGroup> groups;
+};
+// Source of the pass, or "" when its per-thread factors need more than max_vals registers of
+// doubles (the interpreter kernel then runs the pass).
+std::string jit_pauli_source(const PauliJitPass& p, int max_vals);
+int jit_launch_pauli(CUfunction fn, const double2* v, const double2* coef, int64_t tps, double2* partials,
+                     unsigned* counters, double2* out, int grid, int batch, size_t shm, cudaStream_t st);
 int jit_launch_reg(CUfunction fn, double2* v, const double2* tab, const double2* xtab, const double2* xtabs,
                    int64_t xrow, int64_t tstride, int64_t groups, int nsamples, int grid, cudaStream_t st);
 }  // namespace mb

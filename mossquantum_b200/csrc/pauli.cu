@@ -22,6 +22,7 @@
 #include <vector>
 
 #include "internal.h"
+#include "jit.h"
 
 namespace mb {
 
@@ -74,6 +75,8 @@ struct PauliProgram {
   PGroup* d_groups = nullptr;
   PString* d_strings = nullptr;
   double2* d_tables = nullptr;
+  std::vector<void*> jit;        // per pass: specialised expectation kernel (mbk_pauli) or null
+  double2* d_coef = nullptr;     // the observable's string coefficients, for the specialised kernels
 };
 
 struct PauliData {
@@ -360,10 +363,68 @@ void pauli_free(mb_observable o) {
     dev_free(p->d_groups);
     dev_free(p->d_strings);
     dev_free(p->d_tables);
+    dev_free(p->d_coef);
+    for (void* f : p->jit)
+      if (f) jit_release(f);
     delete p;
   }
   delete o->pauli;
   o->pauli = nullptr;
+}
+
+// Specialised kernels (mbk_pauli) for the passes of a program from MB_PAULI_JIT_MIN_BITS qubits
+// (default 14; MB_PAULI_JIT=0 disables them). A pass whose per-thread factors would take too
+// many registers, or whose kernel does not compile, keeps the interpreter kernel.
+static void pauli_specialise(PauliData* pd, PauliProgram* P, const std::vector<PGroup>& hg,
+                             const std::vector<std::vector<int>>& pass_groups) {
+  P->jit.assign(P->passes.size(), nullptr);
+  const int min_bits = getenv("MB_PAULI_JIT_MIN_BITS") ? atoi(getenv("MB_PAULI_JIT_MIN_BITS")) : 14;
+  const char* e = getenv("MB_PAULI_JIT");
+  if ((e && atoi(e) == 0) || P->n < min_bits || !jit_available() || pd->strings.empty()) return;
+  std::vector<std::string> src;
+  std::vector<size_t> which;
+  for (size_t i = 0; i < P->passes.size(); ++i) {
+    const PPassArgs& pa = P->passes[i];
+    if (pa.ngroups == 0) continue;
+    PauliJitPass jp;
+    jp.n = pa.n;
+    jp.nr = pa.nr;
+    for (int r = 0; r < kPRMax; ++r) jp.reg[r] = r < pa.nr ? pa.reg[r] : 0;
+    for (size_t k = 0; k < pass_groups[i].size(); ++k) {
+      const int g = pass_groups[i][k];
+      const PGroup& G = hg[pa.g0 + k];
+      PauliJitGroup jg;
+      jg.x = G.x;
+      jg.xl = G.xl;
+      jg.herm = G.herm;
+      jg.hb = G.hb;
+      const int s0 = pd->groups[g].second.first, ns = pd->groups[g].second.second;
+      for (int s = s0; s < s0 + ns; ++s) jg.strings.push_back(PauliJitString{s, pd->strings[s].z, pd->strings[s].c.y == 0.0});
+      jp.groups.push_back(jg);
+    }
+    std::string code = jit_pauli_source(jp, 48);
+    if (code.empty()) continue;
+    src.push_back(std::move(code));
+    which.push_back(i);
+  }
+  if (src.empty()) return;
+  std::vector<double2> coef;
+  for (const PString& ps : pd->strings) coef.push_back(ps.c);
+  if (dev_alloc((void**)&P->d_coef, sizeof(double2) * coef.size()) != MB_OK) return;
+  if (cudaMemcpyAsync(P->d_coef, coef.data(), sizeof(double2) * coef.size(), cudaMemcpyHostToDevice, g_ctx.stream) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(g_ctx.stream) != cudaSuccess)
+    return;
+  std::vector<CUfunction> fns;
+  std::string err;
+  if (jit_prepare(src, fns, &err, 0.0) != MB_OK) {
+    if (getenv("MB_JIT_VERBOSE")) fprintf(stderr, "mossb200: Pauli passes interpreted: %s\n", err.c_str());
+    return;
+  }
+  for (size_t k = 0; k < which.size(); ++k) {
+    P->jit[which[k]] = (void*)fns[k];
+    if (fns[k]) jit_retain((void*)fns[k]);
+  }
 }
 
 // Pass plan for an n-qubit state, or nullptr when the fused form does not apply (fewer than
@@ -402,6 +463,7 @@ static int pauli_program(mb_observable o, int n, PauliProgram** out) {
   std::vector<PGroup> hg;
   std::vector<PString> hs;
   std::vector<double2> ht;
+  std::vector<std::vector<int>> pass_groups;  // the observable's groups each pass evaluates
   while (!rem.empty() || P->passes.empty()) {
     uint64_t regm = 0;
     for (int g : rem) {
@@ -417,7 +479,7 @@ static int pauli_program(mb_observable o, int n, PauliProgram** out) {
       if ((regm >> q) & 1) pa.reg[k++] = q;
     const uint64_t localm = uint64_t(31) | regm;
     pa.g0 = int(hg.size());
-    std::vector<int> left;
+    std::vector<int> left, took;
     for (int g : rem) {
       const uint64_t x = pd->groups[g].first;
       if ((x & ~localm) != 0 || int(hg.size()) - pa.g0 >= kPMaxGroups) {
@@ -468,7 +530,9 @@ static int pauli_program(mb_observable o, int n, PauliProgram** out) {
         }
       }
       hg.push_back(G);
+      took.push_back(g);
     }
+    pass_groups.push_back(took);
     pa.ngroups = int(hg.size()) - pa.g0;
     pa.tiles_per_sample = int64_t(1) << (n - local);
     P->passes.push_back(pa);
@@ -496,6 +560,7 @@ static int pauli_program(mb_observable o, int n, PauliProgram** out) {
     pa.strings = P->d_strings;
     pa.tables = P->d_tables;
   }
+  pauli_specialise(pd, P.get(), hg, pass_groups);
   *out = P.get();
   pd->programs.push_back(P.release());
   return MB_OK;
@@ -524,7 +589,8 @@ int expect_pauli(mb_observable o, mb_state s, double2* out) {
   if (!P) return expect_keys(o, s, out);
   cudaStream_t st = g_ctx.stream;
   MB_CHECK_CUDA(cudaMemsetAsync(out, 0, sizeof(double2) * s->batch, st));
-  for (const PPassArgs& pa : P->passes) {
+  for (size_t i = 0; i < P->passes.size(); ++i) {
+    const PPassArgs& pa = P->passes[i];
     if (pa.ngroups == 0) continue;
     int64_t per = std::max<int64_t>(1, std::min<int64_t>(int64_t(g_ctx.sm_count) * 8 / s->batch + 1,
                                                       g_ctx.partials_cap / (s->batch + 1) - 1));
@@ -533,8 +599,16 @@ int expect_pauli(mb_observable o, mb_state s, double2* out) {
       set_error("reduction workspace too small for %d samples", s->batch);
       return MB_EUNSUPPORTED;
     }
-    ProfScope ps("k_pauli_pass", 16.0 * double(s->elems) * s->batch, st);
     const size_t shm = size_t(16) << (5 + pa.nr);
+    if (i < P->jit.size() && P->jit[i]) {
+      ProfScope ps("mbk_pauli", 16.0 * double(s->elems) * s->batch, st);
+      if (int rc = jit_launch_pauli((CUfunction)P->jit[i], s->d, P->d_coef, pa.tiles_per_sample, g_ctx.partials,
+                                    g_ctx.counters, out, G, s->batch, shm, st))
+        return rc;
+      MB_LAUNCHED();
+      continue;
+    }
+    ProfScope ps("k_pauli_pass", 16.0 * double(s->elems) * s->batch, st);
     auto launch = [&](auto kern) {
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm));
       kern<<<dim3(G, s->batch), kPThreads, shm, st>>>(s->d, pa, g_ctx.partials, g_ctx.counters, out);

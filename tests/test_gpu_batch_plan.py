@@ -56,11 +56,15 @@ def test_autotune_keeps_results(mq, O):
     assert np.max(np.abs(s.to_numpy() - ref)) <= 1e-12
 
 
-def test_persistent_uneven_launch(mq, O):
-    """Pure samples of 8..17 qubits with per-sample angles run in one persistent launch (a CTA
-    per sample, all of its passes); a 6-qubit and an 18-qubit group take the per-size path
-    after it. Every sample's expectation and every 8- and 17-qubit amplitude against the oracle
-    run alone; the launch list holds exactly one k_uneven per replay."""
+@pytest.mark.parametrize("form,kernel", [("specialised", "mbk_uneven"), ("interpreted", "k_uneven")])
+def test_persistent_uneven_launch(mq, O, monkeypatch, form, kernel):
+    """Pure samples of 8..17 qubits with per-sample angles run in one persistent launch (work
+    items of (pass, sample, chunk of tiles)); a 6-qubit and an 18-qubit group take the per-size
+    path after it. Every sample's expectation and every 8- and 17-qubit amplitude against the
+    oracle run alone; the launch list holds exactly one persistent launch per replay, of the
+    straight-line form (one device function per pass) or of the micro-op interpreter."""
+    if form == "interpreted":
+        monkeypatch.setenv("MB_UNEVEN_JIT", "0")
     from mossquantum_b200 import _native as N
     from mossquantum_b200 import workloads as W
     from mossquantum_b200.batch import BatchPlan
@@ -90,8 +94,8 @@ def test_persistent_uneven_launch(mq, O):
         rep = N.profile_report()
     finally:
         N.profile(False)
-    assert rep["k_uneven"][0] == 1, rep
-    assert "k_tile_pass" not in rep, rep
+    assert rep[kernel][0] == 1, rep
+    assert "k_tile_pass" not in rep and ("k_uneven" if form == "specialised" else "mbk_uneven") not in rep, rep
     plan.close()
 
 

@@ -146,3 +146,49 @@ def test_pauli_pass_matches_dense_keys(mq, O):
     ev = mq.expectation(W.xxz(n), mq.BatchStateVector(cols))
     for b in range(B):
         assert abs(ev[b] - O.expect(cols[:, b], n, W.xxz(n).specs())) <= 1e-11
+
+
+def few_terms(mq, n, rng):
+    """A handful of 1..3-site terms (Y, ladder and projector operators, complex coefficients:
+    non-Hermitian flip groups) on sites spread over the register, few enough for the
+    specialised Pauli passes."""
+    names = ["X", "Y", "Z", "+", "-", "u", "d"]
+    terms = []
+    for k in (1, 2, 2, 3):
+        pos = [int(x) for x in rng.choice(np.arange(1, n + 1), size=k, replace=False)]
+        ops = [names[rng.integers(len(names))] for _ in range(k)]
+        terms.append(mq.QubitsTerm(pos, ops, complex(rng.normal(), rng.normal())))
+    return mq.QubitsOperator(terms)
+
+
+@pytest.mark.parametrize("jit_from", [10, 99])
+def test_specialised_pauli_passes(mq, O, monkeypatch, jit_from):
+    """Expectations through the specialised Pauli passes (strings' masks compiled in, per-thread
+    class factors; jit_from=10) and through the interpreter kernel (jit_from=99) agree with the
+    oracle for TFIM, XXZ and random operators (Y strings, complex coefficients, non-Hermitian
+    groups, strings straddling the tile bits), on single states and batches."""
+    from mossquantum_b200 import _native as N
+    from mossquantum_b200 import workloads as W
+    monkeypatch.setenv("MB_PAULI_JIT_MIN_BITS", str(jit_from))
+    rng = np.random.default_rng(5 + jit_from)
+    N.profile(True)
+    try:
+        for n in (10, 13, 16):
+            psi = random_state(n, rng)
+            s = mq.StateVector(psi)
+            for H in (W.tfim(n), W.xxz(n), random_operator(mq, n, rng, False), random_operator(mq, n, rng, True),
+                      few_terms(mq, n, rng)):
+                ref = O.expect(psi, n, H.specs())
+                assert abs(mq.expectation(H, s) - ref) <= 1e-11, (n, jit_from)
+        B, n = 4, 14
+        cols = rng.normal(size=(1 << n, B)) + 1j * rng.normal(size=(1 << n, B))
+        cols /= np.linalg.norm(cols, axis=0)
+        H = few_terms(mq, n, rng)
+        ev = mq.expectation(H, mq.BatchStateVector(cols))
+        for b in range(B):
+            assert abs(ev[b] - O.expect(cols[:, b], n, H.specs())) <= 1e-11
+        N.synchronize()
+        rep = N.profile_report()
+    finally:
+        N.profile(False)
+    assert ("mbk_pauli" in rep) == (jit_from == 10), rep
