@@ -531,6 +531,14 @@ CUfunction compile_kernel(const std::string& src, std::string* err) {
 
 bool jit_available() { return nvrtc().ok && drv().ok; }
 
+CUfunction jit_cached(const std::string& src) {
+  std::lock_guard<std::mutex> lk(g_jit_mu);
+  auto it = g_cache.find(src);
+  if (it == g_cache.end()) return nullptr;
+  it->second.last = ++g_tick;
+  return it->second.fn;
+}
+
 void jit_retain(void* fn) {
   std::lock_guard<std::mutex> lk(g_jit_mu);
   auto it = g_by_fn.find((CUfunction)fn);
@@ -1352,13 +1360,41 @@ std::string jit_pauli_source(const PauliJitPass& p, int max_vals) {
       }
     }
   }
-  o << "  double ar = 0.0, ai = 0.0;\n";
-  o << "  for (long long T = blockIdx.x; T < tps; T += G) {\n    u64 base = (u64)T << 5;\n";
+  // Tiles of 2^10 amplitudes are double-buffered: each thread's asynchronous copies of the next
+  // tile (cp.async, 16 bytes each) are in flight while the block evaluates the current one.
+  const bool dbl = pauli_jit_shm(p.nr) > (size_t(16) << local);
   std::vector<int> regs(p.reg, p.reg + p.nr);
   std::sort(regs.begin(), regs.end());
-  for (int bit : regs)
-    o << "    base = ((base >> " << bit << ") << " << (bit + 1) << ") | (base & " << ((1ull << bit) - 1) << "ull);\n";
-  for (int k = 0; k < per; ++k) o << "    tile[tx + " << k * kThreads << "u] = vs[base | lk" << k << "];\n";
+  auto tbase = [&](const std::string& t, const std::string& name) {
+    std::ostringstream e;
+    e << "    u64 " << name << " = (u64)(" << t << ") << 5;\n";
+    for (int bit : regs)
+      e << "    " << name << " = ((" << name << " >> " << bit << ") << " << (bit + 1) << ") | (" << name << " & "
+        << ((1ull << bit) - 1) << "ull);\n";
+    return e.str();
+  };
+  auto fetch = [&](const std::string& buf, const std::string& bname) {
+    std::ostringstream e;
+    for (int k = 0; k < per; ++k)
+      e << "      asm volatile(\"cp.async.cg.shared.global [%0], [%1], 16;\" :: \"r\"(sa(" << buf << " + tx + "
+        << k * kThreads << "u)), \"l\"(vs + (" << bname << " | lk" << k << ")) : \"memory\");\n";
+    return e.str();
+  };
+  o << "  double ar = 0.0, ai = 0.0;\n";
+  if (dbl) {
+    o << "  int it = 0;\n  if ((long long)blockIdx.x < tps) {\n" << tbase("blockIdx.x", "nb") << fetch("tile", "nb")
+      << "  }\n  asm volatile(\"cp.async.commit_group;\" ::: \"memory\");\n";
+    o << "  for (long long T = blockIdx.x; T < tps; T += G, ++it) {\n";
+    o << "    double2* const cur = tile + (it & 1) * " << (1 << local) << ";\n";
+    o << "    if (T + G < tps) {\n" << tbase("T + G", "nb") << fetch("tile + ((it + 1) & 1) * " + std::to_string(1 << local), "nb")
+      << "    }\n";
+    o << "    asm volatile(\"cp.async.commit_group;\" ::: \"memory\");\n"
+      << "    asm volatile(\"cp.async.wait_group 1;\" ::: \"memory\");\n";
+    o << tbase("T", "base");
+  } else {
+    o << "  for (long long T = blockIdx.x; T < tps; T += G) {\n    double2* const cur = tile;\n" << tbase("T", "base");
+    for (int k = 0; k < per; ++k) o << "    tile[tx + " << k * kThreads << "u] = vs[base | lk" << k << "];\n";
+  }
   o << "    __syncthreads();\n";
   for (size_t g = 0; g < p.groups.size(); ++g) {
     const PauliJitGroup& G = p.groups[g];
@@ -1391,10 +1427,10 @@ std::string jit_pauli_source(const PauliJitPass& p, int max_vals) {
       }
       const std::string i = idx(g, k);
       if (G.xl == 0) {
-        o << "        const double2 a = tile[" << i << "]; const double p2 = fma(a.x, a.x, a.y * a.y);\n"
+        o << "        const double2 a = cur[" << i << "]; const double p2 = fma(a.x, a.x, a.y * a.y);\n"
           << "        ar = fma(fx, p2, ar);" << (re ? "" : " ai = fma(fy, p2, ai);") << " }\n";
       } else {
-        o << "        const double2 a = tile[" << i << "], q = tile[" << i << " ^ " << G.xl << "u];\n"
+        o << "        const double2 a = cur[" << i << "], q = cur[" << i << " ^ " << G.xl << "u];\n"
           << "        const double cr = fma(a.x, q.x, a.y * q.y), ci = fma(a.x, q.y, -a.y * q.x); (void)ci;\n";
         if (herm)
           o << "        ar = fma(2.0 * fx, cr, " << (re ? "ar" : "fma(-2.0 * fy, ci, ar)") << "); }\n";
@@ -1407,6 +1443,7 @@ std::string jit_pauli_source(const PauliJitPass& p, int max_vals) {
     o << "    }\n";
   }
   o << "    __syncthreads();\n  }\n";
+  if (dbl) o << "  asm volatile(\"cp.async.wait_all;\" ::: \"memory\");\n";
   // block sum, then the last block of the sample adds the blocks' sums in block order
   o << "  for (int d = 16; d > 0; d >>= 1) { ar += __shfl_down_sync(0xffffffffu, ar, d); "
     << "ai += __shfl_down_sync(0xffffffffu, ai, d); }\n";

@@ -24,6 +24,8 @@ std::string jit_reg_source(const Pass& p, int N, bool stage_params);
 // the call still succeeds; a source that fails to compile always fails the call.
 int jit_prepare(std::vector<std::string>& sources, std::vector<CUfunction>& out, std::string* err,
                 double budget_s = 0);
+// The compiled kernel of a source if it is in the cache, else null (nothing is compiled).
+CUfunction jit_cached(const std::string& src);
 int jit_launch_tile(CUfunction fn, const CUtensorMap* map, const double2* tab, const double2* xtab, const double2* xtabs,
                     int64_t xrow, int64_t tstride, int64_t tps, int64_t ntiles, unsigned* err, int threads, size_t shm,
                     int grid, cudaStream_t st);
@@ -76,6 +78,9 @@ struct PauliJitPass {
 // Source of the pass, or "" when its per-thread factors need more than max_vals registers of
 // doubles (the interpreter kernel then runs the pass).
 std::string jit_pauli_source(const PauliJitPass& p, int max_vals);
+// Dynamic shared memory of a specialised Pauli pass: two tiles (double-buffered) of 2^(5+nr)
+// amplitudes up to nr = 5, one above.
+inline size_t pauli_jit_shm(int nr) { return (size_t(16) << (5 + nr)) * (nr <= 5 ? 2 : 1); }
 int jit_launch_pauli(CUfunction fn, const double2* v, const double2* coef, int64_t tps, double2* partials,
                      unsigned* counters, double2* out, int grid, int batch, size_t shm, cudaStream_t st);
 int jit_launch_reg(CUfunction fn, double2* v, const double2* tab, const double2* xtab, const double2* xtabs,

@@ -372,6 +372,8 @@ void pauli_free(mb_observable o) {
   o->pauli = nullptr;
 }
 
+thread_local bool t_pauli_compile = true;
+
 // Specialised kernels (mbk_pauli) for the passes of a program from MB_PAULI_JIT_MIN_BITS qubits
 // (default 14; MB_PAULI_JIT=0 disables them). A pass whose per-thread factors would take too
 // many registers, or whose kernel does not compile, keeps the interpreter kernel.
@@ -417,7 +419,9 @@ static void pauli_specialise(PauliData* pd, PauliProgram* P, const std::vector<P
     return;
   std::vector<CUfunction> fns;
   std::string err;
-  if (jit_prepare(src, fns, &err, 0.0) != MB_OK) {
+  if (!t_pauli_compile) {
+    for (const std::string& x : src) fns.push_back(jit_cached(x));
+  } else if (jit_prepare(src, fns, &err, 0.0) != MB_OK) {
     if (getenv("MB_JIT_VERBOSE")) fprintf(stderr, "mossb200: Pauli passes interpreted: %s\n", err.c_str());
     return;
   }
@@ -566,6 +570,8 @@ static int pauli_program(mb_observable o, int n, PauliProgram** out) {
   return MB_OK;
 }
 
+void pauli_allow_compile(bool on) { t_pauli_compile = on; }
+
 bool pauli_usable(mb_observable o, mb_state s) {
   PauliProgram* p = nullptr;
   if (pauli_program(o, s->n, &p) != MB_OK) return false;
@@ -603,7 +609,7 @@ int expect_pauli(mb_observable o, mb_state s, double2* out) {
     if (i < P->jit.size() && P->jit[i]) {
       ProfScope ps("mbk_pauli", 16.0 * double(s->elems) * s->batch, st);
       if (int rc = jit_launch_pauli((CUfunction)P->jit[i], s->d, P->d_coef, pa.tiles_per_sample, g_ctx.partials,
-                                    g_ctx.counters, out, G, s->batch, shm, st))
+                                    g_ctx.counters, out, G, s->batch, pauli_jit_shm(pa.nr), st))
         return rc;
       MB_LAUNCHED();
       continue;
