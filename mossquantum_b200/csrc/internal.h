@@ -155,8 +155,7 @@ int pauli_compile(mb_observable o, const mb_term* terms, size_t nterms);
 void pauli_free(mb_observable o);
 int expect_pauli(mb_observable o, mb_state s, double2* out = nullptr);
 // Whether Pauli programs built on the calling thread may compile specialised kernels (default
-// yes); when not, they use kernels already compiled for the same pass structure, else the
-// interpreter kernel.
+// yes); when not, they run on the interpreter kernel.
 void pauli_allow_compile(bool on);
 int pauli_apply(mb_observable o, const double2* in, double2* out, int n, int nsamples, double scale, bool* done);
 

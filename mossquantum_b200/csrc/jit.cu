@@ -531,14 +531,6 @@ CUfunction compile_kernel(const std::string& src, std::string* err) {
 
 bool jit_available() { return nvrtc().ok && drv().ok; }
 
-CUfunction jit_cached(const std::string& src) {
-  std::lock_guard<std::mutex> lk(g_jit_mu);
-  auto it = g_cache.find(src);
-  if (it == g_cache.end()) return nullptr;
-  it->second.last = ++g_tick;
-  return it->second.fn;
-}
-
 void jit_retain(void* fn) {
   std::lock_guard<std::mutex> lk(g_jit_mu);
   auto it = g_by_fn.find((CUfunction)fn);
@@ -1310,7 +1302,8 @@ std::string jit_pauli_source(const PauliJitPass& p, int max_vals) {
   o << kPrelude;
   o << "__device__ __forceinline__ double dneg(double a, u64 s) { return __longlong_as_double(__double_as_longlong(a) ^ "
        "(long long)s); }\n";
-  o << "extern \"C\" __global__ void __launch_bounds__(" << kThreads << ", 2) mbk_pauli(const double2* __restrict__ v, "
+  o << "extern \"C\" __global__ void __launch_bounds__(" << kThreads << ", " << std::max(1, std::min(4, p.ctas))
+    << ") mbk_pauli(const double2* __restrict__ v, "
     << "const double2* __restrict__ coef, long long tps, double2* partials, u32* counters, double2* out) {\n";
   o << "  extern __shared__ double2 tile[];\n  __shared__ double2 wp[" << kThreads / 32 << "];\n  __shared__ bool last;\n";
   o << "  const u32 tx = threadIdx.x;\n  const int b = blockIdx.y, G = gridDim.x;\n";
@@ -1425,12 +1418,12 @@ std::string jit_pauli_source(const PauliJitPass& p, int max_vals) {
         else
           o << "        { const double2 t = " << (C.zh ? "cneg(" + F + ", " + s + ")" : F) << "; fx += t.x; fy += t.y; }\n";
       }
-      const std::string i = idx(g, k);
+      const std::string i = idx(g, k), av = "cur[" + i + "]";
       if (G.xl == 0) {
-        o << "        const double2 a = cur[" << i << "]; const double p2 = fma(a.x, a.x, a.y * a.y);\n"
+        o << "        const double2 a = " << av << "; const double p2 = fma(a.x, a.x, a.y * a.y);\n"
           << "        ar = fma(fx, p2, ar);" << (re ? "" : " ai = fma(fy, p2, ai);") << " }\n";
       } else {
-        o << "        const double2 a = cur[" << i << "], q = cur[" << i << " ^ " << G.xl << "u];\n"
+        o << "        const double2 a = " << av << ", q = cur[" << i << " ^ " << G.xl << "u];\n"
           << "        const double cr = fma(a.x, q.x, a.y * q.y), ci = fma(a.x, q.y, -a.y * q.x); (void)ci;\n";
         if (herm)
           o << "        ar = fma(2.0 * fx, cr, " << (re ? "ar" : "fma(-2.0 * fy, ci, ar)") << "); }\n";

@@ -24,8 +24,6 @@ std::string jit_reg_source(const Pass& p, int N, bool stage_params);
 // the call still succeeds; a source that fails to compile always fails the call.
 int jit_prepare(std::vector<std::string>& sources, std::vector<CUfunction>& out, std::string* err,
                 double budget_s = 0);
-// The compiled kernel of a source if it is in the cache, else null (nothing is compiled).
-CUfunction jit_cached(const std::string& src);
 int jit_launch_tile(CUfunction fn, const CUtensorMap* map, const double2* tab, const double2* xtab, const double2* xtabs,
                     int64_t xrow, int64_t tstride, int64_t tps, int64_t ntiles, unsigned* err, int threads, size_t shm,
                     int grid, cudaStream_t st);
@@ -74,6 +72,7 @@ struct PauliJitPass {
   int n, nr;
   int reg[7];
   std::vector<PauliJitGroup> groups;
+  int ctas = 3;   // CTAs per SM the kernel's registers are bounded for
 };
 // Source of the pass, or "" when its per-thread factors need more than max_vals registers of
 // doubles (the interpreter kernel then runs the pass).

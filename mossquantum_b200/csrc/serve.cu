@@ -519,8 +519,8 @@ void issue(mb_server S, size_t* res_off, int* nres) {
 
 void server_loop(mb_server S) {
   cudaSetDevice(g_ctx.device);
-  // Expectation passes on this thread take specialised kernels only from the compile cache: a
-  // request never waits for NVRTC on an observable shape first met here.
+  // Expectation passes built on this thread stay on the interpreter kernel: a request never
+  // waits for NVRTC on an observable first met here.
   pauli_allow_compile(false);
   for (;;) {
     bool stopping;
