@@ -460,8 +460,9 @@ def _case_setup(name, mq, W):
                 mq.apply_(c, st, theta=th)
         return f"uneven batch, pure part: {sum(counts.values())} states, sizes {min(counts)}..{max(counts)}", step
     if name == "uneven":
-        # the uneven batch's sizes below 18 qubits in the persistent launch (k_uneven), run
-        # eagerly (binding and fused products of all sizes, then the one pass launch)
+        # the uneven batch's sizes below 18 qubits in the persistent launch (mbk_uneven, or
+        # k_uneven without NVRTC), run eagerly (binding and fused products of all sizes, then
+        # the one pass launch)
         from mossquantum_b200.batch import BatchPlan
         rng2 = W.rng_for(2)
         sizes = rng2.integers(10, 23, size=512)

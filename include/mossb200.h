@@ -210,12 +210,14 @@ MB_API int mb_graph_free(mb_graph g);
  * (batches of the reference hold one register size, src/states/batch_state_vector.jl; this is
  * the B200 form of many sizes with per-sample parameters). A plan over groups (circuit g on
  * state g: a pure batch of one register size, its parameters staged with mb_theta_upload, one
- * row per sample) runs every group of 8..17 qubits in ONE persistent kernel: CTAs take whole
- * samples from a work counter, largest first, and run all of the sample's tile passes (two
- * small launches before it bind the parameter rows and form the fused single-qubit products
- * of every group). Other groups (more qubits, density matrices, instructions a tile cannot
- * hold) run through mb_apply's fused path after it. Circuits and states must outlive the
- * plan. mb_uneven_apply may be recorded into a graph once it has run eagerly. */
+ * row per sample) runs every pure group of 8..17 qubits in ONE persistent kernel: CTAs take
+ * work items (pass, sample, chunk of tiles) from a work counter, pass by pass, each waiting
+ * for its sample's previous pass; the passes run as straight-line code compiled for the plan
+ * (NVRTC, at mb_uneven_create), or through the micro-op interpreter without NVRTC (two small
+ * launches before it bind the parameter rows and form the fused single-qubit products of every
+ * group). Other groups (more qubits, density matrices, instructions a tile cannot hold) run
+ * through mb_apply's fused path after it. Circuits and states must outlive the plan.
+ * mb_uneven_apply may be recorded into a graph once it has run eagerly. */
 typedef struct mb_uneven_s* mb_uneven;
 #define MB_UNEVEN_ZERO 1  /* start every sample from |0...0> */
 MB_API int mb_uneven_create(const mb_circuit* circuits, const mb_state* states, int ngroups, mb_uneven* out);

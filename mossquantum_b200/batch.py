@@ -3,12 +3,13 @@
 MOSSQuantum's batches share one register size and one parameter vector
 (src/states/batch_state_vector.jl, docs/architecture.md). A ``BatchPlan`` accepts samples
 of different qubit counts, each with its own parameters. Pure samples of 8..17 qubits run in
-ONE persistent kernel launch (``mb_uneven_apply``): its CTAs take whole samples from a work
-counter, largest first, and run every tile pass of the sample's circuit, so no launch is
-spent per size or per pass. Larger samples and density matrices are grouped by size into
-device batches that run the fused pass kernels over all of their samples at once. The whole
-sequence (reset, parameter binding, passes, expectations) is recorded once into a CUDA graph;
-``run`` uploads the parameters and replays the graph.
+ONE persistent kernel launch (``mb_uneven_apply``): its CTAs take work items (pass, sample,
+chunk of tiles) from a work counter, pass by pass, and run them with straight-line code
+compiled for the plan's passes, so no launch is spent per size or per pass. Larger samples and
+density matrices are grouped by size into device batches that run the fused pass kernels over
+all of their samples at once. The whole sequence (reset, parameter binding, passes,
+expectations) is recorded once into a CUDA graph; ``run`` uploads the parameters and replays
+the graph.
 """
 from __future__ import annotations
 
