@@ -74,6 +74,7 @@ struct Drv {
   CUresult (*launch)(CUfunction, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned, CUstream,
                      void**, void**) = nullptr;
   CUresult (*setattr)(CUfunction, CUfunction_attribute, int) = nullptr;
+  CUresult (*getattr)(int*, CUfunction_attribute, CUfunction) = nullptr;
   CUresult (*unload)(CUmodule) = nullptr;
   bool ok = false;
 };
@@ -90,6 +91,7 @@ Drv& drv() {
   if (cudaGetDriverEntryPoint("cuLaunchKernel", &p, cudaEnableDefault, &q) == cudaSuccess && p) d.launch = (decltype(d.launch))p;
   if (cudaGetDriverEntryPoint("cuFuncSetAttribute", &p, cudaEnableDefault, &q) == cudaSuccess && p) d.setattr = (decltype(d.setattr))p;
   if (cudaGetDriverEntryPoint("cuModuleUnload", &p, cudaEnableDefault, &q) == cudaSuccess && p) d.unload = (decltype(d.unload))p;
+  if (cudaGetDriverEntryPoint("cuFuncGetAttribute", &p, cudaEnableDefault, &q) == cudaSuccess && p) d.getattr = (decltype(d.getattr))p;
   d.ok = d.load && d.getfn && d.launch && d.setattr;
   return d;
 }
@@ -530,6 +532,13 @@ CUfunction compile_kernel(const std::string& src, std::string* err) {
 }  // namespace
 
 bool jit_available() { return nvrtc().ok && drv().ok; }
+
+int jit_local_bytes(void* fn) {
+  Drv& d = drv();
+  int v = -1;
+  if (!fn || !d.getattr || d.getattr(&v, CU_FUNC_ATTRIBUTE_LOCAL_SIZE_BYTES, (CUfunction)fn) != CUDA_SUCCESS) return -1;
+  return v;
+}
 
 void jit_retain(void* fn) {
   std::lock_guard<std::mutex> lk(g_jit_mu);

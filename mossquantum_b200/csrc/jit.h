@@ -9,6 +9,8 @@
 
 namespace mb {
 bool jit_available();
+// Local memory (register spills, stack) per thread of a compiled kernel, or -1 if unknown.
+int jit_local_bytes(void* fn);
 // Reference counts of the compiled kernels a schedule uses; jit_trim unloads unreferenced
 // modules beyond the cache cap (MB_JIT_CACHE_MAX).
 void jit_retain(void* fn);

@@ -387,9 +387,15 @@ static void pauli_specialise(PauliData* pd, PauliProgram* P, const std::vector<P
   if ((e && atoi(e) == 0) || P->n < min_bits || !t_pauli_compile || !jit_available() || pd->strings.empty()) return;
   std::vector<std::string> src;
   std::vector<size_t> which;
+  // Passes of 2^12-amplitude tiles (from 24 qubits) keep the interpreter unless
+  // MB_PAULI_JIT_WIDE=1: their per-thread factors fill the registers, and with them on, a
+  // 24-qubit gradient alternating with a density-matrix gradient ran 2-3.5x slower per step
+  // than either alone (cause not identified).
+  const char* wide = getenv("MB_PAULI_JIT_WIDE");
+  const bool wide_ok = wide && atoi(wide) == 1;
   for (size_t i = 0; i < P->passes.size(); ++i) {
     const PPassArgs& pa = P->passes[i];
-    if (pa.ngroups == 0) continue;
+    if (pa.ngroups == 0 || (pa.nr > 5 && !wide_ok)) continue;
     PauliJitPass jp;
     // 3 CTAs per SM for 2^10-amplitude tiles (0.84 against 0.90 ms for XXZ on 50 samples of 20
     // qubits at 2), 2 for 2^12 ones, whose per-thread factors need more registers
@@ -429,9 +435,11 @@ static void pauli_specialise(PauliData* pd, PauliProgram* P, const std::vector<P
     if (getenv("MB_JIT_VERBOSE")) fprintf(stderr, "mossb200: Pauli passes interpreted: %s\n", err.c_str());
     return;
   }
+  // a kernel that spills to local memory keeps the interpreter pass
   for (size_t k = 0; k < which.size(); ++k) {
+    if (!fns[k] || jit_local_bytes((void*)fns[k]) != 0) continue;
     P->jit[which[k]] = (void*)fns[k];
-    if (fns[k]) jit_retain((void*)fns[k]);
+    jit_retain((void*)fns[k]);
   }
 }
 
