@@ -1,5 +1,6 @@
 // Host-only harness for tests/test_jit_sources.py: generates specialised-kernel sources (Pauli
-// expectation passes, a persistent uneven launch) from hand-built pass descriptions, compiles
+// expectation passes, a persistent uneven launch, a tile pass, a dual-state reverse pass with a
+// gradient accumulator) from hand-built pass descriptions, compiles
 // each with NVRTC for sm_100a (no GPU needed) and prints one JSON line per source with the
 // compile status, registers and spill bytes reported by ptxas.
 #include <dlfcn.h>
@@ -153,5 +154,21 @@ int main() {
   const std::string src = jit_uneven_source(passes, 3, 4, &threads, &shm);
   compile_and_report("uneven_n14_n8", src);
   printf("{\"name\": \"uneven_launch\", \"threads\": %d, \"shm\": %zu}\n", threads, shm);
+  // a tile pass and a dual-state reverse pass (with a rotation-generator gradient) of a
+  // 14-qubit state: TMA boxes over bits 0..9 of a two-dimensional amplitude tensor
+  Pass pt = tile_pass(10);
+  pt.geom.ndims = 2;
+  pt.geom.start[0] = 0;
+  pt.geom.bits[0] = 10;
+  pt.geom.boxb[0] = 10;
+  pt.geom.start[1] = 10;
+  pt.geom.bits[1] = 4;
+  pt.geom.boxb[1] = 0;
+  compile_and_report("tile_n14", jit_tile_source(pt, 3, 14, false, 4));
+  Pass pa = pt;
+  pa.mops.push_back(mop(MOP_GRADP, 0, 2, {}, 0, 0, {}));  // closes stage 1 (ops 2..5)
+  pa.stages[1].nops += 1;
+  pa.grad_slots = {0};
+  compile_and_report("adjoint_n14", jit_adjoint_source(pa, 3, 14, true, 3));
   return 0;
 }

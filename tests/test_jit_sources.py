@@ -4,8 +4,9 @@ The harness (tests/jit_sources_harness.cu) links the library's source generator 
 Pauli expectation passes for nearest-neighbour Hamiltonians (XXZ, TFIM) with the tile's
 register bits low and high in the register, and a persistent uneven launch over a 14-qubit
 group (with pass-0 generation of |0..0>) and an 8-qubit group whose tiles need fewer threads
-than the launch has. Every source must compile; the Pauli passes must fit their register
-budget without spills, since a spilling kernel is not used.
+than the launch has, a TMA-staged tile pass and a dual-state reverse pass with a gradient
+accumulator. Every source must compile; the Pauli passes must fit their register budget
+without spills, since a spilling kernel is not used.
 """
 import json
 import os
@@ -50,3 +51,9 @@ def test_persistent_uneven_source_compiles(harness_lines):
     # copy in dynamic shared memory
     assert launch["threads"] == 128
     assert launch["shm"] >= 16 << 10
+
+
+def test_tile_and_reverse_pass_sources_compile(harness_lines):
+    for name in ("tile_n14", "adjoint_n14"):
+        r = harness_lines[name]
+        assert r["rc"] == 0 and r["bytes"] > 0 and r["spill"] == 0, r
