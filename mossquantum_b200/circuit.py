@@ -8,6 +8,7 @@ rebinding never recompiles the circuit.
 """
 from __future__ import annotations
 
+import itertools
 import weakref
 
 import numpy as np
@@ -132,12 +133,13 @@ class QCircuit(Instruction):
     # lowering ---------------------------------------------------------------------------
     def compiled(self, n: int) -> "CompiledCircuit":
         """The C-ABI circuit for an n-qubit register (cached; parameter values excluded)."""
-        key = (n, self._signature())
+        plain = _plain_lowering(self.flat())
+        key = (n, plain[0] if plain is not None else self._signature())
         h = self._compiled.get(key)
         if h is None:
             if len(self._compiled) > 8:
                 self._invalidate()
-            h = CompiledCircuit(self, n)
+            h = CompiledCircuit(self, n, plain)
             self._compiled[key] = h
         return h
 
@@ -167,10 +169,80 @@ class QCircuit(Instruction):
         return f"QCircuit({len(self.items)} instructions)"
 
 
+_OP_DTYPE = np.dtype(N.MbOp)   # mb_op as a numpy record (same layout as the ctypes struct)
+
+
+def _plain_lowering(items):
+    """Vectorised lowering of a circuit made only of matrix gates (``QuantumGate``) and fixed
+    gates: (signature, mb_op records, buffers they point into), or None for any other circuit.
+
+    Every such instruction lowers to one matrix op without parameters, exactly as its own
+    ``_ops`` would: the matrices of the matrix gates are packed column-major into one buffer
+    per size (fixed gates point at their class's shared copy), and the records are filled as
+    columns. The signature hashes the instruction types, positions and matrix bytes; its
+    leading tag keeps it apart from the general signature."""
+    from .gates import QuantumGate, _FixedGate
+    fixed_ops = _FixedGate._ops
+    names, positions = [], []
+    groups, fixed, bynq = {}, {}, {}
+    for i, it in enumerate(items):
+        t = type(it)
+        if t is QuantumGate:
+            groups.setdefault(len(it.pos), []).append(i)
+        elif isinstance(it, _FixedGate) and t._ops is fixed_ops:
+            fixed.setdefault(t, []).append(i)
+        else:
+            return None
+        names.append(t.__name__)
+        positions.append(it.pos)
+        bynq.setdefault(len(it.pos), []).append(i)
+    m = len(items)
+    recs = np.zeros(m, dtype=_OP_DTYPE)
+    keep, blobs, classes = [], [], []
+    for k in sorted(groups):
+        idx = groups[k]
+        d = 1 << k
+        raw = b"".join([items[i].data.tobytes() for i in idx])   # row-major matrices
+        blobs.append(raw)
+        mats = np.frombuffer(raw, dtype=np.complex128).reshape(len(idx), d, d)
+        buf = np.ascontiguousarray(mats.transpose(0, 2, 1)).view(np.float64)
+        keep.append(buf)
+        recs["data"][idx] = np.uint64(buf.ctypes.data) + np.arange(len(idx), dtype=np.uint64) * np.uint64(16 * d * d)
+    for t in sorted(fixed, key=lambda t: t.__name__):
+        b = t._packed_matrix()
+        keep.append(b)
+        recs["data"][fixed[t]] = b.ctypes.data
+        classes.append((t.__name__, b.tobytes()))
+    for k, idx in bynq.items():
+        flat = np.fromiter(itertools.chain.from_iterable(positions[i] for i in idx), dtype=np.int32,
+                           count=len(idx) * k)
+        recs["pos"][idx, :k] = flat.reshape(len(idx), k) - 1
+        recs["nq"][idx] = k
+    recs["kind"] = N.MB_OP_GATE
+    recs["family"] = N.FAMILIES["MATRIX"]
+    recs["slot"] = -1
+    sig = hash(("plain-matrix-and-fixed", tuple(names), tuple(positions), tuple(classes), tuple(blobs)))
+    return sig, recs, keep
+
+
 class CompiledCircuit:
     """Owner of an ``mb_circuit`` handle."""
 
-    def __init__(self, circuit: QCircuit, n: int):
+    def __init__(self, circuit: QCircuit, n: int, plain=None):
+        """plain: the circuit's ``_plain_lowering`` result, when it has one."""
+        self.n = n
+        if plain is not None:
+            _, recs, keep = plain
+            self.nslots = 0
+            self.nparams = 0
+            self.slot_map = []
+            self.gradient_ok = True
+            h = N.ctypes.c_void_p()
+            arr = recs.ctypes.data_as(N.ctypes.POINTER(N.MbOp))
+            N.check(N.lib().mb_circuit_create(arr, len(recs), n, N.ctypes.byref(h)), "mb_circuit_create")
+            self.handle = h
+            self._finalizer = weakref.finalize(self, _free_circuit, h.value)
+            return
         keep = []
         ops = []
         slot = 0
@@ -186,7 +258,6 @@ class CompiledCircuit:
                 pass
             ops.extend(o)
             slot += used
-        self.n = n
         self.nslots = slot
         self.nparams = circuit.nparameters()
         self.slot_map = self._slot_map(circuit)
