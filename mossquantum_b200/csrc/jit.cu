@@ -1476,10 +1476,25 @@ int jit_launch_pauli(CUfunction fn, const double2* v, const double2* coef, int64
 
 int jit_prepare(std::vector<std::string>& sources, std::vector<CUfunction>& out, std::string* err, double budget_s) {
   out.assign(sources.size(), nullptr);
+  // kernels already compiled are taken here; worker threads start only for the others
+  std::vector<size_t> todo;
+  {
+    std::lock_guard<std::mutex> lk(g_jit_mu);
+    for (size_t i = 0; i < sources.size(); ++i) {
+      auto it = g_cache.find(sources[i]);
+      if (it != g_cache.end()) {
+        out[i] = it->second.fn;
+        it->second.last = ++g_tick;
+      } else {
+        todo.push_back(i);
+      }
+    }
+  }
+  if (todo.empty()) return MB_OK;
   std::vector<std::string> errs(sources.size());
   std::vector<char> skipped(sources.size(), 0);
   std::vector<std::thread> pool;
-  const size_t nthreads = std::max<size_t>(1, std::min<size_t>(sources.size(), std::thread::hardware_concurrency()));
+  const size_t nthreads = std::max<size_t>(1, std::min<size_t>(todo.size(), std::thread::hardware_concurrency()));
   // Compilation runs on worker threads; modules load on the worker threads too, which is
   // fine because the runtime's primary context is current on every thread of the process.
   int dev = 0;
@@ -1491,7 +1506,8 @@ int jit_prepare(std::vector<std::string>& sources, std::vector<CUfunction>& out,
     pool.emplace_back([&] {
       cudaSetDevice(dev);
       cudaFree(nullptr);
-      for (size_t i = next++; i < sources.size(); i = next++) {
+      for (size_t j = next++; j < todo.size(); j = next++) {
+        const size_t i = todo[j];
         // Past the budget only kernels already in the cache are taken; the rest run interpreted.
         if (budget_s > 0 && elapsed() > budget_s) {
           std::lock_guard<std::mutex> lk(g_jit_mu);
