@@ -923,6 +923,7 @@ static void build_fops(mb_circuit c, int n, int dm, bool dagger, std::vector<FOp
   out.clear();
   std::vector<FOp> seq;
   if (hi < 0) hi = int(c->ops.size());
+  seq.reserve(size_t(std::max(0, hi - lo)) * (dm ? 2 : 1));
   if (dagger) S = nullptr;
   for (int oi = lo; oi < hi; ++oi) {
     const COp& op = c->ops[oi];
@@ -959,7 +960,7 @@ static void build_fops(mb_circuit c, int n, int dm, bool dagger, std::vector<FOp
     if (S->fuse && !getenv("MB_NO_FUSE")) fuse_runs(c, seq, n, dm, S);
     if (!getenv("MB_NO_SPLIT")) {
       std::vector<FOp> split;
-      split.reserve(seq.size() * 2);
+      split.reserve(seq.size() * 3);  // a fixed 2x2 splits into up to three ops
       for (FOp& f : seq)
         if (!split_fixed_1q(c, f, dm, &S->xtab, split)) split.push_back(std::move(f));
       merge_phases(split, dm, &S->xtab);
