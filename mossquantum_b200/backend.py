@@ -13,7 +13,7 @@ import numpy as np
 
 from . import _native as N
 from .channels import QuantumMap
-from .circuit import QCircuit
+from .circuit import QCircuit, _matrix_lowering
 from .gates import Gate
 from .operators import QubitsOperator, QubitsTerm, as_operator
 from .states import (BatchDensityMatrix, BatchStateVector, DensityMatrix, StateVector, _DeviceState, density_of)
@@ -66,6 +66,18 @@ def _validate_positions(operation, n):
             raise ValueError(f"position out of range for {n} qubits in {it!r}")
 
 
+def _matrix_ops_fit(recs, n):
+    """Every record of a matrix lowering acts on at most five qubits, all inside n."""
+    if len(recs) == 0:
+        return True
+    nq = recs["nq"]
+    if int(nq.max()) > 5:
+        return False
+    pos = recs["pos"]
+    used = np.arange(5)[None, :] < nq[:, None]
+    return bool(np.all(np.where(used, pos, 0) < n))
+
+
 def _as_circuit(operation):
     if isinstance(operation, QCircuit):
         return operation
@@ -89,14 +101,22 @@ def apply_(operation, state, theta=None, plain=False, tensor=False):
     """
     if not isinstance(state, _DeviceState):
         raise TypeError("apply_ needs a B200 state")
-    if not supports(_BACKEND, operation, state, "apply"):
-        raise UnsupportedOperation(f"B200Backend cannot apply {type(operation).__name__}")
-    _validate_positions(operation, state.n)
-    circuit = _as_circuit(operation)
-    if circuit.has_channel() and not state.is_density:
-        state = density_of(state)
-    compiled = circuit.compiled(state.n)
-    values = circuit.active_parameters() if theta is None else theta
+    circuit = _as_circuit(operation) if isinstance(operation, (Gate, QCircuit)) else None
+    lowered = _matrix_lowering(circuit.flat()) if circuit is not None else None
+    if lowered is not None and _matrix_ops_fit(lowered[1], state.n):
+        # matrix and fixed gates of at most five qubits inside the register: supported, no
+        # channels, no parameters; the lowering doubles as the compile-cache signature
+        compiled = circuit.compiled(state.n, lowered=lowered)
+        values = np.zeros(0) if theta is None else theta
+    else:
+        if not supports(_BACKEND, operation, state, "apply"):
+            raise UnsupportedOperation(f"B200Backend cannot apply {type(operation).__name__}")
+        _validate_positions(operation, state.n)
+        circuit = _as_circuit(operation)
+        if circuit.has_channel() and not state.is_density:
+            state = density_of(state)
+        compiled = circuit.compiled(state.n)
+        values = circuit.active_parameters() if theta is None else theta
     values = np.asarray(values, dtype=np.float64)
     flags = N.MB_APPLY_PLAIN if plain else N.MB_APPLY_FUSED
     if plain and tensor:

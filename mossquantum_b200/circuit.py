@@ -131,15 +131,17 @@ class QCircuit(Instruction):
         return [it.spec() for it in self.flat()]
 
     # lowering ---------------------------------------------------------------------------
-    def compiled(self, n: int) -> "CompiledCircuit":
-        """The C-ABI circuit for an n-qubit register (cached; parameter values excluded)."""
-        plain = _plain_lowering(self.flat())
-        key = (n, plain[0] if plain is not None else self._signature())
+    def compiled(self, n: int, lowered=None) -> "CompiledCircuit":
+        """The C-ABI circuit for an n-qubit register (cached; parameter values excluded).
+        lowered: this circuit's ``_matrix_lowering`` when the caller has it already."""
+        if lowered is None:
+            lowered = _matrix_lowering(self.flat())
+        key = (n, lowered[0] if lowered is not None else self._signature())
         h = self._compiled.get(key)
         if h is None:
             if len(self._compiled) > 8:
                 self._invalidate()
-            h = CompiledCircuit(self, n, plain)
+            h = CompiledCircuit(self, n, lowered)
             self._compiled[key] = h
         return h
 
@@ -172,7 +174,7 @@ class QCircuit(Instruction):
 _OP_DTYPE = np.dtype(N.MbOp)   # mb_op as a numpy record (same layout as the ctypes struct)
 
 
-def _plain_lowering(items):
+def _matrix_lowering(items):
     """Vectorised lowering of a circuit made only of matrix gates (``QuantumGate``) and fixed
     gates: (signature, mb_op records, buffers they point into), or None for any other circuit.
 
@@ -221,18 +223,18 @@ def _plain_lowering(items):
     recs["kind"] = N.MB_OP_GATE
     recs["family"] = N.FAMILIES["MATRIX"]
     recs["slot"] = -1
-    sig = hash(("plain-matrix-and-fixed", tuple(names), tuple(positions), tuple(classes), tuple(blobs)))
+    sig = hash(("matrix-and-fixed-gates", tuple(names), tuple(positions), tuple(classes), tuple(blobs)))
     return sig, recs, keep
 
 
 class CompiledCircuit:
     """Owner of an ``mb_circuit`` handle."""
 
-    def __init__(self, circuit: QCircuit, n: int, plain=None):
-        """plain: the circuit's ``_plain_lowering`` result, when it has one."""
+    def __init__(self, circuit: QCircuit, n: int, lowered=None):
+        """lowered: the circuit's ``_matrix_lowering`` result, when it has one."""
         self.n = n
-        if plain is not None:
-            _, recs, keep = plain
+        if lowered is not None:
+            _, recs, keep = lowered
             self.nslots = 0
             self.nparams = 0
             self.slot_map = []
