@@ -147,6 +147,7 @@ int main() {
   compile_and_report("pauli_xxz_n20_bits5_9", jit_pauli_source(nn_pass(20, low, true), 48));
   compile_and_report("pauli_xxz_n20_bits9_13", jit_pauli_source(nn_pass(20, high, true), 48));
   compile_and_report("pauli_tfim_n22_bits5_9", jit_pauli_source(nn_pass(22, low, false), 48));
+  compile_and_report("pauli_xxz_n22_bits5_9", jit_pauli_source(nn_pass(22, low, true), 48));
   const Pass p10 = tile_pass(10), p8 = tile_pass(8);
   std::vector<UnevenJitPass> passes = {{&p10, 14, true, 4}, {&p10, 14, false, 4}, {&p8, 8, true, 1}};
   int threads = 0;

@@ -36,7 +36,8 @@ def harness_lines(tmp_path_factory):
 
 
 def test_pauli_pass_sources_compile_without_spills(harness_lines):
-    for name in ("pauli_xxz_n20_bits5_9", "pauli_xxz_n20_bits9_13", "pauli_tfim_n22_bits5_9"):
+    for name in ("pauli_xxz_n20_bits5_9", "pauli_xxz_n20_bits9_13", "pauli_tfim_n22_bits5_9",
+                 "pauli_xxz_n22_bits5_9"):
         r = harness_lines[name]
         assert r["bytes"] > 0, name
         assert r["rc"] == 0, name
